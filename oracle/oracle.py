@@ -1,0 +1,227 @@
+"""TEST INFRASTRUCTURE (oracle).  ctypes binding of liboracle.so.
+
+liboracle.so is the plain-C restatement of the reference's Langevin step
+(nspt_oracle.c).  Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline
+leg of ``bench.py`` import this module, and only as the checker.
+
+Also drives the reference's own code built by ``build_ref.sh`` (``oracle/_ref``)
+when that binary is present: ``run_reference`` runs it and parses its outputs.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def build() -> str:
+    """Compile liboracle.so (gcc, seconds)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return os.path.join(HERE, "liboracle.so")
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        src = os.path.join(HERE, "nspt_oracle.c")
+        if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+            build()
+        L = ctypes.CDLL(path)
+        P = ctypes.c_void_p
+        D = ctypes.POINTER(ctypes.c_double)
+        L.oracle_create.restype = P
+        L.oracle_create.argtypes = [ctypes.POINTER(ctypes.c_int), ctypes.c_int, ctypes.c_int]
+        L.oracle_destroy.argtypes = [P]
+        L.oracle_links.restype = D
+        L.oracle_links.argtypes = [P]
+        L.oracle_volume.restype = ctypes.c_long
+        L.oracle_volume.argtypes = [P]
+        L.oracle_cold_start.argtypes = [P]
+        L.oracle_random_start.argtypes = [P, ctypes.c_long, ctypes.c_double]
+        L.oracle_sweep.argtypes = [P, ctypes.c_double, D, D, D, D, ctypes.c_int]
+        L.oracle_zero_modes.argtypes = [P]
+        L.oracle_fa_gauge_fix.argtypes = [P, ctypes.c_double]
+        L.oracle_local_gauge_fix.argtypes = [P, ctypes.c_double]
+        L.oracle_plaquette.argtypes = [P, D]
+        for f in ("oracle_ser_mul",):
+            getattr(L, f).argtypes = [ctypes.c_int, D, D, D]
+        for f in ("oracle_ser_exp", "oracle_ser_log", "oracle_ser_dag"):
+            getattr(L, f).argtypes = [ctypes.c_int, D, D]
+        L.oracle_ser_reH.argtypes = [ctypes.c_int, D]
+        L.oracle_rng_create.restype = P
+        L.oracle_rng_create.argtypes = [ctypes.c_long]
+        L.oracle_rng_destroy.argtypes = [P]
+        L.oracle_rng_gauss.argtypes = [P, D, ctypes.c_long]
+        L.oracle_su3rand.argtypes = [D, D]
+        _LIB = L
+    return _LIB
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def series_len(N: int) -> int:
+    """Doubles per series: flag + N orders x 9 complex."""
+    return 2 + 18 * N
+
+
+class Rand55:
+    """The reference's MyRand generator (rand55 + Box-Muller, MyRand.cc)."""
+
+    def __init__(self, seed: int):
+        self._h = lib().oracle_rng_create(int(seed))
+
+    def gauss(self, n: int) -> np.ndarray:
+        out = np.empty(int(n), dtype=np.float64)
+        lib().oracle_rng_gauss(self._h, _dp(out), int(n))
+        return out
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _LIB is not None:
+            _LIB.oracle_rng_destroy(h)
+            self._h = None
+
+
+@dataclass
+class SweepObs:
+    plaq: np.ndarray  # (N+1, 2)
+    norm: np.ndarray  # (N,)
+    tru: np.ndarray  # (4, N, 2)
+
+
+class Oracle:
+    """One lattice field on the host, reference AoS layout."""
+
+    def __init__(self, L, N: int, twist_mask: int = 0):
+        self.L = tuple(int(x) for x in L)
+        self.N = int(N)
+        arr = (ctypes.c_int * 4)(*self.L)
+        self._h = lib().oracle_create(arr, self.N, int(twist_mask))
+        if not self._h:
+            raise ValueError("oracle_create rejected the lattice")
+        self.V = int(lib().oracle_volume(self._h))
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h and _LIB is not None:
+            _LIB.oracle_destroy(h)
+            self._h = None
+
+    @property
+    def links(self) -> np.ndarray:
+        """View (V, 4, 2+18N) of the field (reference byte layout)."""
+        p = lib().oracle_links(self._h)
+        n = self.V * 4 * series_len(self.N)
+        flat = np.ctypeslib.as_array(p, shape=(n,))
+        return flat.reshape(self.V, 4, series_len(self.N))
+
+    def set_links(self, a: np.ndarray):
+        self.links[...] = np.asarray(a, dtype=np.float64).reshape(self.links.shape)
+
+    def cold_start(self):
+        lib().oracle_cold_start(self._h)
+
+    def random_start(self, seed: int, sigma: float = 0.5):
+        lib().oracle_random_start(self._h, int(seed), float(sigma))
+
+    def sweep(self, dt: float, noise: np.ndarray, zero_modes: bool = False) -> SweepObs:
+        N = self.N
+        noise = np.ascontiguousarray(noise, dtype=np.float64)
+        assert noise.size == self.V * 4 * 8
+        plaq = np.zeros((N + 1, 2))
+        norm = np.zeros(N)
+        tru = np.zeros((4, N, 2))
+        lib().oracle_sweep(self._h, float(dt), _dp(noise), _dp(plaq), _dp(norm), _dp(tru),
+                           1 if zero_modes else 0)
+        return SweepObs(plaq, norm, tru)
+
+    def zero_modes(self):
+        lib().oracle_zero_modes(self._h)
+
+    def fa_gauge_fix(self, alpha: float):
+        lib().oracle_fa_gauge_fix(self._h, float(alpha))
+
+    def local_gauge_fix(self, alpha: float):
+        lib().oracle_local_gauge_fix(self._h, float(alpha))
+
+    def plaquette(self) -> np.ndarray:
+        out = np.zeros((self.N + 1, 2))
+        lib().oracle_plaquette(self._h, _dp(out))
+        return out
+
+
+def ser_op(name: str, N: int, *args: np.ndarray) -> np.ndarray:
+    out = np.zeros(series_len(N))
+    fn = getattr(lib(), "oracle_ser_" + name)
+    fn(int(N), *[_dp(np.ascontiguousarray(a, dtype=np.float64)) for a in args], _dp(out))
+    return out
+
+
+# ---------------------------------------------------------------------------
+# The reference's own code (oracle/_ref, built by build_ref.sh)
+# ---------------------------------------------------------------------------
+
+def ref_binary(N: int, bc: str = "pbc", gf: str = "local", grid=(1, 1, 1)) -> str:
+    return os.path.join(HERE, "_ref", "ref_N%d_%s_%s_t%d%d%d" % ((N, bc, gf) + tuple(grid)),
+                        "ref_harness")
+
+
+def build_reference(N: int, bc: str = "pbc", gf: str = "local", grid=(1, 1, 1)) -> str:
+    subprocess.run([os.path.join(HERE, "build_ref.sh"), str(N), bc, gf] +
+                   [str(g) for g in grid], check=True, stdout=subprocess.DEVNULL)
+    return ref_binary(N, bc, gf, grid)
+
+
+def read_config(path: str, V: int, N: int):
+    """Reference configuration file: V*4 series + (N+1) complex plaquette."""
+    raw = np.fromfile(path, dtype=np.float64)
+    nl = V * 4 * series_len(N)
+    assert raw.size == nl + 2 * (N + 1), (raw.size, nl)
+    return raw[:nl].reshape(V, 4, series_len(N)), raw[nl:].reshape(N + 1, 2)
+
+
+def write_config(path: str, links: np.ndarray, plaq: np.ndarray):
+    with open(path, "wb") as f:
+        np.ascontiguousarray(links, dtype=np.float64).tofile(f)
+        np.ascontiguousarray(plaq, dtype=np.float64).tofile(f)
+
+
+def run_reference(binary: str, L, steps: int, dt: float, alpha: float, seed: int,
+                  workdir: str, start: str = "cold", noise: bool = True,
+                  twist_init: bool = False, project: bool = False, timing: bool = False):
+    """Run the reference harness; returns dict of parsed outputs."""
+    out = os.path.join(workdir, "ref")
+    cmd = [binary, "--L", *[str(x) for x in L], "--steps", str(steps), "--dt", repr(dt),
+           "--alpha", repr(alpha), "--seed", str(seed), "--start", start, "--out", out]
+    if noise:
+        cmd += ["--noise", out + ".noise"]
+    if twist_init:
+        cmd.append("--twist-init")
+    if project:
+        cmd.append("--project")
+    if timing:
+        cmd.append("--time")
+    p = subprocess.run(cmd, check=True, capture_output=True, text=True)
+    V = int(np.prod(L))
+    res = {"stdout": p.stdout}
+    N = None
+    plaq = np.loadtxt(out + ".plaq").reshape(steps, -1, 2)
+    N = plaq.shape[1] - 1
+    res["plaq"] = plaq
+    res["norm"] = np.loadtxt(out + ".nor").reshape(steps, N)
+    res["tru"] = np.loadtxt(out + ".tru").reshape(steps, N, 4, 2).transpose(0, 2, 1, 3)
+    res["plaq0"] = np.loadtxt(out + ".plaq0").reshape(N + 1, 2)
+    res["links"], res["plaq_final"] = read_config(out + ".dat", V, N)
+    if noise:
+        res["noise"] = np.fromfile(out + ".noise", dtype=np.float64).reshape(steps, V * 4 * 8)
+    return res
