@@ -1,0 +1,338 @@
+#!/usr/bin/env python
+"""Benchmark: Langevin sweeps/s of quenched SU(3) NSPT on B200.
+
+Workload (default): 32^4 lattice, 24 perturbative orders, FP64 complex 3x3
+series links (~14.5 GB per field), twisted boundary conditions in y and z,
+Euler dt = 0.005, plain Jacobi Langevin sweep (no gauge fixing in the timed
+step), noise from the device Philox generator, field resident in HBM.
+
+One step = one full sweep over all 4 V links.  `value` is whole-job sweeps/s
+(sum over replicas: every rank runs its own independent lattice, so scaling is
+weak, "replicas only").  `e2e` is the same metric through the public C ABI
+with the configuration on the host: upload, K sweeps each reading the
+plaquette / norm / trU back, download -- host<->device copies inside the
+timed region.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Langevin sweeps/s at 32^4 x 24 orders (FP64, twisted y,z)"
+
+
+def canonical_flops_per_link(N: int) -> float:
+    """14 series products + 1 series exp per link update; a 3x3 complex
+    multiply-accumulate is 216 flops; a truncated product of N-order series
+    is N(N-1)/2 of them, the pruned exp C(N+1,3)."""
+    P = N * (N - 1) // 2
+    E = (N - 1) * N * (N + 1) // 6
+    return (14 * P + E) * 216.0
+
+
+def algorithmic_bytes_per_sweep(V: int, N: int) -> float:
+    """Read U and write U' once (order-0 flags not counted)."""
+    return 2.0 * 4 * V * 9 * N * 16
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9:
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    mx = max(mx, float(p[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, p[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        except OSError:
+            pass
+        finally:
+            if self.path and os.path.exists(self.path):
+                os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def read_profile_traffic():
+    """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "sweep_32x4_n24_traffic.txt")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return float(line.split(":", 1)[1])
+    except OSError:
+        pass
+    return None
+
+
+def cpu_reference_sample(N: int, L_sample, steps: int, threads_cap: int | None = None):
+    """Time the reference's own code (oracle/_ref) on a bounded sample with the
+    largest OpenMP grid the sample and the host allow; returns (seconds per
+    sweep, threads, kind, sample description)."""
+    from oracle import oracle as O
+    ncpu = os.cpu_count() or 1
+    if threads_cap:
+        ncpu = min(ncpu, threads_cap)
+    grids = [(1, 1, 1), (2, 1, 1), (2, 2, 1), (2, 2, 2), (4, 2, 2), (4, 4, 2), (4, 4, 4)]
+    best = (1, 1, 1)
+    for gr in grids:
+        n = gr[0] * gr[1] * gr[2]
+        if n <= ncpu and all(L_sample[d + 1] // gr[d] >= 2 for d in range(3)):
+            best = gr
+    binary = O.ref_binary(N, "tw", "local", best)
+    if not os.path.exists(binary):
+        try:
+            binary = O.build_reference(N, "tw", "local", best)
+        except Exception:
+            binary = None
+    if binary and os.path.exists(binary):
+        with tempfile.TemporaryDirectory() as d:
+            r = O.run_reference(binary, L_sample, steps, 0.005, 0.0, 1, d, noise=False,
+                                timing=True)
+        tok = r["stdout"].split()
+        spp = float(tok[tok.index("seconds_per_sweep") + 1])
+        return spp, best[0] * best[1] * best[2], "reference", binary
+    # the reference binary cannot be built here: time the oracle port
+    o = O.Oracle(L_sample, N, twist_mask=6)
+    rng = O.Rand55(1)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.sweep(0.005, rng.gauss(o.V * 32))
+    spp = (time.perf_counter() - t0) / steps
+    return spp, ncpu, "port", "oracle/liboracle.so"
+
+
+def run_reference_arm(args, world, rank):
+    L = tuple(args.L)
+    V = 1
+    for x in L:
+        V *= x
+    if rank != 0:
+        return
+    L_sample = (8, 8, 8, 8)
+    Vs = 8 ** 4
+    per = []
+    kind = threads = None
+    for _ in range(args.steps):
+        spp, threads, kind, _b = cpu_reference_sample(args.N, L_sample, 1)
+        per.append(spp)
+    spp = statistics.median(per)
+    spp_full = spp * V / Vs  # cost is exactly linear in V at fixed N
+    value = 1.0 / spp_full
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "sweeps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": spp_full * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (cold start)",
+        "config": {"workload": "sweep_32^4_N24_twisted_yz", "L": list(L), "N": args.N,
+                   "dt": 0.005, "bc": "twisted y,z", "update": "Jacobi"},
+        "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": threads, "kind": kind,
+                         "sample": "%d sweep(s) of 8^4 x %d orders per step, scaled by V to 32^4"
+                                   % (1, args.N)},
+        "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import numpy as np
+    import torch
+
+    import prlgt2020_b200 as P
+    from prlgt2020_b200 import _lib
+
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py: no CUDA device")
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    L = tuple(args.L)
+    N = args.N
+    V = int(np.prod(L))
+    lib = _lib.load()
+    peak = P.fp64_peak_tflops()
+
+    eng = P.NsptEngine(L, N, twist="yz")
+    eng.seed(1000 + rank, 0)
+    eng.cold_start()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    # warm-up sweeps (also move the field away from the cold start)
+    eng.NsptEvolve(args.dt, args.warmup, 0)
+    barrier()
+    with ClockSampler(local) as clk:
+        eng.NsptEvolve(args.dt, args.steps, 0)
+        ms = eng.last_step_ms()
+    barrier()
+    clocks = clk.summary()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    ms_step = ms_max / args.steps
+    value = world * args.steps / (ms_max * 1e-3)
+
+    # roofline of the dominant kernel (the sweep): canonical flops / sweep time
+    flops = canonical_flops_per_link(N) * 4 * V
+    achieved = flops / (ms_step * 1e-3) / 1e12
+
+    # end to end through the C ABI with the configuration on the host
+    host = torch.empty((V * 4 * P.series_len(N),), dtype=torch.float64, pin_memory=True)
+    eng.cold_start()
+    obs_p = np.zeros((N + 1, 2))
+    obs_n = np.zeros(N)
+    obs_t = np.zeros((4, N, 2))
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    host_ptr = host.data_ptr()
+    h = eng._h
+    barrier()
+    t0 = time.perf_counter()
+    _lib.check(lib.nspt_download_links(h, ctypes.c_void_p(host_ptr), N), "download")
+    t1 = time.perf_counter()
+    e2e_steps = args.steps
+    _lib.check(lib.nspt_upload_links(h, ctypes.c_void_p(host_ptr), N), "upload")
+    for _ in range(e2e_steps):
+        _lib.check(lib.nspt_step(h, args.dt, 1, 0), "step")
+        _lib.check(lib.nspt_observables(h, dp(obs_p), dp(obs_n), dp(obs_t)), "observables")
+    _lib.check(lib.nspt_download_links(h, ctypes.c_void_p(host_ptr), N), "download")
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    e2e_s = t2 - t1
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps / float(te.item())
+    field_bytes = V * 4 * P.series_len(N) * 8
+    obs_bytes = obs_p.nbytes + obs_n.nbytes + obs_t.nbytes
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        spp, threads, kind, _b = cpu_reference_sample(N, (8, 8, 8, 8), 1)
+        cpu = {"value": 1.0 / (spp * V / 8 ** 4), "unit": "sweeps/s", "cores": threads,
+               "kind": kind,
+               "sample": "1 sweep of 8^4 x %d orders (twisted y,z), scaled by V to 32^4" % N}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "sweeps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (cold start, device Philox noise)",
+            "config": {"workload": "sweep_32^4_N24_twisted_yz", "L": list(L), "N": N,
+                       "dt": args.dt, "bc": "twisted y,z", "update": "Jacobi",
+                       "gauge_fixing": "none in the timed sweep",
+                       "l2": "inputs larger than L2 (field %.1f GB)" % (field_bytes / 1e9),
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": read_profile_traffic(),
+                         "peak_source": "FP64 FMA microbenchmark on this GPU "
+                                        "(nspt_measure_fp64_peak); MEASURED_PEAKS.json has no FP64 entry",
+                         "flops_per_sweep": flops,
+                         "algorithmic_bytes_per_sweep": algorithmic_bytes_per_sweep(V, N),
+                         "hbm_gbs_equiv": algorithmic_bytes_per_sweep(V, N) / (ms_step * 1e-3) / 1e9},
+            "clocks": clocks,
+            "e2e": {"value": e2e_value, "unit": "sweeps/s",
+                    "h2d_bytes_per_step": (field_bytes + 0) / e2e_steps,
+                    "d2h_bytes_per_step": field_bytes / e2e_steps + obs_bytes,
+                    "note": "upload + %d x (sweep + observables read-back) + download" % e2e_steps},
+            "gpu_launches": 4 * args.steps,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--L", type=int, nargs=4, default=[32, 32, 32, 32])
+    ap.add_argument("--N", type=int, default=24)
+    ap.add_argument("--dt", type=float, default=0.005)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        return
+    run_ours(args, world, rank, local)
+
+
+if __name__ == "__main__":
+    main()

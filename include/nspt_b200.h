@@ -1,0 +1,127 @@
+/*
+ * nspt_b200.h -- C ABI of the B200 NSPT Langevin engine.
+ *
+ * The reference (PRlgt2020) has no FFI layer: its hot path is the C++
+ * function set of nspt.h:55-94, operating on a ptGluon_fld plus file-scope
+ * globals (defined in Quenched.cc:42-81).  This header is the drop-in
+ * boundary a host driver calls instead; every entry point names the
+ * reference function it replaces.  No torch or CUDA types cross it: plain
+ * pointers, sizes and int status codes (0 = success, as Quenched.cc:776 and
+ * the reference's load/save helpers, QCDenvNODEpt_test.h:359-374).
+ *
+ * Field layout on the host side is the reference's own (ptGluon,
+ * QCDpt.h:249-252; ptSU3, QCDpt.h:42-50): site-major (t fastest,
+ * lattice.h:37), then mu = 0..3, then one series of 1 + 9*allocORD complex
+ * doubles {flag, order 1 [3x3 row major], ..., order allocORD}.  On the
+ * device the engine keeps structure-of-arrays planes (mu, order, colour
+ * component, site) of complex doubles.
+ *
+ * Threading: one context per host thread; each context owns one CUDA stream
+ * and all of its device memory.  Calls are synchronous unless noted.
+ */
+#ifndef NSPT_B200_H
+#define NSPT_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define NSPT_OK 0
+#define NSPT_ERR_ARG 1       /* invalid argument */
+#define NSPT_ERR_ORDER 2     /* perturbative order outside [1, NSPT_MAX_ORDER] */
+#define NSPT_ERR_NOMEM 3     /* device or host allocation failed */
+#define NSPT_ERR_CUDA 4      /* CUDA runtime error */
+#define NSPT_ERR_NODEVICE 5  /* no CUDA device */
+#define NSPT_ERR_STATE 6     /* call out of sequence (e.g. no noise set) */
+#define NSPT_ERR_IO 7        /* file I/O error */
+
+#define NSPT_MAX_ORDER 48
+
+/* ---- nspt_create flags (choices.h:42-89 as run-time options) ---- */
+#define NSPT_TWIST_Y (1u << 1)   /* twisted y boundary (choices.h:47) */
+#define NSPT_TWIST_Z (1u << 2)   /* twisted z boundary (choices.h:48) */
+#define NSPT_TWIST_T (1u << 3)   /* twisted t boundary (choices.h:49) */
+#define NSPT_ZEROMODE (1u << 4)  /* REMOVE_GLUON_ZEROMOM (choices.h:82-84) */
+#define NSPT_GF_FA (1u << 5)     /* Fourier-accelerated gauge fixing */
+
+typedef struct nspt_ctx nspt_ctx;
+
+/* Create a context for an L[0] x L[1] x L[2] x L[3] lattice (lattice.h:139)
+ * with N perturbative orders (PTORD; allocORD == N on the device).
+ * alpha is the gauge-fixing parameter act_pars.alpha (input.h:58).
+ * Allocates both link fields (Jacobi update) on the current device. */
+int nspt_create(const int L[4], int N, unsigned flags, double alpha,
+                nspt_ctx **out);
+int nspt_destroy(nspt_ctx *ctx);
+const char *nspt_error_string(int code);
+const char *nspt_last_error(nspt_ctx *ctx);
+
+/* Device and memory footprint of a context (bytes). */
+size_t nspt_device_bytes(const nspt_ctx *ctx);
+
+/* Replace ptGluon_fld::load / save (QCDenvNODEpt_test.h:342-374):
+ * copy a host field in the reference's AoS layout (allocORD orders per
+ * series, allocORD >= N; orders above N are ignored on upload and written
+ * as zero on download). */
+int nspt_upload_links(nspt_ctx *ctx, const void *aos, int allocORD);
+int nspt_download_links(nspt_ctx *ctx, void *aos, int allocORD);
+/* Cold start, Quenched.cc:596-603 (flag 1, all orders zero). */
+int nspt_cold_start(nspt_ctx *ctx);
+
+/* Noise.  Either inject the 8 Gaussians SU3rand draws per link
+ * (MyMath.cc:256-292) for the next sweep -- eta[V][4][8], site-major as
+ * the reference draws them (nspt.cc:365-423) -- or seed the device
+ * counter-based generator (Philox-4x32-10) used when nothing is injected.
+ * Injected noise is consumed by exactly one sweep. */
+int nspt_set_noise(nspt_ctx *ctx, const double *eta);
+int nspt_seed(nspt_ctx *ctx, uint64_t seed, uint64_t counter);
+
+/* NsptEvolve (nspt.cc:953-1039) with Beat = nsteps and dt = tau_g of
+ * Quench.cfg (before the /(-2 NC) of Quenched.cc:584-589): per step a
+ * Jacobi Langevin sweep, then the zero-mode subtraction and the gauge
+ * fixing selected at creation.  Twisted boundaries are applied on the fly
+ * (no copy sites), so twist_boundary (nspt.cc:163-255) has no separate
+ * call.  gf_every > 1 gauge-fixes only every gf_every-th step (0 = never). */
+int nspt_step(nspt_ctx *ctx, double dt, int nsteps, int gf_every);
+
+/* The three pieces of NsptEvolve, separately:
+ * gauge_wilson (nspt.cc:258-600, Jacobi branch; also accumulates the zero
+ * mode when the context has NSPT_ZEROMODE); zero_modes_subtraction
+ * (nspt.cc:605-654); FAstochastic_gauge_fixing (nspt.cc:866-948). */
+int nspt_gauge_wilson(nspt_ctx *ctx, double dt);
+int nspt_zero_modes_subtraction(nspt_ctx *ctx);
+int nspt_fa_gauge_fixing(nspt_ctx *ctx, double alpha);
+
+/* Observables of the last sweep, normalised as nspt.cc:570-597:
+ * plaq[(N+1)*2] (/72V), norm[N] (/12V), trU[4*N*2] (/3V, mu major).
+ * Any pointer may be NULL. */
+int nspt_observables(nspt_ctx *ctx, double *plaq, double *norm, double *trU);
+
+/* plaquette_measure (nspt.cc:1316-1406): static plaquette of the current
+ * field, plaq[(N+1)*2]. */
+int nspt_plaquette_measure(nspt_ctx *ctx, double *plaq);
+
+/* Configuration files in the reference's binary format
+ * (QCDenvNODEpt_test.h:359-374: field, then (allocORD+1) complex plaquette).
+ * save writes plaquette_measure of the current field as the trailer. */
+int nspt_save_config(nspt_ctx *ctx, const char *path, int allocORD);
+int nspt_load_config(nspt_ctx *ctx, const char *path, int allocORD,
+                     double *plaq_trailer);
+
+/* Wall time of the last nspt_step / sweep call on the device (CUDA events on
+ * the context's stream), milliseconds. */
+double nspt_last_step_ms(const nspt_ctx *ctx);
+
+/* Measured FP64 FMA throughput of the current device (independent FMA
+ * chains on every SM), TFLOP/s.  Roofline denominator for the sweep. */
+int nspt_measure_fp64_peak(double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NSPT_B200_H */

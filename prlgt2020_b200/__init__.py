@@ -1,0 +1,254 @@
+"""prlgt2020_b200 -- B200 NSPT Langevin engine behind the reference's API.
+
+Host-side mirror of the PRlgt2020 hot path (nspt.h:55-94): the names and the
+argument meaning follow the reference, the work runs in the CUDA engine
+(libnspt_b200.so, C ABI in include/nspt_b200.h).  There is no CPU fallback:
+without the built library or a CUDA device every compute call raises.
+
+    eng = NsptEngine((4, 4, 4, 4), N=8, zero_modes=True)
+    eng.cold_start()
+    obs = eng.gauge_wilson(dt=0.01)        # one Jacobi sweep
+    eng.zero_modes_subtraction()
+    plaq = eng.plaquette_measure()
+
+Field data on the host use the reference's AoS layout (ptGluon_fld,
+QCDenvNODEpt_test.h:331-338): shape (V, 4, 2 + 18*allocORD) float64 =
+site (t fastest), mu, {flag re/im, order 1 [3x3 row major re/im], ...}.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import (NSPT_GF_FA, NSPT_TWIST_T, NSPT_TWIST_Y, NSPT_TWIST_Z, NSPT_ZEROMODE,
+                   NsptError, build as build_library, check, load as load_library)
+
+__all__ = ["NsptEngine", "ptGluon_fld", "SweepObservables", "build", "series_len",
+           "NsptError", "fp64_peak_tflops"]
+
+_DIRS = {"x": 0, "y": 1, "z": 2, "t": 3}
+
+
+def build(verbose: bool = False) -> str:
+    return build_library(verbose)
+
+
+def series_len(allocORD: int) -> int:
+    """Doubles in one ptSU3 (QCDpt.h:47-48): flag + allocORD 3x3 complex."""
+    return 2 + 18 * int(allocORD)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+@dataclass
+class SweepObservables:
+    """Per-sweep output of gauge_wilson (nspt.cc:570-597)."""
+    plaq: np.ndarray  # (N+1, 2): Tr(U * staples) / 72V per order (re, im)
+    norm: np.ndarray  # (N,):     Re Tr(U_k U_k^dag) / 12V
+    tru: np.ndarray   # (4, N, 2): Tr U_k / 3V per mu
+
+
+class ptGluon_fld:
+    """Host gauge field in the reference's layout and file format.
+
+    Mirrors ptGluon_fld (QCDenvNODEpt_test.h:331-426): `links` is
+    (V, 4, 2 + 18*allocORD) float64; save/load use the binary format of
+    ptGluon_fld::save(char*, Cplx*) -- the field then (allocORD+1) complex
+    plaquette values -- and load checks the byte count like io::load.
+    """
+
+    def __init__(self, L, allocORD: int, links: np.ndarray | None = None):
+        self.L = tuple(int(x) for x in L)
+        self.allocORD = int(allocORD)
+        self.V = int(np.prod(self.L))
+        shape = (self.V, 4, series_len(self.allocORD))
+        if links is None:
+            self.links = np.zeros(shape)
+            self.links[:, :, 0] = 1.0  # cold start: flag = VACUUM = 1
+        else:
+            self.links = np.ascontiguousarray(links, dtype=np.float64).reshape(shape)
+
+    def id(self):
+        """Cold configuration (ptSU3::id, QCDpt.h:69-72)."""
+        self.links[...] = 0.0
+        self.links[:, :, 0] = 1.0
+
+    def save(self, path: str, plaquette: np.ndarray | None = None):
+        trailer = np.zeros((self.allocORD + 1, 2))
+        if plaquette is not None:
+            p = np.asarray(plaquette, dtype=np.float64).reshape(-1, 2)
+            trailer[: p.shape[0]] = p
+        with open(path, "wb") as f:
+            self.links.tofile(f)
+            trailer.tofile(f)
+
+    @classmethod
+    def load(cls, path: str, L, allocORD: int):
+        V = int(np.prod(L))
+        n = V * 4 * series_len(allocORD)
+        want = 8 * (n + 2 * (allocORD + 1))
+        size = os.path.getsize(path)
+        if size != want:
+            raise IOError("%s: %d bytes, expected %d for L=%s allocORD=%d"
+                          % (path, size, want, tuple(L), allocORD))
+        raw = np.fromfile(path, dtype=np.float64)
+        fld = cls(L, allocORD, raw[:n])
+        fld.plaquette_trailer = raw[n:].reshape(allocORD + 1, 2)
+        return fld
+
+
+def fp64_peak_tflops() -> float:
+    """Measured FP64 FMA throughput of the current device (TFLOP/s)."""
+    out = ctypes.c_double(0.0)
+    check(load_library().nspt_measure_fp64_peak(ctypes.byref(out)), "nspt_measure_fp64_peak")
+    return out.value
+
+
+class NsptEngine:
+    """One lattice on the current CUDA device (a context of the C ABI).
+
+    L           lattice extents (x, y, z, t), lattice.h:139
+    N           perturbative order PTORD (device allocORD == N)
+    twist       twisted directions, subset of "yzt" (choices.h:45-50)
+    zero_modes  REMOVE_GLUON_ZEROMOM (choices.h:82-84), periodic only
+    fa          Fourier-accelerated Landau gauge fixing (nspt.cc:866-948)
+    alpha       act_pars.alpha as in Quench.cfg (negative in the reference
+                config; FA multiplies by -alpha/p^2)
+    """
+
+    def __init__(self, L, N: int, twist: str = "", zero_modes: bool = False, fa: bool = False,
+                 alpha: float = 0.0):
+        lib = load_library()
+        self.L = tuple(int(x) for x in L)
+        if len(self.L) != 4:
+            raise ValueError("L must have 4 extents")
+        self.N = int(N)
+        self.V = int(np.prod(self.L))
+        flags = 0
+        for d in twist:
+            flags |= {"y": NSPT_TWIST_Y, "z": NSPT_TWIST_Z, "t": NSPT_TWIST_T}[d]
+        if zero_modes:
+            flags |= NSPT_ZEROMODE
+        if fa:
+            flags |= NSPT_GF_FA
+        self.flags = flags
+        self.alpha = float(alpha)
+        arr = (ctypes.c_int * 4)(*self.L)
+        h = ctypes.c_void_p()
+        check(lib.nspt_create(arr, self.N, flags, self.alpha, ctypes.byref(h)), "nspt_create")
+        self._h = h
+
+    # -- lifetime -------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().nspt_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, code, where):
+        check(code, where, self._h)
+
+    @property
+    def device_bytes(self) -> int:
+        return int(load_library().nspt_device_bytes(self._h))
+
+    # -- field transfer -------------------------------------------------
+    def cold_start(self):
+        self._check(load_library().nspt_cold_start(self._h), "nspt_cold_start")
+
+    def upload(self, links, allocORD: int | None = None):
+        """Copy a host field (reference AoS layout) to the device."""
+        if isinstance(links, ptGluon_fld):
+            allocORD, links = links.allocORD, links.links
+        A = self.N if allocORD is None else int(allocORD)
+        a = np.ascontiguousarray(links, dtype=np.float64)
+        if a.size != self.V * 4 * series_len(A):
+            raise ValueError("field has %d doubles, expected %d" % (a.size, self.V * 4 * series_len(A)))
+        self._check(load_library().nspt_upload_links(self._h, a.ctypes.data, A), "nspt_upload_links")
+
+    def download(self, allocORD: int | None = None) -> np.ndarray:
+        A = self.N if allocORD is None else int(allocORD)
+        out = np.empty((self.V, 4, series_len(A)))
+        self._check(load_library().nspt_download_links(self._h, out.ctypes.data, A),
+                    "nspt_download_links")
+        return out
+
+    def save(self, path: str, allocORD: int | None = None):
+        A = self.N if allocORD is None else int(allocORD)
+        self._check(load_library().nspt_save_config(self._h, path.encode(), A), "nspt_save_config")
+
+    def load(self, path: str, allocORD: int | None = None) -> np.ndarray:
+        A = self.N if allocORD is None else int(allocORD)
+        trailer = np.zeros((A + 1, 2))
+        self._check(load_library().nspt_load_config(self._h, path.encode(), A, _dp(trailer)),
+                    "nspt_load_config")
+        return trailer
+
+    # -- noise ------------------------------------------------------------
+    def set_noise(self, eta: np.ndarray):
+        """Inject the 8 Gaussians per link SU3rand draws (V, 4, 8) for the next sweep."""
+        a = np.ascontiguousarray(eta, dtype=np.float64)
+        if a.size != self.V * 32:
+            raise ValueError("noise needs V*4*8 values")
+        self._check(load_library().nspt_set_noise(self._h, _dp(a)), "nspt_set_noise")
+
+    def seed(self, seed: int, counter: int = 0):
+        self._check(load_library().nspt_seed(self._h, int(seed), int(counter)), "nspt_seed")
+
+    # -- the reference's hot-path functions (nspt.h:55-94) -----------------
+    def gauge_wilson(self, dt: float) -> SweepObservables:
+        """One Jacobi Langevin sweep (nspt.cc:258-600); dt = tau_g of Quench.cfg."""
+        self._check(load_library().nspt_gauge_wilson(self._h, float(dt)), "nspt_gauge_wilson")
+        return self.observables()
+
+    def zero_modes_subtraction(self):
+        self._check(load_library().nspt_zero_modes_subtraction(self._h),
+                    "nspt_zero_modes_subtraction")
+
+    def FAstochastic_gauge_fixing(self, alpha: float | None = None):
+        a = self.alpha if alpha is None else float(alpha)
+        self._check(load_library().nspt_fa_gauge_fixing(self._h, a), "nspt_fa_gauge_fixing")
+
+    def twist_boundary(self):
+        """No-op: twisted boundaries are applied inside every neighbour read,
+        so there are no copy sites to refresh (nspt.cc:163-255)."""
+
+    def NsptEvolve(self, dt: float, beat: int = 1, gf_every: int = 1):
+        """Beat Langevin steps (nspt.cc:953-1039)."""
+        self._check(load_library().nspt_step(self._h, float(dt), int(beat), int(gf_every)),
+                    "nspt_step")
+
+    def plaquette_measure(self) -> np.ndarray:
+        out = np.zeros((self.N + 1, 2))
+        self._check(load_library().nspt_plaquette_measure(self._h, _dp(out)),
+                    "nspt_plaquette_measure")
+        return out
+
+    def observables(self) -> SweepObservables:
+        N = self.N
+        plaq = np.zeros((N + 1, 2))
+        norm = np.zeros(N)
+        tru = np.zeros((4, N, 2))
+        self._check(load_library().nspt_observables(self._h, _dp(plaq), _dp(norm), _dp(tru)),
+                    "nspt_observables")
+        return SweepObservables(plaq, norm, tru)
+
+    def last_step_ms(self) -> float:
+        return float(load_library().nspt_last_step_ms(self._h))

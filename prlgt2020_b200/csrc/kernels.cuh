@@ -1,0 +1,710 @@
+// kernels.cuh -- the NSPT Langevin kernels for sm_100a (FP64).
+//
+// Device layout of a link field (structure of arrays, row major colour):
+//   U[((mu*9*N + 9*(k-1) + 3*r + c) * V + site]   double2, order k = 1..N
+//   Uf[mu*V + site]                               double2 flag (order 0)
+// site = lexicographic index with t fastest (GETINDEX, lattice.h:37).
+// Consecutive sites of one (mu, order, component) plane are contiguous.
+//
+// Every link update is done by one 9-lane "link group" (series.cuh); a warp
+// holds 3 groups (lanes 0-26) working on 3 consecutive sites of one mu, each
+// group with up to 3 shared-memory series slots.  Groups are independent:
+// only group-local __syncwarp is used, never a block barrier.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "series.cuh"
+
+namespace nspt {
+
+constexpr int GROUP = 9;  // lanes per link group
+constexpr int LPW = 3;    // link groups per warp
+constexpr int MO = 8;     // result orders per lane per pass (3*MO orders)
+
+struct Geo {
+  int L[4];
+  int V;
+  int s0, s1, s2;  // site strides of directions 0, 1, 2 (direction 3: 1)
+  unsigned twist;  // bit d: direction d twisted
+};
+
+// Lattice momenta p2hat[d][n] = 4 sin^2(pi n / L_d)  (lattice.h:1144-1169).
+__constant__ double c_p2hat[4][128];
+// exp(-2 pi i k / 64), k < 64, radix-2 FFT twiddles.
+__constant__ double2 c_tw64[64];
+
+__device__ __forceinline__ void coords(const Geo &g, int site, int *x) {
+  x[0] = site / g.s0;
+  int r = site - x[0] * g.s0;
+  x[1] = r / g.s1;
+  r -= x[1] * g.s1;
+  x[2] = r / g.s2;
+  x[3] = r - x[2] * g.s2;
+}
+
+struct Nb {
+  int site;
+  unsigned fwd, bwd;  // directions wrapped forward / backward
+};
+
+// Site of x + s1*e_d1 + s2*e_d2 (s = -1, 0, +1) with periodic wrap.
+__device__ __forceinline__ Nb neighbour(const Geo &g, const int *x, int d1, int s1, int d2 = 0,
+                                        int s2 = 0) {
+  int y[4] = {x[0], x[1], x[2], x[3]};
+  y[d1] += s1;
+  y[d2] += s2;
+  Nb n;
+  n.fwd = 0;
+  n.bwd = 0;
+#pragma unroll
+  for (int d = 0; d < 4; d++) {
+    if (y[d] < 0) {
+      y[d] += g.L[d];
+      n.bwd |= 1u << d;
+    } else if (y[d] >= g.L[d]) {
+      y[d] -= g.L[d];
+      n.fwd |= 1u << d;
+    }
+  }
+  n.site = y[0] * g.s0 + y[1] * g.s1 + y[2] * g.s2 + y[3];
+  return n;
+}
+
+// Copy link (mu, n.site) from the row-major planes into a column-major slot
+// (DAG: store its dagger), applying the twists of the faces the read crossed.
+// Twisted links get flag 1 (twist_* returns a default flag, nspt.cc:115-121).
+__device__ __forceinline__ void stage(double2 *slot, const double2 *__restrict__ U,
+                                      const double2 *__restrict__ Uf, int mu, Nb n,
+                                      const Geo &g, int N, const Lane &L, bool dag = false) {
+  const size_t V = (size_t)g.V;
+  const double2 *src = U + (size_t)mu * 9 * N * V + n.site;
+  const unsigned tb = n.bwd & g.twist, tf = n.fwd & g.twist;
+  if (!(tb | tf)) {
+    // lane j copies colour component j (= 3r + c) of every order
+    const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
+    const int off = dag ? 3 * r + c : 3 * c + r;
+    for (int k = 1; k <= N; k++) {
+      const double2 v = __ldg(src + (size_t)(9 * (k - 1) + L.j) * V);
+      slot[1 + 9 * (k - 1) + off] = dag ? cconj(v) : v;
+    }
+    if (L.j == 0) {
+      const double2 f = __ldg(Uf + (size_t)mu * V + n.site);
+      slot[0] = dag ? cconj(f) : f;
+    }
+  } else {
+    for (int k = 1 + L.j; k <= N; k += GROUP) {
+      double2 m[9];
+#pragma unroll
+      for (int e = 0; e < 9; e++) m[e] = __ldg(src + (size_t)(9 * (k - 1) + e) * V);
+      twist3(m, tb, tf);
+      double2 *p = slot + 1 + 9 * (k - 1);
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) p[dag ? 3 * r + c : 3 * c + r] = dag ? cconj(m[3 * r + c]) : m[3 * r + c];
+    }
+    if (L.j == 0) slot[0] = make_double2(1.0, 0.0);
+  }
+  __syncwarp(L.mask);
+}
+
+// Copy a per-site series (planes src[e*V + site], row major) into a slot.
+__device__ __forceinline__ void stage_site(double2 *slot, const double2 *__restrict__ src, int site,
+                                           size_t V, int N, const Lane &L, double2 flag,
+                                           bool dag = false) {
+  const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
+  const int off = dag ? 3 * r + c : 3 * c + r;
+  for (int k = 1; k <= N; k++) {
+    const double2 v = __ldg(src + (size_t)(9 * (k - 1) + L.j) * V + site);
+    slot[1 + 9 * (k - 1) + off] = dag ? cconj(v) : v;
+  }
+  if (L.j == 0) slot[0] = dag ? cconj(flag) : flag;
+  __syncwarp(L.mask);
+}
+
+// Flag of link (mu, n): 1 after a twist, else the stored flag.
+__device__ __forceinline__ double2 link_flag(const double2 *Uf, int mu, Nb n, const Geo &g) {
+  if ((n.bwd | n.fwd) & g.twist) return make_double2(1.0, 0.0);
+  return __ldg(Uf + (size_t)mu * g.V + n.site);
+}
+
+// ---------------- Philox-4x32-10 (Salmon et al., SC'11) ----------------
+__device__ __forceinline__ uint4 philox(uint4 c, uint2 k) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    if (r) {
+      k.x += 0x9E3779B9u;
+      k.y += 0xBB67AE85u;
+    }
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
+    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
+  }
+  return c;
+}
+// uniform in (0, 1] with 53 random bits
+__device__ __forceinline__ double u53(uint32_t hi, uint32_t lo) {
+  const uint64_t b = ((((uint64_t)hi) << 32) | lo) >> 11;
+  return ((double)b + 1.0) * (1.0 / 9007199254740992.0);
+}
+// 8 Gaussians of variance 1/2 (the reference's convention, MyRand.cc:119-127)
+__device__ __forceinline__ void philox_gauss8(uint64_t seed, uint64_t step, uint32_t link,
+                                              double *g) {
+  const uint2 key = make_uint2((uint32_t)seed, (uint32_t)(seed >> 32));
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    uint4 r = philox(make_uint4(link, (uint32_t)q, (uint32_t)step, (uint32_t)(step >> 32)), key);
+    const double u1 = u53(r.x, r.y), u2 = u53(r.z, r.w);
+    const double rad = sqrt(-log(u1));
+    double sn, cs;
+    sincospi(2.0 * u2, &sn, &cs);
+    g[2 * q] = rad * cs;
+    g[2 * q + 1] = rad * sn;
+  }
+}
+
+// SU3rand mapping of 8 Gaussians to a row-major 3x3, MyMath.cc:256-292.
+__device__ __forceinline__ void su3rand(const double *g, double2 *P) {
+  const double sD3 = 0.57735026918962573;  // sqrt(1/3), MyMath.h:49
+#pragma unroll
+  for (int e = 0; e < 9; e++) P[e] = cz();
+  P[1] = make_double2(g[1], g[0]);
+  P[3] = make_double2(-g[1], g[0]);
+  P[2] = make_double2(g[3], g[2]);
+  P[6] = make_double2(-g[3], g[2]);
+  P[5] = make_double2(g[5], g[4]);
+  P[7] = make_double2(-g[5], g[4]);
+  const double gg = g[7] * sD3;
+  P[0] = make_double2(0.0, gg + g[6]);
+  P[4] = make_double2(0.0, gg - g[6]);
+  P[8] = make_double2(0.0, -2. * gg);
+}
+
+struct SweepArgs {
+  const double2 *U, *Uf;
+  double2 *F, *Ff;
+  double2 *Lg;         // log(U') per link (zero modes) or null
+  double2 *obs_tr;     // [(N+1)][4V] Tr(U * staples) per order
+  double *obs_norm;    // [N][4V]     Re Tr(U_k U_k^dag)
+  double2 *obs_tru;    // [N][4V]     Tr U_k
+  const double *noise; // [V][4][8] injected, or null (Philox)
+  uint64_t seed, step;
+  double tau_g, stau;  // -dt/6, sqrt(dt)  (Quenched.cc:584-589)
+  int N, SS;
+  Geo g;
+};
+
+// Lane identity; lanes 27..31 of a warp have no group.
+__device__ __forceinline__ bool make_lane(Lane &L, int &g) {
+  const int lane = threadIdx.x & 31;
+  g = lane / GROUP;
+  if (g >= LPW) return false;
+  L.j = lane - g * GROUP;
+  L.c = L.j / 3;
+  L.s = L.j - 3 * L.c;
+  L.mask = ((1u << GROUP) - 1u) << (g * GROUP);
+  return true;
+}
+
+// Unit (link or site) handled by this group; clamps to the last unit.
+__device__ __forceinline__ long group_unit(int g, long nunits, bool &valid) {
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  long u = ((long)blockIdx.x * nw + warp) * LPW + g;
+  valid = u < nunits;
+  return valid ? u : nunits - 1;
+}
+
+// Jacobi Langevin sweep, one link per group: gauge_wilson, nspt.cc:362-439.
+// MEASURE: only the plaquette traces (plaquette_measure, nspt.cc:1362-1383).
+template <bool MEASURE>
+__global__ void __launch_bounds__(256, 1) k_sweep(SweepArgs a) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5;
+  const int N = a.N, SS = a.SS, c = L.c;
+  const size_t V = (size_t)a.g.V;
+  double2 *W = sm + (size_t)(warp * LPW + g) * (3 * SS + RING), *T = W + SS, *Y = T + SS;
+  double2 *ring = Y + SS;
+  bool valid;
+  const long link = group_unit(g, 4L * a.g.V, valid);
+  const int mu = (int)(link / a.g.V);
+  const int site = (int)(link - (long)mu * a.g.V);
+  int x[4];
+  coords(a.g, site, x);
+  const size_t plane_mu = (size_t)9 * N * V;
+  const unsigned tw = a.g.twist;
+
+  double2 wflag = cz();
+  bool first = true;
+  for (int nu = 0; nu < 4; nu++) {
+    if (nu == mu) continue;
+    // ---- upper staple U_nu(x+mu) [U_nu(x) U_mu(x+nu)]^dag (QCDenvNODEpt_test.h:555)
+    {
+      const Nb b = neighbour(a.g, x, nu, 1);
+      stage(Y, a.U, a.Uf, mu, b, a.g, N, L);
+      const double2 a0 = __ldg(a.Uf + (size_t)nu * V + site);
+      const LeftG A{a.U + nu * plane_mu + site, V, 0u, 0u, ring};
+      // T holds dag(U_nu(x) U_mu(x+nu))
+      product<MO, false>(A, a0, Y, Y[0], N, L,
+                         [&](int k, int r, double2 v) { T[sidx(k, c, r)] = cconj(v); });
+      if (L.j == 0) T[0] = cconj(flag_mul(a0, Y[0]));
+      __syncwarp(L.mask);
+    }
+    {
+      const Nb m = neighbour(a.g, x, mu, 1);
+      const double2 a0 = link_flag(a.Uf, nu, m, a.g);
+      const LeftG A{a.U + nu * plane_mu + m.site, V, m.bwd & tw, m.fwd & tw, ring};
+      const double2 b0 = T[0];
+      if (first)
+        product<MO, false>(A, a0, T, b0, N, L, [&](int k, int r, double2 v) { W[sidx(k, r, c)] = v; });
+      else
+        product<MO, false>(A, a0, T, b0, N, L, [&](int k, int r, double2 v) {
+          double2 &w = W[sidx(k, r, c)];
+          w = cadd(w, v);
+        });
+      const double2 f = flag_mul(a0, b0);
+      wflag = first ? f : cadd(wflag, f);
+      first = false;
+    }
+    // ---- lower staple [U_mu(x-nu) U_nu(x-nu+mu)]^dag U_nu(x-nu) (QCDenvNODEpt_test.h:556)
+    {
+      const Nb d = neighbour(a.g, x, nu, -1);
+      const Nb dm = neighbour(a.g, x, nu, -1, mu, 1);
+      stage(Y, a.U, a.Uf, nu, dm, a.g, N, L);
+      const double2 a0 = link_flag(a.Uf, mu, d, a.g);
+      const LeftG A{a.U + mu * plane_mu + d.site, V, d.bwd & tw, d.fwd & tw, ring};
+      product<MO, false>(A, a0, Y, Y[0], N, L,
+                         [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+      if (L.j == 0) T[0] = flag_mul(a0, Y[0]);
+      __syncwarp(L.mask);
+      stage(Y, a.U, a.Uf, nu, d, a.g, N, L);
+      const double2 ta = cconj(T[0]);
+      const LeftS A2{T};
+      product<MO, true>(A2, ta, Y, Y[0], N, L, [&](int k, int r, double2 v) {
+        double2 &w = W[sidx(k, r, c)];
+        w = cadd(w, v);
+      });
+      wflag = cadd(wflag, flag_mul(ta, Y[0]));
+    }
+  }
+  if (L.j == 0) W[0] = wflag;
+  // ---- P = U_mu(x) * staples (nspt.cc:392); U_mu(x) stays in Y for F = exp(.) U
+  {
+    Nb self;
+    self.site = site;
+    self.fwd = self.bwd = 0;
+    stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
+  }
+  const double2 pflag = flag_mul(Y[0], wflag);
+  product<MO, false>(LeftS{Y}, Y[0], W, wflag, N, L,
+                     [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+  if (L.j == 0) T[0] = pflag;
+  __syncwarp(L.mask);
+  // ---- traces (ptSU3::Tr, QCDpt.cc:115-122), norm and Tr U_k (nspt.cc:393-402)
+  if (valid) {
+    const size_t nl4 = 4 * V;
+    if (L.j == 0) a.obs_tr[link] = make_double2(3. * pflag.x, 3. * pflag.y);
+    for (int k = 1 + L.j; k <= N; k += GROUP) {
+      a.obs_tr[(size_t)k * nl4 + link] =
+          cadd(cadd(T[sidx(k, 0, 0)], T[sidx(k, 1, 1)]), T[sidx(k, 2, 2)]);
+      if constexpr (!MEASURE) {
+        double nrm = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          double d = 0.0;
+#pragma unroll
+          for (int l = 0; l < 3; l++) {
+            const double2 u = Y[sidx(k, i, l)];
+            d += u.x * u.x + u.y * u.y;
+          }
+          nrm += d;
+        }
+        a.obs_norm[(size_t)(k - 1) * nl4 + link] = nrm;
+        a.obs_tru[(size_t)(k - 1) * nl4 + link] =
+            cadd(cadd(Y[sidx(k, 0, 0)], Y[sidx(k, 1, 1)]), Y[sidx(k, 2, 2)]);
+      }
+    }
+  }
+  if constexpr (MEASURE) return;
+  __syncwarp(L.mask);
+  // ---- W1 = reH(W1) * tau_g; W1.ptU[0] -= stau * SU3rand  (nspt.cc:416-423)
+  ser_reH(T, N, L);
+  {
+    double gz[8];
+    if (L.j == 0) {
+      if (a.noise) {
+#pragma unroll
+        for (int q = 0; q < 8; q++) gz[q] = __ldg(a.noise + ((size_t)site * 4 + mu) * 8 + q);
+      } else {
+        philox_gauss8(a.seed, a.step, (uint32_t)link, gz);
+      }
+    }
+    for (int k = 1 + L.j; k <= N; k += GROUP) {
+      double2 *p = T + 1 + 9 * (k - 1);
+#pragma unroll
+      for (int e = 0; e < 9; e++) p[e] = cscale(p[e], a.tau_g);
+      if (k == 1) {
+        double2 eta[9];
+        su3rand(gz, eta);
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int q = 0; q < 3; q++) p[3 * q + r] = csub(p[3 * q + r], cscale(eta[3 * r + q], a.stau));
+      }
+    }
+    if (L.j == 0) T[0] = cscale(cz(), a.tau_g);
+    __syncwarp(L.mask);
+  }
+  // ---- F = exp(W1) * U  (nspt.cc:429)
+  ser_exp<MO>(T, W, N, L);
+  const bool zm = a.Lg != nullptr;
+  double2 *Fo = a.F + (size_t)mu * plane_mu + site;
+  product<MO, false>(LeftS{W}, make_double2(1.0, 0.0), Y, Y[0], N, L,
+                     [&](int k, int r, double2 v) {
+                       if (valid) Fo[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
+                       if (zm) T[sidx(k, r, c)] = v;
+                     });
+  if (L.j == 0) {
+    if (valid) a.Ff[(size_t)mu * V + site] = Y[0];
+    T[0] = Y[0];
+  }
+  if (!zm) return;
+  __syncwarp(L.mask);
+  // ---- MM[mu] += log(F[link])  (nspt.cc:432-439): logs stored per link
+  double2 *Lo = a.Lg + (size_t)mu * plane_mu + site;
+  ser_log<MO>(T, W, N, L, [&](int k, int r, double2 v) {
+    if (valid) Lo[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
+  });
+}
+
+// U = exp(reH(log U - MM[mu]/V)) per link: zero_modes_subtraction,
+// nspt.cc:605-654 (log U is the per-link log stored by the sweep).
+__global__ void __launch_bounds__(256, 1)
+    k_zero_modes(double2 *U, double2 *Uf, const double2 *Lg, const double2 *MMs, int N, int SS,
+                 Geo geo) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5;
+  const size_t V = (size_t)geo.V;
+  double2 *P = sm + (size_t)(warp * LPW + g) * 2 * SS, *R = P + SS;
+  bool valid;
+  const long link = group_unit(g, 4L * geo.V, valid);
+  const int mu = (int)(link / geo.V);
+  const int site = (int)(link - (long)mu * geo.V);
+  const double2 *src = Lg + (size_t)mu * 9 * N * V + site;
+  const double2 *mm = MMs + (size_t)mu * 9 * N;
+  {
+    const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
+    for (int k = 1; k <= N; k++) {
+      const int e = 9 * (k - 1) + L.j;
+      P[sidx(k, r, c)] = csub(__ldg(src + (size_t)e * V), mm[e]);
+    }
+  }
+  if (L.j == 0) P[0] = cz();
+  __syncwarp(L.mask);
+  ser_reH(P, N, L);
+  __syncwarp(L.mask);
+  ser_exp<MO>(P, R, N, L);
+  if (!valid) return;
+  double2 *dst = U + (size_t)mu * 9 * N * V + site;
+  const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
+  for (int k = 1; k <= N; k++) dst[(size_t)(9 * (k - 1) + L.j) * V] = R[sidx(k, r, c)];
+  if (L.j == 0) Uf[(size_t)mu * V + site] = make_double2(1.0, 0.0);
+}
+
+// Lg = log(U) per link (the logs FAstochastic_gauge_fixing needs, nspt.cc:874-875).
+__global__ void __launch_bounds__(256, 1)
+    k_log_links(const double2 *U, const double2 *Uf, double2 *Lg, int N, int SS, Geo geo) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5;
+  const size_t V = (size_t)geo.V;
+  double2 *X = sm + (size_t)(warp * LPW + g) * 2 * SS, *Sc = X + SS;
+  bool valid;
+  const long link = group_unit(g, 4L * geo.V, valid);
+  const int mu = (int)(link / geo.V);
+  const int site = (int)(link - (long)mu * geo.V);
+  Nb n;
+  n.site = site;
+  n.fwd = n.bwd = 0;
+  stage(X, U, Uf, mu, n, geo, N, L);
+  double2 *dst = Lg + (size_t)mu * 9 * N * V + site;
+  const int c = L.c;
+  ser_log<MO>(X, Sc, N, L, [&](int k, int r, double2 v) {
+    if (valid) dst[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
+  });
+}
+
+// G(x) = exp(reH(Wg(x) / V))  (nspt.cc:902-906), one group per site.
+__global__ void __launch_bounds__(256, 1)
+    k_fa_gt(const double2 *Wg, double2 *Gx, int N, int SS, Geo geo) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5;
+  const size_t V = (size_t)geo.V;
+  double2 *P = sm + (size_t)(warp * LPW + g) * 2 * SS, *R = P + SS;
+  bool valid;
+  const long site = group_unit(g, geo.V, valid);
+  const double dv = (double)geo.V;
+  const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
+  for (int k = 1; k <= N; k++) {
+    const double2 w = __ldg(Wg + (size_t)(9 * (k - 1) + L.j) * V + site);
+    P[sidx(k, r, c)] = make_double2(w.x / dv, w.y / dv);
+  }
+  if (L.j == 0) P[0] = cz();
+  __syncwarp(L.mask);
+  ser_reH(P, N, L);
+  __syncwarp(L.mask);
+  ser_exp<MO>(P, R, N, L);
+  if (!valid) return;
+  for (int k = 1; k <= N; k++) Gx[(size_t)(9 * (k - 1) + L.j) * V + site] = R[sidx(k, r, c)];
+}
+
+// U_mu(x) <- G(x) U_mu(x) G(x+mu)^dag  (nspt.cc:912-916), written to F.
+__global__ void __launch_bounds__(256, 1)
+    k_fa_apply(const double2 *U, const double2 *Uf, const double2 *Gx, double2 *F, double2 *Ff,
+               int N, int SS, Geo geo) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5;
+  const size_t V = (size_t)geo.V;
+  double2 *T = sm + (size_t)(warp * LPW + g) * (2 * SS + RING), *Y = T + SS, *ring = Y + SS;
+  bool valid;
+  const long link = group_unit(g, 4L * geo.V, valid);
+  const int mu = (int)(link / geo.V);
+  const int site = (int)(link - (long)mu * geo.V);
+  int x[4];
+  coords(geo, site, x);
+  const int c = L.c;
+  const double2 one = make_double2(1.0, 0.0);
+  Nb n;
+  n.site = site;
+  n.fwd = n.bwd = 0;
+  stage(Y, U, Uf, mu, n, geo, N, L);
+  const double2 tflag = cmul(one, Y[0]);
+  product<MO, false>(LeftG{Gx + site, V, 0u, 0u, ring}, one, Y, Y[0], N, L,
+                     [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+  if (L.j == 0) T[0] = tflag;
+  __syncwarp(L.mask);
+  const Nb up = neighbour(geo, x, mu, 1);
+  stage_site(Y, Gx, up.site, V, N, L, one, true);
+  double2 *dst = F + (size_t)mu * 9 * N * V + site;
+  product<MO, false>(LeftS{T}, tflag, Y, one, N, L, [&](int k, int r, double2 v) {
+    if (valid) dst[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
+  });
+  if (L.j == 0 && valid) Ff[(size_t)mu * V + site] = cmul(tflag, one);
+}
+
+// Wg(x) = sum_mu [log U_mu(x) - log U_mu(x-mu)]  (nspt.cc:871-877)
+__global__ void k_fa_div(const double2 *__restrict__ Lg, double2 *__restrict__ Wg, int N, Geo geo) {
+  const size_t V = (size_t)geo.V;
+  const size_t tot = (size_t)9 * N * V;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = i / V;
+    const int site = (int)(i - e * V);
+    int x[4];
+    coords(geo, site, x);
+    double2 w = cz();
+#pragma unroll
+    for (int mu = 0; mu < 4; mu++) {
+      const Nb b = neighbour(geo, x, mu, -1, 0, 0);
+      const double2 *pl = Lg + ((size_t)mu * 9 * N + e) * V;
+      w = cadd(w, csub(pl[site], pl[b.site]));
+    }
+    Wg[i] = w;
+  }
+}
+
+// Wg(p) *= -alpha / p2hat(p), Wg(0) = 0  (nspt.cc:881-894)
+__global__ void k_fa_scale(double2 *Wg, int N, Geo geo, double alpha) {
+  const size_t V = (size_t)geo.V;
+  const size_t tot = (size_t)9 * N * V;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t e = i / V;
+    const int site = (int)(i - e * V);
+    double f = 0.0;
+    if (site != 0) {
+      int x[4];
+      coords(geo, site, x);
+      f = -(alpha / (c_p2hat[0][x[0]] + c_p2hat[1][x[1]] + c_p2hat[2][x[2]] + c_p2hat[3][x[3]]));
+    }
+    Wg[i] = cscale(Wg[i], f);
+  }
+}
+
+// One pass of a 4-D FFT: all lines along one direction (length n, site stride
+// st) of every plane, one thread per line; unnormalised, sign -1 forward
+// (FFTW_FORWARD) / +1 backward.  Power-of-two n: radix-2 in registers.
+template <int n>
+__global__ void k_fft_pow2(double2 *data, long nlines, int st, size_t V, int sign) {
+  const long id = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (id >= nlines) return;
+  const long per_plane = (long)V / n;
+  const long p = id / per_plane, rem = id - p * per_plane;
+  const long outer = rem / st, inner = rem - outer * st;
+  double2 *b = data + (size_t)p * V + (size_t)outer * n * st + inner;
+  double2 v[n];
+#pragma unroll
+  for (int i = 0; i < n; i++) {
+    int r = 0;
+#pragma unroll
+    for (int q = 1, t = i; q < n; q <<= 1, t >>= 1) r = (r << 1) | (t & 1);
+    v[r] = b[(size_t)i * st];
+  }
+#pragma unroll
+  for (int len = 2; len <= n; len <<= 1) {
+    const int half = len >> 1;
+#pragma unroll
+    for (int k = 0; k < half; k++) {
+      double2 w = c_tw64[k * (64 / len)];
+      if (sign > 0) w.y = -w.y;
+#pragma unroll
+      for (int s0 = 0; s0 < n; s0 += len) {
+        const double2 bb = cmul(v[s0 + k + half], w);
+        v[s0 + k + half] = csub(v[s0 + k], bb);
+        v[s0 + k] = cadd(v[s0 + k], bb);
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < n; i++) b[(size_t)i * st] = v[i];
+}
+
+// Direct DFT for other lengths (n <= 128), one thread per line.
+__global__ void k_fft_direct(double2 *data, long nlines, int n, int st, size_t V, int sign) {
+  const long id = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (id >= nlines) return;
+  const long per_plane = (long)V / n;
+  const long p = id / per_plane, rem = id - p * per_plane;
+  const long outer = rem / st, inner = rem - outer * st;
+  double2 *b = data + (size_t)p * V + (size_t)outer * n * st + inner;
+  double2 in[128];
+  for (int i = 0; i < n; i++) in[i] = b[(size_t)i * st];
+  for (int k = 0; k < n; k++) {
+    double2 acc = cz();
+    for (int i = 0; i < n; i++) {
+      const int m = (int)(((long)k * i) % n);
+      double sn, cs;
+      sincospi((double)sign * 2.0 * (double)m / (double)n, &sn, &cs);
+      acc = cadd(acc, cmul(in[i], make_double2(cs, sn)));
+    }
+    b[(size_t)k * st] = acc;
+  }
+}
+
+// Deterministic row sums: out[r] = sum_i in[r*stride + i], i < n.
+template <class T>
+__global__ void k_rowsum(const T *__restrict__ in, size_t stride, long n, T *out) {
+  __shared__ T sh[256];
+  const T *row = in + (size_t)blockIdx.x * stride;
+  T acc;
+  if constexpr (sizeof(T) == 16) {
+    acc = cz();
+    for (long i = threadIdx.x; i < n; i += blockDim.x) acc = cadd(acc, row[i]);
+  } else {
+    acc = 0.0;
+    for (long i = threadIdx.x; i < n; i += blockDim.x) acc += row[i];
+  }
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      if constexpr (sizeof(T) == 16)
+        sh[threadIdx.x] = cadd(sh[threadIdx.x], sh[threadIdx.x + w]);
+      else
+        sh[threadIdx.x] += sh[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+}
+
+// MMs[mu][e] = MM[mu][e] * (1/V)  (MM[mu] *= rVol, nspt.cc:607-609)
+__global__ void k_scale_mm(double2 *MM, int n, double rvol) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) MM[i] = cscale(MM[i], rvol);
+}
+
+// Host AoS chunk (sites [s0, s0+cs), reference ptGluon layout with A orders)
+// <-> device planes.
+__global__ void k_unpack(const double2 *__restrict__ aos, int A, int s0, int cs, double2 *U,
+                         double2 *Uf, int N, size_t V) {
+  const int ser = 1 + 9 * A;
+  const long tot = (long)cs * 4 * (1 + 9 * N);
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < tot;
+       i += (long)gridDim.x * blockDim.x) {
+    const int ls = (int)(i % cs);
+    const long q = i / cs;
+    const int e = (int)(q % (1 + 9 * N));
+    const int mu = (int)(q / (1 + 9 * N));
+    const double2 v = aos[((size_t)ls * 4 + mu) * ser + e];
+    const size_t site = (size_t)s0 + ls;
+    if (e == 0)
+      Uf[(size_t)mu * V + site] = v;
+    else
+      U[((size_t)mu * 9 * N + (e - 1)) * V + site] = v;
+  }
+}
+__global__ void k_pack(double2 *__restrict__ aos, int A, int s0, int cs, const double2 *U,
+                       const double2 *Uf, int N, size_t V) {
+  const int ser = 1 + 9 * A;
+  const long tot = (long)cs * 4 * ser;
+  for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < tot;
+       i += (long)gridDim.x * blockDim.x) {
+    const int ls = (int)(i % cs);
+    const long q = i / cs;
+    const int e = (int)(q % ser);
+    const int mu = (int)(q / ser);
+    const size_t site = (size_t)s0 + ls;
+    double2 v;
+    if (e == 0)
+      v = Uf[(size_t)mu * V + site];
+    else if (e - 1 < 9 * N)
+      v = U[((size_t)mu * 9 * N + (e - 1)) * V + site];
+    else
+      v = cz();
+    aos[((size_t)ls * 4 + mu) * ser + e] = v;
+  }
+}
+
+__global__ void k_cold(double2 *U, double2 *Uf, size_t nU, size_t nF) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nU;
+       i += (size_t)gridDim.x * blockDim.x)
+    U[i] = cz();
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < nF;
+       i += (size_t)gridDim.x * blockDim.x)
+    Uf[i] = make_double2(1.0, 0.0);
+}
+
+// FP64 FMA throughput probe: 8 independent chains per thread.
+__global__ void k_fp64_peak(double *out, int iters, double seed) {
+  double a[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) a[q] = seed + q + threadIdx.x * 1e-9;
+  const double m = 0.999999999, ad = 1e-12;
+  for (int it = 0; it < iters; it++) {
+#pragma unroll
+    for (int u = 0; u < 16; u++)
+#pragma unroll
+      for (int q = 0; q < 8; q++) a[q] = fma(a[q], m, ad);
+  }
+  double s = 0;
+#pragma unroll
+  for (int q = 0; q < 8; q++) s += a[q];
+  if (s == 12345.678) out[0] = s;  // keeps the chains live
+}
+
+}  // namespace nspt

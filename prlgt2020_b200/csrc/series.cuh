@@ -1,0 +1,326 @@
+// series.cuh -- device arithmetic on truncated power series of 3x3 complex
+// matrices (the reference's ptSU3, QCDpt.h:42-226), FP64.
+//
+// Shared-memory "slot" of one series, 1 + 9*N double2, COLUMN major inside
+// each order:
+//   slot[0]                     flag (order-0 coefficient times the identity)
+//   slot[1 + 9*(k-1) + 3*c + r] order k, row r, column c        (k = 1..N)
+// Global link planes (kernels.cuh) are row major: element (k, r, c) of link
+// (mu, site) at  U[((mu*9N + 9(k-1) + 3r + c) * V + site].
+//
+// Work split of one series product C = A * B.  A "link group" of 9 lanes
+// owns one series computation.  Lane (c, s), c, s in {0,1,2}, owns column c
+// of the result orders k = s+1, s+4, s+7, ... (all orders of the column
+// between the three lanes of that column).  Since C_k[:,c] = sum_i A_i
+// B_{k-i}[:,c], the lane needs the whole left operand A and column c of the
+// right operand B:
+//   * every lane of the group walks the same i, so each left coefficient A_i
+//     (9 complex) is one broadcast read for the group -- straight from the
+//     global planes (L1/L2, prefetched one order ahead) or from a slot;
+//   * each right column B_j[:,c] (3 complex, one 48-byte column of the slot)
+//     feeds 9 complex FMAs; the 27 lanes of a warp read 27 distinct columns
+//     that fall on distinct bank quads (slot stride = 1 mod 8 quads, column
+//     major, group stride = 3 mod 8 quads).
+// Accumulators of up to 3*MO orders per pass stay in registers; passes run
+// from high to low order and every lane finishes reading a pass before any
+// lane writes it, so a result may overwrite its right operand in place.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nspt {
+
+__device__ __forceinline__ double2 cz() { return make_double2(0.0, 0.0); }
+__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
+  return make_double2(a.x + b.x, a.y + b.y);
+}
+__device__ __forceinline__ double2 csub(double2 a, double2 b) {
+  return make_double2(a.x - b.x, a.y - b.y);
+}
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.y * b.x + a.x * b.y);
+}
+__device__ __forceinline__ double2 cconj(double2 a) { return make_double2(a.x, -a.y); }
+__device__ __forceinline__ double2 cscale(double2 a, double x) {
+  return make_double2(a.x * x, a.y * x);
+}
+__device__ __forceinline__ bool cis0(double2 a) { return a.x == 0.0 && a.y == 0.0; }
+// acc += a * b  (4 FP64 FMAs)
+__device__ __forceinline__ void cfma(double2 &acc, double2 a, double2 b) {
+  acc.x = fma(a.x, b.x, acc.x);
+  acc.x = fma(-a.y, b.y, acc.x);
+  acc.y = fma(a.x, b.y, acc.y);
+  acc.y = fma(a.y, b.x, acc.y);
+}
+// flag of a product: a0*b0, or an exact 0 when both are 0 (QCDpt.h:102-104)
+__device__ __forceinline__ double2 flag_mul(double2 a0, double2 b0) {
+  return (cis0(a0) && cis0(b0)) ? cz() : cmul(a0, b0);
+}
+
+// slot index of (order k, row r, column c)
+__device__ __forceinline__ int sidx(int k, int r, int c) { return 1 + 9 * (k - 1) + 3 * c + r; }
+
+// Twist matrices Omega_d and Omega_d^dag (twistmatrices.h:158-240).
+__constant__ double2 c_om[4][9];
+__constant__ double2 c_omd[4][9];
+
+// 3x3 complex product r = a * b, row major (SU3::operator*, MyMath.h:791-849).
+__device__ __forceinline__ void m3_mul(double2 *r, const double2 *a, const double2 *b) {
+#pragma unroll
+  for (int i = 0; i < 3; i++)
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      double2 t = cmul(a[3 * i], b[q]);
+      t = cadd(t, cmul(a[3 * i + 1], b[3 + q]));
+      t = cadd(t, cmul(a[3 * i + 2], b[6 + q]));
+      r[3 * i + q] = t;
+    }
+}
+
+// Omega U Omega^dag for every twisted face a read crossed: backward wraps
+// first (Omega_d^dag U Omega_d), then forward wraps, as the reference's
+// backward copy slabs hold them (lattice.h:733-790, nspt.cc:221-253).
+// m is row major.
+__device__ __forceinline__ void twist3(double2 *m, unsigned tb, unsigned tf) {
+  double2 t[9];
+#pragma unroll
+  for (int d = 1; d < 4; d++)
+    if ((tb >> d) & 1) {
+      m3_mul(t, c_omd[d], m);
+      m3_mul(m, t, c_om[d]);
+    }
+#pragma unroll
+  for (int d = 1; d < 4; d++)
+    if ((tf >> d) & 1) {
+      m3_mul(t, c_om[d], m);
+      m3_mul(m, t, c_omd[d]);
+    }
+}
+
+// Identity of a lane inside its 9-lane link group.
+struct Lane {
+  int c;          // owned column
+  int s;          // owned residue: orders k = s+1 (mod 3)
+  int j;          // 3*c + s, 0..8
+  unsigned mask;  // the group's lanes
+};
+
+// Left operand in the global row-major planes of one link, optionally
+// twisted on load.  Element (k, r, l) at p[(9(k-1) + 3r + l) * V].  The
+// product streams it through a 3-order ring in shared memory: lane j of the
+// group copies colour component j of order i+2 with cp.async while order i
+// is in use, so the L2 latency of the next coefficients is hidden.
+constexpr int RING = 32;  // double2 per group: 3 orders x 9, padded to 0 mod 8
+struct LeftG {
+  static constexpr bool kRing = true;
+  const double2 *p;
+  size_t V;
+  unsigned tb, tf;
+  double2 *ring;
+  __device__ __forceinline__ void issue(int k, int j) const {
+    const double2 *src = p + (size_t)(9 * (k - 1) + j) * V;
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(ring + 9 * ((k - 1) % 3) + j);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
+  }
+  template <bool DAG>
+  __device__ __forceinline__ void from_ring(int k, double2 *a) const {
+    double2 m[9];
+    const double2 *q = ring + 9 * ((k - 1) % 3);
+#pragma unroll
+    for (int e = 0; e < 9; e++) m[e] = q[e];
+    if (tb | tf) twist3(m, tb, tf);
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int l = 0; l < 3; l++) a[3 * r + l] = DAG ? cconj(m[3 * l + r]) : m[3 * r + l];
+  }
+  // column c of op(A)_k (flag terms), straight from global
+  template <bool DAG>
+  __device__ __forceinline__ void col(int k, int c, double2 *o) const {
+    double2 m[9];
+    const double2 *q = p + (size_t)9 * (k - 1) * V;
+    if (tb | tf) {
+#pragma unroll
+      for (int e = 0; e < 9; e++) m[e] = __ldg(q + (size_t)e * V);
+      twist3(m, tb, tf);
+#pragma unroll
+      for (int r = 0; r < 3; r++) o[r] = DAG ? cconj(m[3 * c + r]) : m[3 * r + c];
+      return;
+    }
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+      o[r] = DAG ? cconj(__ldg(q + (size_t)(3 * c + r) * V)) : __ldg(q + (size_t)(3 * r + c) * V);
+  }
+};
+
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
+
+// Left operand in a slot (column major).
+struct LeftS {
+  static constexpr bool kRing = false;
+  const double2 *s;
+  template <bool DAG>
+  __device__ __forceinline__ void load(int k, double2 *a) const {
+    const double2 *q = s + 1 + 9 * (k - 1);
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int l = 0; l < 3; l++) a[3 * r + l] = DAG ? cconj(q[3 * r + l]) : q[3 * l + r];
+  }
+  template <bool DAG>
+  __device__ __forceinline__ void col(int k, int c, double2 *o) const {
+#pragma unroll
+    for (int r = 0; r < 3; r++) o[r] = DAG ? cconj(s[sidx(k, c, r)]) : s[sidx(k, r, c)];
+  }
+};
+
+// C = op(A) * B, orders 1..M (truncated Cauchy product, ptSU3::operator*,
+// QCDpt.h:92-114); op = dagger when DA.  a0 = flag of op(A), b0 = flag of B,
+// supplied by the caller (the result's flag is the caller's business).
+// emit(k, r, v) is called by the lane owning (k, column c) for r = 0..2.
+template <int MO, bool DA, class Left, class Emit>
+__device__ __forceinline__ void product(const Left &A, double2 a0, const double2 *B, double2 b0,
+                                        int M, const Lane &L, Emit emit) {
+  const int c = L.c;
+  constexpr int PASS = 3 * MO;
+  const int npass = (M + PASS - 1) / PASS;
+  for (int ps = npass - 1; ps >= 0; --ps) {
+    const int kb = ps * PASS;
+    const int kend = min(kb + PASS, M);  // last order of the pass
+    double2 acc[MO][3];
+#pragma unroll
+    for (int q = 0; q < MO; q++)
+#pragma unroll
+      for (int r = 0; r < 3; r++) acc[q][r] = cz();
+    double2 a[9];
+    if constexpr (Left::kRing) {
+      // orders 1 and 2 in flight before the loop; one commit group per order
+      if (1 < kend) A.issue(1, L.j);
+      cp_commit();
+      if (2 < kend) A.issue(2, L.j);
+      cp_commit();
+    }
+    for (int i = 1; i < kend; i++) {
+      if constexpr (Left::kRing) {
+        cp_wait1();               // this lane's copy of order i has landed
+        __syncwarp(L.mask);       // ... and every lane's; order i-1 is free
+        if (i + 2 < kend) A.issue(i + 2, L.j);
+        cp_commit();
+        A.template from_ring<DA>(i, a);
+      } else {
+        A.template load<DA>(i, a);
+      }
+#pragma unroll
+      for (int q = 0; q < MO; q++) {
+        const int k = kb + L.s + 1 + 3 * q;
+        if (k <= kend && k > i) {
+          const double2 *bj = B + 1 + 9 * (k - i - 1) + 3 * c;
+          const double2 b0_ = bj[0], b1 = bj[1], b2 = bj[2];
+#pragma unroll
+          for (int r = 0; r < 3; r++) {
+            cfma(acc[q][r], a[3 * r], b0_);
+            cfma(acc[q][r], a[3 * r + 1], b1);
+            cfma(acc[q][r], a[3 * r + 2], b2);
+          }
+        }
+      }
+    }
+    if constexpr (Left::kRing) cp_wait0();
+    __syncwarp(L.mask);
+    const bool fa = !cis0(a0), fb = !cis0(b0);
+#pragma unroll
+    for (int q = 0; q < MO; q++) {
+      const int k = kb + L.s + 1 + 3 * q;
+      if (k <= kend) {
+        double2 ak[3];
+        if (fb) A.template col<DA>(k, c, ak);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          double2 v = acc[q][r];
+          // b0*A_k + a0*B_k; a zero flag contributes an exact zero, so its
+          // term is skipped (the operand may be unset there)
+          if (fa || fb) {
+            double2 u;
+            if (!fa)
+              u = cmul(b0, ak[r]);
+            else if (!fb)
+              u = cmul(a0, B[sidx(k, r, c)]);
+            else
+              u = cadd(cmul(b0, ak[r]), cmul(a0, B[sidx(k, r, c)]));
+            v = cadd(v, u);
+          }
+          emit(k, r, v);
+        }
+      }
+    }
+    __syncwarp(L.mask);
+  }
+}
+
+// R = exp(P) for P with flag 0 (exp(const ptSU3&), QCDpt.h:200-220), by
+// Horner's rule R <- 1 + (P R)/n, n = N..1, step n truncated at order N-n+1;
+// the number of 3x3 products equals the reference's pruned power sum,
+// C(N+1,3).  P and R are slots; R is updated in place.
+template <int MO>
+__device__ __forceinline__ void ser_exp(const double2 *P, double2 *R, int N, const Lane &L) {
+  if (L.j == 0) R[0] = make_double2(1.0, 0.0);
+  __syncwarp(L.mask);
+  const int c = L.c;
+  const LeftS A{P};
+  for (int n = N; n >= 1; --n) {
+    const int M = N - n + 1;
+    const double inv = 1.0 / (double)n;
+    product<MO, false>(A, cz(), R, make_double2(1.0, 0.0), M, L,
+                       [&](int k, int r, double2 v) { R[sidx(k, r, c)] = cscale(v, inv); });
+  }
+}
+
+// Horner form of log (log(const ptSU3&), QCDpt.h:176-198) for U with flag 1:
+// X = U - 1, S_N = 1/N, S_n = 1/n - X S_{n+1} (orders <= N-n), log = X S_1.
+// U and the scratch Sc are slots; emit(k, r, v) receives log_k[r][c].
+template <int MO, class Emit>
+__device__ __forceinline__ void ser_log(const double2 *U, double2 *Sc, int N, const Lane &L,
+                                        Emit emit) {
+  const int c = L.c;
+  const LeftS A{U};
+  for (int n = N - 1; n >= 1; --n) {
+    const int M = N - n;
+    const double b0 = 1.0 / (double)(n + 1);
+    product<MO, false>(A, cz(), Sc, make_double2(b0, 0.0), M, L,
+                       [&](int k, int r, double2 v) { Sc[sidx(k, r, c)] = make_double2(-v.x, -v.y); });
+  }
+  product<MO, false>(A, cz(), Sc, make_double2(1.0, 0.0), N, L, emit);
+}
+
+// reH on a slot (ptSU3::reH, QCDpt.cc:197-209): per order (M - M^dag)/2
+// minus a third of the trace times 1; flag 0.  The formula is the same for
+// row- and column-major storage.  Lanes split the orders.
+__device__ __forceinline__ void ser_reH(double2 *P, int N, const Lane &L) {
+  const double D3 = 1.0 / 3.0;
+  for (int k = 1 + L.j; k <= N; k += 9) {
+    double2 *m = P + 1 + 9 * (k - 1);
+    double2 a[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) a[e] = m[e];
+    double2 b[9];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        double2 d = csub(a[3 * r + q], cconj(a[3 * q + r]));
+        b[3 * r + q] = make_double2(.5 * d.x, .5 * d.y);
+      }
+    double2 tr = cadd(cadd(b[0], b[4]), b[8]);
+    tr = make_double2(tr.x * D3, D3 * tr.y);
+    b[0] = csub(b[0], tr);
+    b[4] = csub(b[4], tr);
+    b[8] = csub(b[8], tr);
+#pragma unroll
+    for (int e = 0; e < 9; e++) m[e] = b[e];
+  }
+  if (L.j == 0) P[0] = cz();
+}
+
+}  // namespace nspt
