@@ -105,6 +105,14 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def barrier(world: int):
+    import torch
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -194,6 +202,45 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def e2e_leg(args, eng, lib, _lib, P, N, V, world, field_bytes):
+    """Upload from pinned host memory, K x (sweep + observables read-back),
+    download -- all through the C ABI, wall-clocked on the host."""
+    import numpy as np
+    import torch
+    host = torch.empty((V * 4 * P.series_len(N),), dtype=torch.float64, pin_memory=True)
+    eng.cold_start()
+    obs_p = np.zeros((N + 1, 2))
+    obs_n = np.zeros(N)
+    obs_t = np.zeros((4, N, 2))
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    host_ptr = host.data_ptr()
+    h = eng._h
+    barrier(world)
+    t0 = time.perf_counter()
+    _lib.check(lib.nspt_download_links(h, ctypes.c_void_p(host_ptr), N), "download")
+    t1 = time.perf_counter()
+    e2e_steps = args.steps
+    _lib.check(lib.nspt_upload_links(h, ctypes.c_void_p(host_ptr), N), "upload")
+    for _ in range(e2e_steps):
+        _lib.check(lib.nspt_step(h, args.dt, 1, 0), "step")
+        _lib.check(lib.nspt_observables(h, dp(obs_p), dp(obs_n), dp(obs_t)), "observables")
+    _lib.check(lib.nspt_download_links(h, ctypes.c_void_p(host_ptr), N), "download")
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    e2e_s = t2 - t1
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * e2e_steps / float(te.item())
+    obs_bytes = obs_p.nbytes + obs_n.nbytes + obs_t.nbytes
+
+    return {"value": e2e_value, "unit": "sweeps/s",
+            "h2d_bytes_per_step": field_bytes / e2e_steps,
+            "d2h_bytes_per_step": field_bytes / e2e_steps + obs_bytes,
+            "note": "upload + %d x (sweep + observables read-back) + download" % e2e_steps}
+
+
 def run_ours(args, world, rank, local):
     import numpy as np
     import torch
@@ -219,19 +266,13 @@ def run_ours(args, world, rank, local):
     eng.seed(1000 + rank, 0)
     eng.cold_start()
 
-    def barrier():
-        torch.cuda.synchronize()
-        if world > 1:
-            import torch.distributed as dist
-            dist.barrier()
-
     # warm-up sweeps (also move the field away from the cold start)
     eng.NsptEvolve(args.dt, args.warmup, 0)
-    barrier()
+    barrier(world)
     with ClockSampler(local) as clk:
         eng.NsptEvolve(args.dt, args.steps, 0)
         ms = eng.last_step_ms()
-    barrier()
+    barrier(world)
     clocks = clk.summary()
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if world > 1:
@@ -246,35 +287,11 @@ def run_ours(args, world, rank, local):
     achieved = flops / (ms_step * 1e-3) / 1e12
 
     # end to end through the C ABI with the configuration on the host
-    host = torch.empty((V * 4 * P.series_len(N),), dtype=torch.float64, pin_memory=True)
-    eng.cold_start()
-    obs_p = np.zeros((N + 1, 2))
-    obs_n = np.zeros(N)
-    obs_t = np.zeros((4, N, 2))
-    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
-    host_ptr = host.data_ptr()
-    h = eng._h
-    barrier()
-    t0 = time.perf_counter()
-    _lib.check(lib.nspt_download_links(h, ctypes.c_void_p(host_ptr), N), "download")
-    t1 = time.perf_counter()
-    e2e_steps = args.steps
-    _lib.check(lib.nspt_upload_links(h, ctypes.c_void_p(host_ptr), N), "upload")
-    for _ in range(e2e_steps):
-        _lib.check(lib.nspt_step(h, args.dt, 1, 0), "step")
-        _lib.check(lib.nspt_observables(h, dp(obs_p), dp(obs_n), dp(obs_t)), "observables")
-    _lib.check(lib.nspt_download_links(h, ctypes.c_void_p(host_ptr), N), "download")
-    torch.cuda.synchronize()
-    t2 = time.perf_counter()
-    e2e_s = t2 - t1
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_steps / float(te.item())
     field_bytes = V * 4 * P.series_len(N) * 8
-    obs_bytes = obs_p.nbytes + obs_n.nbytes + obs_t.nbytes
-
+    if args.no_e2e:
+        e2e = None
+    else:
+        e2e = e2e_leg(args, eng, lib, _lib, P, N, V, world, field_bytes)
     cpu = None
     if rank == 0 and not args.no_cpu:
         spp, threads, kind, _b = cpu_reference_sample(N, (8, 8, 8, 8), 1)
@@ -301,10 +318,7 @@ def run_ours(args, world, rank, local):
                          "algorithmic_bytes_per_sweep": algorithmic_bytes_per_sweep(V, N),
                          "hbm_gbs_equiv": algorithmic_bytes_per_sweep(V, N) / (ms_step * 1e-3) / 1e9},
             "clocks": clocks,
-            "e2e": {"value": e2e_value, "unit": "sweeps/s",
-                    "h2d_bytes_per_step": (field_bytes + 0) / e2e_steps,
-                    "d2h_bytes_per_step": field_bytes / e2e_steps + obs_bytes,
-                    "note": "upload + %d x (sweep + observables read-back) + download" % e2e_steps},
+            "e2e": e2e,
             "gpu_launches": 4 * args.steps,
             "cpu_baseline": cpu,
         }
@@ -325,7 +339,8 @@ def main():
     ap.add_argument("--L", type=int, nargs=4, default=[32, 32, 32, 32])
     ap.add_argument("--N", type=int, default=24)
     ap.add_argument("--dt", type=float, default=0.005)
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
