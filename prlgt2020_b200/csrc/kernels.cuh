@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(256, 1) k_sweep(SweepArgs a) {
       const Nb b = neighbour(a.g, x, nu, 1);
       stage(Y, a.U, a.Uf, mu, b, a.g, N, L);
       const double2 a0 = __ldg(a.Uf + (size_t)nu * V + site);
-      const LeftG A{a.U + nu * plane_mu + site, V, 0u, 0u, ring};
+      const LeftG A{a.U + nu * plane_mu + site, V, ring};
       // T holds dag(U_nu(x) U_mu(x+nu))
       product<MO, false>(A, a0, Y, Y[0], N, L,
                          [&](int k, int r, double2 v) { T[sidx(k, c, r)] = cconj(v); });
@@ -254,17 +254,16 @@ __global__ void __launch_bounds__(256, 1) k_sweep(SweepArgs a) {
       __syncwarp(L.mask);
     }
     {
+      // U_nu(x+mu) is staged (twisted when it crosses a twisted face)
       const Nb m = neighbour(a.g, x, mu, 1);
-      const double2 a0 = link_flag(a.Uf, nu, m, a.g);
-      const LeftG A{a.U + nu * plane_mu + m.site, V, m.bwd & tw, m.fwd & tw, ring};
+      stage(Y, a.U, a.Uf, nu, m, a.g, N, L);
+      const double2 a0 = Y[0];
       const double2 b0 = T[0];
-      if (first)
-        product<MO, false>(A, a0, T, b0, N, L, [&](int k, int r, double2 v) { W[sidx(k, r, c)] = v; });
-      else
-        product<MO, false>(A, a0, T, b0, N, L, [&](int k, int r, double2 v) {
-          double2 &w = W[sidx(k, r, c)];
-          w = cadd(w, v);
-        });
+      const bool f0 = first;
+      product<MO, false>(LeftS{Y}, a0, T, b0, N, L, [&](int k, int r, double2 v) {
+        double2 &w = W[sidx(k, r, c)];
+        w = f0 ? v : cadd(w, v);
+      });
       const double2 f = flag_mul(a0, b0);
       wflag = first ? f : cadd(wflag, f);
       first = false;
@@ -274,11 +273,14 @@ __global__ void __launch_bounds__(256, 1) k_sweep(SweepArgs a) {
       const Nb d = neighbour(a.g, x, nu, -1);
       const Nb dm = neighbour(a.g, x, nu, -1, mu, 1);
       stage(Y, a.U, a.Uf, nu, dm, a.g, N, L);
-      const double2 a0 = link_flag(a.Uf, mu, d, a.g);
-      const LeftG A{a.U + mu * plane_mu + d.site, V, d.bwd & tw, d.fwd & tw, ring};
-      product<MO, false>(A, a0, Y, Y[0], N, L,
+      // U_mu(x-nu) is staged into T and the product overwrites it in place:
+      // every lane reads a pass before any lane writes it, and the flag term
+      // of a result cell reads only that cell's own column of the left operand
+      stage(T, a.U, a.Uf, mu, d, a.g, N, L);
+      const double2 a0 = T[0], y0 = Y[0];
+      product<MO, false>(LeftS{T}, a0, Y, y0, N, L,
                          [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
-      if (L.j == 0) T[0] = flag_mul(a0, Y[0]);
+      if (L.j == 0) T[0] = flag_mul(a0, y0);
       __syncwarp(L.mask);
       stage(Y, a.U, a.Uf, nu, d, a.g, N, L);
       const double2 ta = cconj(T[0]);
@@ -493,7 +495,7 @@ __global__ void __launch_bounds__(256, 1)
   n.fwd = n.bwd = 0;
   stage(Y, U, Uf, mu, n, geo, N, L);
   const double2 tflag = cmul(one, Y[0]);
-  product<MO, false>(LeftG{Gx + site, V, 0u, 0u, ring}, one, Y, Y[0], N, L,
+  product<MO, false>(LeftG{Gx + site, V, ring}, one, Y, Y[0], N, L,
                      [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
   if (L.j == 0) T[0] = tflag;
   __syncwarp(L.mask);

@@ -105,8 +105,8 @@ struct Lane {
   unsigned mask;  // the group's lanes
 };
 
-// Left operand in the global row-major planes of one link, optionally
-// twisted on load.  Element (k, r, l) at p[(9(k-1) + 3r + l) * V].  The
+// Left operand in the global row-major planes of one link (never a twisted
+// read: those are staged).  Element (k, r, l) at p[(9(k-1) + 3r + l) * V].  The
 // product streams it through a 3-order ring in shared memory: lane j of the
 // group copies colour component j of order i+2 with cp.async while order i
 // is in use, so the L2 latency of the next coefficients is hidden.
@@ -115,7 +115,6 @@ struct LeftG {
   static constexpr bool kRing = true;
   const double2 *p;
   size_t V;
-  unsigned tb, tf;
   double2 *ring;
   __device__ __forceinline__ void issue(int k, int j) const {
     const double2 *src = p + (size_t)(9 * (k - 1) + j) * V;
@@ -124,29 +123,16 @@ struct LeftG {
   }
   template <bool DAG>
   __device__ __forceinline__ void from_ring(int k, double2 *a) const {
-    double2 m[9];
     const double2 *q = ring + 9 * ((k - 1) % 3);
-#pragma unroll
-    for (int e = 0; e < 9; e++) m[e] = q[e];
-    if (tb | tf) twist3(m, tb, tf);
 #pragma unroll
     for (int r = 0; r < 3; r++)
 #pragma unroll
-      for (int l = 0; l < 3; l++) a[3 * r + l] = DAG ? cconj(m[3 * l + r]) : m[3 * r + l];
+      for (int l = 0; l < 3; l++) a[3 * r + l] = DAG ? cconj(q[3 * l + r]) : q[3 * r + l];
   }
   // column c of op(A)_k (flag terms), straight from global
   template <bool DAG>
   __device__ __forceinline__ void col(int k, int c, double2 *o) const {
-    double2 m[9];
     const double2 *q = p + (size_t)9 * (k - 1) * V;
-    if (tb | tf) {
-#pragma unroll
-      for (int e = 0; e < 9; e++) m[e] = __ldg(q + (size_t)e * V);
-      twist3(m, tb, tf);
-#pragma unroll
-      for (int r = 0; r < 3; r++) o[r] = DAG ? cconj(m[3 * c + r]) : m[3 * r + c];
-      return;
-    }
 #pragma unroll
     for (int r = 0; r < 3; r++)
       o[r] = DAG ? cconj(__ldg(q + (size_t)(3 * c + r) * V)) : __ldg(q + (size_t)(3 * r + c) * V);
