@@ -11,7 +11,7 @@ import os
 import subprocess
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "lib", "libnspt_b200.so")
+LIB_PATH = os.environ.get("NSPT_B200_LIB") or os.path.join(HERE, "lib", "libnspt_b200.so")
 CSRC = os.path.join(HERE, "csrc")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "nspt_b200.h")
 

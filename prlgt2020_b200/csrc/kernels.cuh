@@ -20,7 +20,10 @@ namespace nspt {
 
 constexpr int GROUP = 9;  // lanes per link group
 constexpr int LPW = 3;    // link groups per warp
-constexpr int MO = 8;     // result orders per lane per pass (3*MO orders)
+#ifndef NSPT_MO
+#define NSPT_MO 8
+#endif
+constexpr int MO = NSPT_MO;  // result orders per lane per pass (3*MO orders)
 
 struct Geo {
   int L[4];
