@@ -114,10 +114,8 @@ def barrier(world: int):
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from prlgt2020_b200.replicas import world_info
+    return world_info()
 
 
 def read_profile_traffic():
@@ -207,6 +205,8 @@ def e2e_leg(args, eng, lib, _lib, P, N, V, world, field_bytes):
     download -- all through the C ABI, wall-clocked on the host."""
     import numpy as np
     import torch
+
+    from prlgt2020_b200.replicas import max_over_ranks, whole_job_rate
     host = torch.empty((V * 4 * P.series_len(N),), dtype=torch.float64, pin_memory=True)
     eng.cold_start()
     obs_p = np.zeros((N + 1, 2))
@@ -227,12 +227,7 @@ def e2e_leg(args, eng, lib, _lib, P, N, V, world, field_bytes):
     _lib.check(lib.nspt_download_links(h, ctypes.c_void_p(host_ptr), N), "download")
     torch.cuda.synchronize()
     t2 = time.perf_counter()
-    e2e_s = t2 - t1
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * e2e_steps / float(te.item())
+    e2e_value = whole_job_rate(e2e_steps, world, max_over_ranks(t2 - t1))
     obs_bytes = obs_p.nbytes + obs_n.nbytes + obs_t.nbytes
 
     return {"value": e2e_value, "unit": "sweeps/s",
@@ -247,6 +242,7 @@ def run_ours(args, world, rank, local):
 
     import prlgt2020_b200 as P
     from prlgt2020_b200 import _lib
+    from prlgt2020_b200.replicas import max_over_ranks, replica_seed, whole_job_rate
 
     if not torch.cuda.is_available():
         raise SystemExit("bench.py: no CUDA device")
@@ -263,7 +259,7 @@ def run_ours(args, world, rank, local):
     peak = P.fp64_peak_tflops()
 
     eng = P.NsptEngine(L, N, twist="yz")
-    eng.seed(1000 + rank, 0)
+    eng.seed(replica_seed(1000, rank), 0)
     eng.cold_start()
 
     # warm-up sweeps (also move the field away from the cold start)
@@ -274,13 +270,9 @@ def run_ours(args, world, rank, local):
         ms = eng.last_step_ms()
     barrier(world)
     clocks = clk.summary()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        import torch.distributed as dist
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
+    ms_max = max_over_ranks(ms)
     ms_step = ms_max / args.steps
-    value = world * args.steps / (ms_max * 1e-3)
+    value = whole_job_rate(args.steps, world, ms_max * 1e-3)
 
     # roofline of the dominant kernel (the sweep): canonical flops / sweep time
     flops = canonical_flops_per_link(N) * 4 * V

@@ -88,11 +88,12 @@ static size_t group_bytes(const nspt_ctx *ctx, int slots, int extra) {
   return ((size_t)slots * ctx->SS + extra) * sizeof(double2);
 }
 
-static KernelShape choose_shape(const nspt_ctx *ctx, int slots, long units, int extra = 0) {
+static KernelShape choose_shape(const nspt_ctx *ctx, int slots, long units, int extra = 0,
+                                int max_warps = 8) {
   KernelShape k;
   k.slots = slots;
   const size_t per_warp = (size_t)LPW * group_bytes(ctx, slots, extra);
-  int wmax = (int)std::min<size_t>(8, ctx->smem_optin / per_warp);
+  int wmax = (int)std::min<size_t>(max_warps, ctx->smem_optin / per_warp);
   if (wmax < 1) wmax = 1;
   // spread small lattices over the SMs: about two CTAs per SM if possible
   const long want = (units + (long)LPW * 2 * ctx->nsm - 1) / ((long)LPW * 2 * ctx->nsm);
@@ -102,8 +103,8 @@ static KernelShape choose_shape(const nspt_ctx *ctx, int slots, long units, int 
 
 static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
   const long nl = 4 * ctx->V;
-  KernelShape k = choose_shape(ctx, 3, nl, RING);
-  const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, 3, RING);
+  KernelShape k = choose_shape(ctx, 2, nl, RING, SWEEP_THREADS / 32);
+  const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, 2, RING);
   const long per_cta = (long)k.warps * LPW;
   const unsigned grid = (unsigned)((nl + per_cta - 1) / per_cta);
   const dim3 blk(32 * k.warps);
@@ -361,7 +362,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->SS = 1 + 9 * N;
   while (ctx->SS % 8 != 1) ctx->SS++;
   // one warp (3 link groups of 3 slots) must fit in a CTA
-  if ((size_t)LPW * group_bytes(ctx, 3, RING) > ctx->smem_optin) return fail(NSPT_ERR_ORDER);
+  if ((size_t)LPW * group_bytes(ctx, 2, RING) > ctx->smem_optin) return fail(NSPT_ERR_ORDER);
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return fail(NSPT_ERR_CUDA);
   cudaEventCreate(&ctx->ev0);
   cudaEventCreate(&ctx->ev1);
@@ -580,6 +581,7 @@ extern "C" int nspt_plaquette_measure(nspt_ctx *ctx, double *plaq) {
   memset(&a, 0, sizeof(a));
   a.U = ctx->U;
   a.Uf = ctx->Uf;
+  a.F = ctx->F;  // scratch for the staple sums; the field in U is untouched
   a.obs_tr = ctx->obs_tr;
   a.N = ctx->N;
   a.SS = ctx->SS;

@@ -220,8 +220,22 @@ __device__ __forceinline__ long group_unit(int g, long nunits, bool &valid) {
 
 // Jacobi Langevin sweep, one link per group: gauge_wilson, nspt.cc:362-439.
 // MEASURE: only the plaquette traces (plaquette_measure, nspt.cc:1362-1383).
+//
+// Two series slots per group (T, Y) plus the left-operand ring.  The staple
+// sum W never occupies a slot: each lane accumulates the cells it owns
+// (orders k = s+1 mod 3 of column c, every row) in this link's own rows of
+// the output field F -- a store for the first staple, then red.add -- and
+// reads them back before U * W.  Only that lane ever touches those addresses
+// until it writes the updated link there, so the additions happen in program
+// order (the same order, hence the same rounding, as a running sum) and no
+// other thread can observe them.
+#ifndef NSPT_SWEEP_THREADS
+#define NSPT_SWEEP_THREADS 256
+#endif
+constexpr int SWEEP_THREADS = NSPT_SWEEP_THREADS;
+
 template <bool MEASURE>
-__global__ void __launch_bounds__(256, 1) k_sweep(SweepArgs a) {
+__global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
   extern __shared__ double2 sm[];
   Lane L;
   int g;
@@ -229,7 +243,7 @@ __global__ void __launch_bounds__(256, 1) k_sweep(SweepArgs a) {
   const int warp = threadIdx.x >> 5;
   const int N = a.N, SS = a.SS, c = L.c;
   const size_t V = (size_t)a.g.V;
-  double2 *W = sm + (size_t)(warp * LPW + g) * (3 * SS + RING), *T = W + SS, *Y = T + SS;
+  double2 *T = sm + (size_t)(warp * LPW + g) * (2 * SS + RING), *Y = T + SS;
   double2 *ring = Y + SS;
   bool valid;
   const long link = group_unit(g, 4L * a.g.V, valid);
@@ -238,7 +252,9 @@ __global__ void __launch_bounds__(256, 1) k_sweep(SweepArgs a) {
   int x[4];
   coords(a.g, site, x);
   const size_t plane_mu = (size_t)9 * N * V;
-  const unsigned tw = a.g.twist;
+  // this link's rows of F: the staple sum first, the updated link at the end
+  double *Fo = reinterpret_cast<double *>(a.F + (size_t)mu * plane_mu + site);
+  auto fcell = [&](int k, int r) { return Fo + 2 * (size_t)(9 * (k - 1) + 3 * r + c) * V; };
 
   double2 wflag = cz();
   bool first = true;
@@ -264,8 +280,14 @@ __global__ void __launch_bounds__(256, 1) k_sweep(SweepArgs a) {
       const double2 b0 = T[0];
       const bool f0 = first;
       product<MO, false>(LeftS{Y}, a0, T, b0, N, L, [&](int k, int r, double2 v) {
-        double2 &w = W[sidx(k, r, c)];
-        w = f0 ? v : cadd(w, v);
+        if (!valid) return;
+        double *w = fcell(k, r);
+        if (f0) {
+          __stcg(reinterpret_cast<double2 *>(w), v);
+        } else {
+          atomicAdd(w, v.x);
+          atomicAdd(w + 1, v.y);
+        }
       });
       const double2 f = flag_mul(a0, b0);
       wflag = first ? f : cadd(wflag, f);
@@ -289,22 +311,31 @@ __global__ void __launch_bounds__(256, 1) k_sweep(SweepArgs a) {
       const double2 ta = cconj(T[0]);
       const LeftS A2{T};
       product<MO, true>(A2, ta, Y, Y[0], N, L, [&](int k, int r, double2 v) {
-        double2 &w = W[sidx(k, r, c)];
-        w = cadd(w, v);
+        if (!valid) return;
+        double *w = fcell(k, r);
+        atomicAdd(w, v.x);
+        atomicAdd(w + 1, v.y);
       });
       wflag = cadd(wflag, flag_mul(ta, Y[0]));
     }
   }
-  if (L.j == 0) W[0] = wflag;
-  // ---- P = U_mu(x) * staples (nspt.cc:392); U_mu(x) stays in Y for F = exp(.) U
+  // ---- the staple sum back into T (each lane its own cells), U_mu(x) into Y
   {
     Nb self;
     self.site = site;
     self.fwd = self.bwd = 0;
     stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
   }
+  for (int k = L.s + 1; k <= N; k += 3) {
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+      T[sidx(k, r, c)] = valid ? __ldcg(reinterpret_cast<const double2 *>(fcell(k, r))) : cz();
+  }
+  if (L.j == 0) T[0] = wflag;
+  __syncwarp(L.mask);
+  // ---- P = U_mu(x) * staples (nspt.cc:392), in place over the staple sum
   const double2 pflag = flag_mul(Y[0], wflag);
-  product<MO, false>(LeftS{Y}, Y[0], W, wflag, N, L,
+  product<MO, false>(LeftS{Y}, Y[0], T, wflag, N, L,
                      [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
   if (L.j == 0) T[0] = pflag;
   __syncwarp(L.mask);
@@ -363,24 +394,27 @@ __global__ void __launch_bounds__(256, 1) k_sweep(SweepArgs a) {
     if (L.j == 0) T[0] = cscale(cz(), a.tau_g);
     __syncwarp(L.mask);
   }
-  // ---- F = exp(W1) * U  (nspt.cc:429)
-  ser_exp<MO>(T, W, N, L);
+  // ---- F = exp(W1) * U  (nspt.cc:429): exp into Y, U_mu(x) restaged into T
+  ser_exp<MO>(T, Y, N, L);
+  {
+    Nb self;
+    self.site = site;
+    self.fwd = self.bwd = 0;
+    stage(T, a.U, a.Uf, mu, self, a.g, N, L);
+  }
   const bool zm = a.Lg != nullptr;
-  double2 *Fo = a.F + (size_t)mu * plane_mu + site;
-  product<MO, false>(LeftS{W}, make_double2(1.0, 0.0), Y, Y[0], N, L,
+  double2 *Fc = a.F + (size_t)mu * plane_mu + site;
+  product<MO, false>(LeftS{Y}, make_double2(1.0, 0.0), T, T[0], N, L,
                      [&](int k, int r, double2 v) {
-                       if (valid) Fo[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
+                       if (valid) Fc[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
                        if (zm) T[sidx(k, r, c)] = v;
                      });
-  if (L.j == 0) {
-    if (valid) a.Ff[(size_t)mu * V + site] = Y[0];
-    T[0] = Y[0];
-  }
+  if (L.j == 0 && valid) a.Ff[(size_t)mu * V + site] = T[0];
   if (!zm) return;
   __syncwarp(L.mask);
   // ---- MM[mu] += log(F[link])  (nspt.cc:432-439): logs stored per link
   double2 *Lo = a.Lg + (size_t)mu * plane_mu + site;
-  ser_log<MO>(T, W, N, L, [&](int k, int r, double2 v) {
+  ser_log<MO>(T, Y, N, L, [&](int k, int r, double2 v) {
     if (valid) Lo[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
   });
 }

@@ -1,0 +1,63 @@
+"""Independent replicas, one lattice per rank (one process per GPU).
+
+The Langevin step does not shard: every rank advances its own lattice with
+its own noise stream and no exchange during a step.  Ranks meet only to
+time the job (a barrier, then the max of the per-rank device times) and to
+gather per-replica observables at the end.  These helpers work on any
+process group: NCCL with CUDA tensors on GPUs, gloo with CPU tensors.
+"""
+from __future__ import annotations
+
+import os
+
+
+def world_info():
+    """(world_size, rank, local_rank) from the torchrun environment."""
+    return (int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def replica_seed(base: int, rank: int) -> int:
+    """Noise seed of replica `rank`: distinct per rank, reproducible."""
+    if rank < 0:
+        raise ValueError("rank must be >= 0")
+    return int(base) + 1000003 * int(rank)
+
+
+def _device():
+    import torch
+    import torch.distributed as dist
+    if dist.is_initialized() and dist.get_backend() == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
+def max_over_ranks(x: float) -> float:
+    """Max of a scalar over all ranks (identity without a process group)."""
+    import torch
+    import torch.distributed as dist
+    if not dist.is_initialized() or dist.get_world_size() == 1:
+        return float(x)
+    t = torch.tensor([float(x)], dtype=torch.float64, device=_device())
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def gather_series(values) -> list:
+    """All ranks' per-replica series (e.g. plaquette per order), rank order."""
+    import torch
+    import torch.distributed as dist
+    t = torch.as_tensor(values, dtype=torch.float64).reshape(-1).to(_device())
+    if not dist.is_initialized() or dist.get_world_size() == 1:
+        return [t.cpu().tolist()]
+    out = [torch.empty_like(t) for _ in range(dist.get_world_size())]
+    dist.all_gather(out, t)
+    return [o.cpu().tolist() for o in out]
+
+
+def whole_job_rate(units_per_rank: float, world: int, seconds_max: float) -> float:
+    """Units per second of the whole job: every rank processed
+    `units_per_rank` units and the slowest rank took `seconds_max`."""
+    if seconds_max <= 0:
+        raise ValueError("seconds_max must be > 0")
+    return world * units_per_rank / seconds_max
