@@ -120,6 +120,37 @@ double nspt_last_step_ms(const nspt_ctx *ctx);
  * chains on every SM), TFLOP/s.  Roofline denominator for the sweep. */
 int nspt_measure_fp64_peak(double *tflops);
 
+/* Static plaquette of a field the caller already holds in device memory,
+ * without a context and without allocating anything.  This entry point has
+ * no counterpart in the reference.  It computes what nspt_plaquette_measure
+ * computes (plaquette_measure, nspt.cc:1316-1406): plaq[(N+1)*2], per order
+ * sum Tr(U * staples) / 72V.
+ *
+ * Who needs it: a program that keeps its own device copy of a
+ * configuration.  Examples: a driver that moved it with its own copies, a
+ * framework with a fixed memory pool, or a job whose device memory is
+ * already spent on evolution fields.  nspt_create would allocate two more
+ * field-sized buffers (29 GB at 32^4 x 24) just to look at one number.  The
+ * caller may not have that memory, or may not be allowed to allocate at that
+ * point without synchronising the device or breaking its memory plan.
+ *
+ * links_dev: the reference's AoS layout (site-major, mu, {flag, allocORD x
+ * 9 complex}), 16-byte aligned, in device memory of the current device.
+ * flags: NSPT_TWIST_Y | NSPT_TWIST_Z | NSPT_TWIST_T only.  stream: a
+ * cudaStream_t (NULL = the default stream); the call waits for it.
+ *
+ * Scratch: a fixed static device array of 803,600 bytes (1024 partial rows
+ * plus one result row of NSPT_MAX_ORDER + 1 complex doubles).  Its address
+ * is looked up once per device on the first call, with that device
+ * current; make that first call before any stream capture.  No call relies
+ * on the array's earlier contents.  Calls that overlap on one device share
+ * the array and race: serialise them.  N > NSPT_MAX_ORDER (more orders than
+ * the scratch rows hold) returns NSPT_ERR_ORDER; N > allocORD, a bad flag,
+ * a misaligned pointer or a volume above 2^29 sites returns NSPT_ERR_ARG. */
+int nspt_plaquette_measure_noalloc(const void *links_dev, int allocORD,
+                                   const int L[4], int N, unsigned flags,
+                                   double *plaq, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -669,3 +669,6 @@ extern "C" int nspt_measure_fp64_peak(double *tflops) {
   *tflops = flops / (ms * 1e-3) / 1e12;
   return NSPT_OK;
 }
+
+// allocation-free plaquette of a caller-owned device field
+#include "noalloc.cuh"
