@@ -46,6 +46,7 @@ struct nspt_ctx {
   double *obs_norm;
   double2 *red2;  // [(N+1) + 4N + 4*9N] reduced sums
   double *red1;   // [N]
+  double *p2;     // lattice momenta p2hat[4][128] of this context's extents
   double *noise;  // injected noise
   bool noise_pending;
   bool have_obs;
@@ -240,7 +241,7 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
   k_fa_div<<<eg, 256, 0, st>>>(Lg, Wg, N, geo);
   CK(cudaGetLastError());
   if ((rc = fft4d(ctx, Wg, -1))) return rc;
-  k_fa_scale<<<eg, 256, 0, st>>>(Wg, N, geo, alpha);
+  k_fa_scale<<<eg, 256, 0, st>>>(Wg, N, geo, alpha, ctx->p2);
   CK(cudaGetLastError());
   if ((rc = fft4d(ctx, Wg, +1))) return rc;
   rc = launch_groups(
@@ -287,7 +288,7 @@ static int upload_constants(nspt_ctx *ctx) {
       h *= 4 * h;
       p2[d][i] = h;
     }
-  CK(cudaMemcpyToSymbol(c_p2hat, p2, sizeof(p2)));
+  CK(cudaMemcpy(ctx->p2, p2, sizeof(p2), cudaMemcpyHostToDevice));
   double2 tw[64];
   for (int k = 0; k < 64; k++) {
     double ang = -1.0 * 2.0 * M_PI * (double)k / 64.0;
@@ -298,7 +299,7 @@ static int upload_constants(nspt_ctx *ctx) {
 }
 
 static void free_all(nspt_ctx *ctx) {
-  void *ptrs[] = {ctx->U, ctx->Uf, ctx->F, ctx->Ff, ctx->Lg, ctx->Wg, ctx->Gx,
+  void *ptrs[] = {ctx->U, ctx->Uf, ctx->F, ctx->Ff, ctx->Lg, ctx->Wg, ctx->Gx, ctx->p2,
                   ctx->obs_tr, ctx->obs_tru, ctx->obs_norm, ctx->red2, ctx->red1, ctx->noise};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -330,6 +331,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->alpha = alpha;
   ctx->V = V;
   ctx->U = ctx->Uf = ctx->F = ctx->Ff = ctx->Lg = ctx->Wg = ctx->Gx = nullptr;
+  ctx->p2 = nullptr;
   ctx->obs_tr = ctx->obs_tru = ctx->red2 = nullptr;
   ctx->obs_norm = ctx->red1 = ctx->noise = nullptr;
   ctx->noise_pending = false;
@@ -380,7 +382,8 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
             alloc((void **)&ctx->obs_tru, N * nl * sizeof(double2)) &&
             alloc((void **)&ctx->obs_norm, N * nl * sizeof(double)) &&
             alloc((void **)&ctx->red2, ((N + 1) + 4 * N + 36 * N) * sizeof(double2)) &&
-            alloc((void **)&ctx->red1, N * sizeof(double));
+            alloc((void **)&ctx->red1, N * sizeof(double)) &&
+            alloc((void **)&ctx->p2, 4 * 128 * sizeof(double));
   if (ok && (flags & (NSPT_ZEROMODE | NSPT_GF_FA))) ok = alloc((void **)&ctx->Lg, field);
   if (ok && (flags & NSPT_GF_FA))
     ok = alloc((void **)&ctx->Wg, field / 4) && alloc((void **)&ctx->Gx, field / 4);

@@ -32,8 +32,7 @@ struct Geo {
   unsigned twist;  // bit d: direction d twisted
 };
 
-// Lattice momenta p2hat[d][n] = 4 sin^2(pi n / L_d)  (lattice.h:1144-1169).
-__constant__ double c_p2hat[4][128];
+
 // exp(-2 pi i k / 64), k < 64, radix-2 FFT twiddles.
 __constant__ double2 c_tw64[64];
 
@@ -567,7 +566,9 @@ __global__ void k_fa_div(const double2 *__restrict__ Lg, double2 *__restrict__ W
 }
 
 // Wg(p) *= -alpha / p2hat(p), Wg(0) = 0  (nspt.cc:881-894)
-__global__ void k_fa_scale(double2 *Wg, int N, Geo geo, double alpha) {
+// p2: the context's lattice momenta p2hat[d][n] = 4 sin^2(pi n / L_d)
+// (lattice.h:1144-1169), 128 entries per direction.
+__global__ void k_fa_scale(double2 *Wg, int N, Geo geo, double alpha, const double *__restrict__ p2) {
   const size_t V = (size_t)geo.V;
   const size_t tot = (size_t)9 * N * V;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot;
@@ -578,7 +579,7 @@ __global__ void k_fa_scale(double2 *Wg, int N, Geo geo, double alpha) {
     if (site != 0) {
       int x[4];
       coords(geo, site, x);
-      f = -(alpha / (c_p2hat[0][x[0]] + c_p2hat[1][x[1]] + c_p2hat[2][x[2]] + c_p2hat[3][x[3]]));
+      f = -(alpha / (p2[x[0]] + p2[128 + x[1]] + p2[256 + x[2]] + p2[384 + x[3]]));
     }
     Wg[i] = cscale(Wg[i], f);
   }

@@ -224,3 +224,18 @@ def test_device_noise_statistics_and_determinism(engine_mod):
     m = m.reshape(-1, 3, 3)
     assert np.abs(m + np.conj(m.transpose(0, 2, 1))).max() < 1e-12
     assert np.abs(np.trace(m, axis1=1, axis2=2)).max() < 1e-12
+
+
+def test_two_contexts_with_different_extents_interleaved(engine_mod, oracle_mod):
+    """Contexts are independent: two FA contexts of different extents on one
+    device, stepped alternately, each match their own oracle run."""
+    cases = [((4, 4, 4, 4), 5, -0.05, 21), ((6, 4, 2, 4), 5, -0.08, 22)]
+    pairs = [make_pair(engine_mod, oracle_mod, L, N, zm=True, fa=True, alpha=a, start=st)
+             for L, N, a, st in cases]
+    rngs = [oracle_mod.Rand55(40 + i) for i in range(len(cases))]
+    for _ in range(2):
+        for (e, o), rng, (_, _, alpha, _) in zip(pairs, rngs, cases):
+            eo, oo = step_both(e, o, 0.01, rng, zm=True, fa=True, alpha=alpha)
+            check_obs(eo, oo, 1e-11)
+    for (e, o), (L, N, _, _) in zip(pairs, cases):
+        assert per_order_rel(e.download(), o.links, N).max() <= 1e-11
