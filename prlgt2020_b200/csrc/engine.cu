@@ -104,8 +104,8 @@ static KernelShape choose_shape(const nspt_ctx *ctx, int slots, long units, int 
 
 static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
   const long nl = 4 * ctx->V;
-  KernelShape k = choose_shape(ctx, 2, nl, RING, SWEEP_THREADS / 32);
-  const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, 2, RING);
+  KernelShape k = choose_shape(ctx, SWEEP_SLOTS, nl, RING, SWEEP_THREADS / 32);
+  const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, SWEEP_SLOTS, RING);
   const long per_cta = (long)k.warps * LPW;
   const unsigned grid = (unsigned)((nl + per_cta - 1) / per_cta);
   const dim3 blk(32 * k.warps);
@@ -196,7 +196,7 @@ static int do_zero_modes(nspt_ctx *ctx) {
   const Geo geo = ctx->geo;
   cudaStream_t st = ctx->st;
   return launch_groups(
-      ctx, (const void *)k_zero_modes, 2, nl,
+      ctx, (const void *)k_zero_modes, 3, nl,
       [&](unsigned g, dim3 b, size_t sm) { k_zero_modes<<<g, b, sm, st>>>(U, Uf, Lg, MM, N, SS, geo); },
       "zero modes");
 }
@@ -232,7 +232,7 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
   double2 *U = ctx->U, *Uf = ctx->Uf, *F = ctx->F, *Ff = ctx->Ff, *Lg = ctx->Lg, *Wg = ctx->Wg,
           *Gx = ctx->Gx;
   int rc = launch_groups(
-      ctx, (const void *)k_log_links, 2, nl,
+      ctx, (const void *)k_log_links, 3, nl,
       [&](unsigned g, dim3 b, size_t sm) { k_log_links<<<g, b, sm, st>>>(U, Uf, Lg, N, SS, geo); },
       "FA logs");
   if (rc) return rc;
@@ -245,7 +245,7 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
   CK(cudaGetLastError());
   if ((rc = fft4d(ctx, Wg, +1))) return rc;
   rc = launch_groups(
-      ctx, (const void *)k_fa_gt, 2, ctx->V,
+      ctx, (const void *)k_fa_gt, 3, ctx->V,
       [&](unsigned g, dim3 b, size_t sm) { k_fa_gt<<<g, b, sm, st>>>(Wg, Gx, N, SS, geo); },
       "FA gauge transform");
   if (rc) return rc;
@@ -364,7 +364,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->SS = 1 + 9 * N;
   while (ctx->SS % 8 != 1) ctx->SS++;
   // one warp (3 link groups of 3 slots) must fit in a CTA
-  if ((size_t)LPW * group_bytes(ctx, 2, RING) > ctx->smem_optin) return fail(NSPT_ERR_ORDER);
+  if ((size_t)LPW * group_bytes(ctx, SWEEP_SLOTS, RING) > ctx->smem_optin) return fail(NSPT_ERR_ORDER);
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return fail(NSPT_ERR_CUDA);
   cudaEventCreate(&ctx->ev0);
   cudaEventCreate(&ctx->ev1);
@@ -584,7 +584,6 @@ extern "C" int nspt_plaquette_measure(nspt_ctx *ctx, double *plaq) {
   memset(&a, 0, sizeof(a));
   a.U = ctx->U;
   a.Uf = ctx->Uf;
-  a.F = ctx->F;  // scratch for the staple sums; the field in U is untouched
   a.obs_tr = ctx->obs_tr;
   a.N = ctx->N;
   a.SS = ctx->SS;

@@ -220,18 +220,14 @@ __device__ __forceinline__ long group_unit(int g, long nunits, bool &valid) {
 // Jacobi Langevin sweep, one link per group: gauge_wilson, nspt.cc:362-439.
 // MEASURE: only the plaquette traces (plaquette_measure, nspt.cc:1362-1383).
 //
-// Two series slots per group (T, Y) plus the left-operand ring.  The staple
-// sum W never occupies a slot: each lane accumulates the cells it owns
-// (orders k = s+1 mod 3 of column c, every row) in this link's own rows of
-// the output field F -- a store for the first staple, then red.add -- and
-// reads them back before U * W.  Only that lane ever touches those addresses
-// until it writes the updated link there, so the additions happen in program
-// order (the same order, hence the same rounding, as a running sum) and no
-// other thread can observe them.
+// Three series slots per group (T, Y, W) plus the left-operand ring: W
+// holds the staple sum, then X^2 of the series exp; T and Y hold staged
+// operands, products, the force and the exp.
 #ifndef NSPT_SWEEP_THREADS
 #define NSPT_SWEEP_THREADS 256
 #endif
 constexpr int SWEEP_THREADS = NSPT_SWEEP_THREADS;
+constexpr int SWEEP_SLOTS = 3;
 
 template <bool MEASURE>
 __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
@@ -242,18 +238,16 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
   const int warp = threadIdx.x >> 5;
   const int N = a.N, SS = a.SS, c = L.c;
   const size_t V = (size_t)a.g.V;
-  double2 *T = sm + (size_t)(warp * LPW + g) * (2 * SS + RING), *Y = T + SS;
-  double2 *ring = Y + SS;
+  double2 *T = sm + (size_t)(warp * LPW + g) * (SWEEP_SLOTS * SS + RING), *Y = T + SS;
+  double2 *W = Y + SS, *ring = W + SS;
   bool valid;
   const long link = group_unit(g, 4L * a.g.V, valid);
+  if (!valid) return;  // groups are independent: a group past the end has no work
   const int mu = (int)(link / a.g.V);
   const int site = (int)(link - (long)mu * a.g.V);
   int x[4];
   coords(a.g, site, x);
   const size_t plane_mu = (size_t)9 * N * V;
-  // this link's rows of F: the staple sum first, the updated link at the end
-  double *Fo = reinterpret_cast<double *>(a.F + (size_t)mu * plane_mu + site);
-  auto fcell = [&](int k, int r) { return Fo + 2 * (size_t)(9 * (k - 1) + 3 * r + c) * V; };
 
   double2 wflag = cz();
   bool first = true;
@@ -279,14 +273,8 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
       const double2 b0 = T[0];
       const bool f0 = first;
       product<MO, false>(LeftS{Y}, a0, T, b0, N, L, [&](int k, int r, double2 v) {
-        if (!valid) return;
-        double *w = fcell(k, r);
-        if (f0) {
-          __stcg(reinterpret_cast<double2 *>(w), v);
-        } else {
-          atomicAdd(w, v.x);
-          atomicAdd(w + 1, v.y);
-        }
+        double2 &w = W[sidx(k, r, c)];
+        w = f0 ? v : cadd(w, v);
       });
       const double2 f = flag_mul(a0, b0);
       wflag = first ? f : cadd(wflag, f);
@@ -308,38 +296,26 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
       __syncwarp(L.mask);
       stage(Y, a.U, a.Uf, nu, d, a.g, N, L);
       const double2 ta = cconj(T[0]);
-      const LeftS A2{T};
-      product<MO, true>(A2, ta, Y, Y[0], N, L, [&](int k, int r, double2 v) {
-        if (!valid) return;
-        double *w = fcell(k, r);
-        atomicAdd(w, v.x);
-        atomicAdd(w + 1, v.y);
+      product<MO, true>(LeftS{T}, ta, Y, Y[0], N, L, [&](int k, int r, double2 v) {
+        double2 &w = W[sidx(k, r, c)];
+        w = cadd(w, v);
       });
       wflag = cadd(wflag, flag_mul(ta, Y[0]));
     }
   }
-  // ---- the staple sum back into T (each lane its own cells), U_mu(x) into Y
-  {
-    Nb self;
-    self.site = site;
-    self.fwd = self.bwd = 0;
-    stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
-  }
-  for (int k = L.s + 1; k <= N; k += 3) {
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-      T[sidx(k, r, c)] = valid ? __ldcg(reinterpret_cast<const double2 *>(fcell(k, r))) : cz();
-  }
-  if (L.j == 0) T[0] = wflag;
-  __syncwarp(L.mask);
-  // ---- P = U_mu(x) * staples (nspt.cc:392), in place over the staple sum
+  if (L.j == 0) W[0] = wflag;
+  // ---- P = U_mu(x) * staples (nspt.cc:392) into T; U_mu(x) in Y
+  Nb self;
+  self.site = site;
+  self.fwd = self.bwd = 0;
+  stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
   const double2 pflag = flag_mul(Y[0], wflag);
-  product<MO, false>(LeftS{Y}, Y[0], T, wflag, N, L,
+  product<MO, false>(LeftS{Y}, Y[0], W, wflag, N, L,
                      [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
   if (L.j == 0) T[0] = pflag;
   __syncwarp(L.mask);
   // ---- traces (ptSU3::Tr, QCDpt.cc:115-122), norm and Tr U_k (nspt.cc:393-402)
-  if (valid) {
+  {
     const size_t nl4 = 4 * V;
     if (L.j == 0) a.obs_tr[link] = make_double2(3. * pflag.x, 3. * pflag.y);
     for (int k = 1 + L.j; k <= N; k += GROUP) {
@@ -393,28 +369,24 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
     if (L.j == 0) T[0] = cscale(cz(), a.tau_g);
     __syncwarp(L.mask);
   }
-  // ---- F = exp(W1) * U  (nspt.cc:429): exp into Y, U_mu(x) restaged into T
-  ser_exp<MO>(T, Y, N, L);
-  {
-    Nb self;
-    self.site = site;
-    self.fwd = self.bwd = 0;
-    stage(T, a.U, a.Uf, mu, self, a.g, N, L);
-  }
+  // ---- F = exp(W1) * U  (nspt.cc:429): exp into Y (W holds the square of
+  // W1), U_mu(x) restaged into W
+  ser_exp<MO>(T, W, Y, N, L);
+  stage(W, a.U, a.Uf, mu, self, a.g, N, L);
   const bool zm = a.Lg != nullptr;
   double2 *Fc = a.F + (size_t)mu * plane_mu + site;
-  product<MO, false>(LeftS{Y}, make_double2(1.0, 0.0), T, T[0], N, L,
+  product<MO, false>(LeftS{Y}, make_double2(1.0, 0.0), W, W[0], N, L,
                      [&](int k, int r, double2 v) {
-                       if (valid) Fc[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
-                       if (zm) T[sidx(k, r, c)] = v;
+                       Fc[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
+                       if (zm) W[sidx(k, r, c)] = v;
                      });
-  if (L.j == 0 && valid) a.Ff[(size_t)mu * V + site] = T[0];
+  if (L.j == 0) a.Ff[(size_t)mu * V + site] = W[0];
   if (!zm) return;
   __syncwarp(L.mask);
   // ---- MM[mu] += log(F[link])  (nspt.cc:432-439): logs stored per link
   double2 *Lo = a.Lg + (size_t)mu * plane_mu + site;
-  ser_log<MO>(T, Y, N, L, [&](int k, int r, double2 v) {
-    if (valid) Lo[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
+  ser_log<MO>(W, T, Y, N, L, [&](int k, int r, double2 v) {
+    Lo[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
   });
 }
 
@@ -429,9 +401,10 @@ __global__ void __launch_bounds__(256, 1)
   if (!make_lane(L, g)) return;
   const int warp = threadIdx.x >> 5;
   const size_t V = (size_t)geo.V;
-  double2 *P = sm + (size_t)(warp * LPW + g) * 2 * SS, *R = P + SS;
+  double2 *P = sm + (size_t)(warp * LPW + g) * 3 * SS, *R = P + SS, *Y2 = R + SS;
   bool valid;
   const long link = group_unit(g, 4L * geo.V, valid);
+  if (!valid) return;
   const int mu = (int)(link / geo.V);
   const int site = (int)(link - (long)mu * geo.V);
   const double2 *src = Lg + (size_t)mu * 9 * N * V + site;
@@ -447,8 +420,7 @@ __global__ void __launch_bounds__(256, 1)
   __syncwarp(L.mask);
   ser_reH(P, N, L);
   __syncwarp(L.mask);
-  ser_exp<MO>(P, R, N, L);
-  if (!valid) return;
+  ser_exp<MO>(P, Y2, R, N, L);
   double2 *dst = U + (size_t)mu * 9 * N * V + site;
   const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
   for (int k = 1; k <= N; k++) dst[(size_t)(9 * (k - 1) + L.j) * V] = R[sidx(k, r, c)];
@@ -464,9 +436,10 @@ __global__ void __launch_bounds__(256, 1)
   if (!make_lane(L, g)) return;
   const int warp = threadIdx.x >> 5;
   const size_t V = (size_t)geo.V;
-  double2 *X = sm + (size_t)(warp * LPW + g) * 2 * SS, *Sc = X + SS;
+  double2 *X = sm + (size_t)(warp * LPW + g) * 3 * SS, *Sc = X + SS, *Y2 = Sc + SS;
   bool valid;
   const long link = group_unit(g, 4L * geo.V, valid);
+  if (!valid) return;
   const int mu = (int)(link / geo.V);
   const int site = (int)(link - (long)mu * geo.V);
   Nb n;
@@ -475,8 +448,8 @@ __global__ void __launch_bounds__(256, 1)
   stage(X, U, Uf, mu, n, geo, N, L);
   double2 *dst = Lg + (size_t)mu * 9 * N * V + site;
   const int c = L.c;
-  ser_log<MO>(X, Sc, N, L, [&](int k, int r, double2 v) {
-    if (valid) dst[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
+  ser_log<MO>(X, Y2, Sc, N, L, [&](int k, int r, double2 v) {
+    dst[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
   });
 }
 
@@ -489,9 +462,10 @@ __global__ void __launch_bounds__(256, 1)
   if (!make_lane(L, g)) return;
   const int warp = threadIdx.x >> 5;
   const size_t V = (size_t)geo.V;
-  double2 *P = sm + (size_t)(warp * LPW + g) * 2 * SS, *R = P + SS;
+  double2 *P = sm + (size_t)(warp * LPW + g) * 3 * SS, *R = P + SS, *Y2 = R + SS;
   bool valid;
   const long site = group_unit(g, geo.V, valid);
+  if (!valid) return;
   const double dv = (double)geo.V;
   const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
   for (int k = 1; k <= N; k++) {
@@ -502,8 +476,7 @@ __global__ void __launch_bounds__(256, 1)
   __syncwarp(L.mask);
   ser_reH(P, N, L);
   __syncwarp(L.mask);
-  ser_exp<MO>(P, R, N, L);
-  if (!valid) return;
+  ser_exp<MO>(P, Y2, R, N, L);
   for (int k = 1; k <= N; k++) Gx[(size_t)(9 * (k - 1) + L.j) * V + site] = R[sidx(k, r, c)];
 }
 

@@ -23,7 +23,7 @@
 //     major, group stride = 3 mod 8 quads).
 // Accumulators of up to 3*MO orders per pass stay in registers; passes run
 // from high to low order and every lane finishes reading a pass before any
-// lane writes it, so a result may overwrite its right operand in place.
+// lane writes it, so a result may overwrite either operand in place.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -245,39 +245,88 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
   }
 }
 
-// R = exp(P) for P with flag 0 (exp(const ptSU3&), QCDpt.h:200-220), by
-// Horner's rule R <- 1 + (P R)/n, n = N..1, step n truncated at order N-n+1;
-// the number of 3x3 products equals the reference's pruned power sum,
-// C(N+1,3).  P and R are slots; R is updated in place.
-template <int MO>
-__device__ __forceinline__ void ser_exp(const double2 *P, double2 *R, int N, const Lane &L) {
-  if (L.j == 0) R[0] = make_double2(1.0, 0.0);
-  __syncwarp(L.mask);
+// Polynomial p(X) = sum_{n<=N} coef(n) X^n of a series X with flag 0,
+// truncated at order N, by Paterson-Stockmeyer with block 2.  Y = X^2 is
+// formed once; then Horner in Y,
+//   S_J = B_J,  S_j = Y S_{j+1} + B_j,  B_j = coef(2j) + coef(2j+1) X,
+// with S_j needed only to order N - 2j (Y^j starts at order 2j).  X^n starts
+// at order n, so this is the same truncated sum as Horner in X, with
+// 1 + N/2 series products of sizes 2, 4, ..., N instead of N products of
+// sizes 1..N (1354 instead of 2300 3x3 products at N = 24).  The last step
+// goes to last(k, r, v) instead of S.  X, Y and S are slots.
+template <int MO, class Coef, class Last>
+__device__ __forceinline__ void ser_poly2(const double2 *X, double2 *Y, double2 *S, int N,
+                                          const Lane &L, Coef coef, Last last) {
   const int c = L.c;
-  const LeftS A{P};
-  for (int n = N; n >= 1; --n) {
-    const int M = N - n + 1;
-    const double inv = 1.0 / (double)n;
-    product<MO, false>(A, cz(), R, make_double2(1.0, 0.0), M, L,
-                       [&](int k, int r, double2 v) { R[sidx(k, r, c)] = cscale(v, inv); });
+  // Y = X X (order 1 comes out as an exact zero)
+  product<MO, false>(LeftS{X}, cz(), X, cz(), N, L,
+                     [&](int k, int r, double2 v) { Y[sidx(k, r, c)] = v; });
+  const int J = N / 2;
+  // S_J = coef(2J) + coef(2J+1) X to order N - 2J; higher orders zero (they
+  // meet Y's zero order-1 coefficient and must be finite)
+  {
+    const double cx = coef(2 * J + 1);
+    for (int k = L.s + 1; k <= N; k += 3) {
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+        S[sidx(k, r, c)] = k <= N - 2 * J ? cscale(X[sidx(k, r, c)], cx) : cz();
+    }
+    if (L.j == 0) S[0] = make_double2(coef(2 * J), 0.0);
+    __syncwarp(L.mask);
+  }
+  if (J == 0) {  // N = 1: S_0 is the result
+    for (int k = L.s + 1; k <= N; k += 3) {
+#pragma unroll
+      for (int r = 0; r < 3; r++) last(k, r, S[sidx(k, r, c)]);
+    }
+    __syncwarp(L.mask);
+    return;
+  }
+  const LeftS Yl{Y};
+  for (int j = J - 1; j >= 0; --j) {
+    const int M = N - 2 * j;
+    const double2 sf = S[0];
+    const double cx = coef(2 * j + 1);
+    if (j > 0) {
+      product<MO, false>(Yl, cz(), S, sf, M, L, [&](int k, int r, double2 v) {
+        S[sidx(k, r, c)] = cadd(v, cscale(X[sidx(k, r, c)], cx));
+      });
+      if (L.j == 0) S[0] = make_double2(coef(2 * j), 0.0);
+      __syncwarp(L.mask);
+    } else {
+      product<MO, false>(Yl, cz(), S, sf, M, L, [&](int k, int r, double2 v) {
+        last(k, r, cadd(v, cscale(X[sidx(k, r, c)], cx)));
+      });
+    }
   }
 }
 
-// Horner form of log (log(const ptSU3&), QCDpt.h:176-198) for U with flag 1:
-// X = U - 1, S_N = 1/N, S_n = 1/n - X S_{n+1} (orders <= N-n), log = X S_1.
-// U and the scratch Sc are slots; emit(k, r, v) receives log_k[r][c].
-template <int MO, class Emit>
-__device__ __forceinline__ void ser_log(const double2 *U, double2 *Sc, int N, const Lane &L,
-                                        Emit emit) {
+__device__ __forceinline__ double inv_factorial(int n) {
+  double f = 1.0;
+  for (int m = 2; m <= n; m++) f *= (double)m;
+  return 1.0 / f;
+}
+
+// R = exp(P) for P with flag 0 (exp(const ptSU3&), QCDpt.h:200-220):
+// sum_{n<=N} P^n / n!, flag 1.  P, Y (scratch) and R are slots.
+template <int MO>
+__device__ __forceinline__ void ser_exp(const double2 *P, double2 *Y, double2 *R, int N,
+                                        const Lane &L) {
   const int c = L.c;
-  const LeftS A{U};
-  for (int n = N - 1; n >= 1; --n) {
-    const int M = N - n;
-    const double b0 = 1.0 / (double)(n + 1);
-    product<MO, false>(A, cz(), Sc, make_double2(b0, 0.0), M, L,
-                       [&](int k, int r, double2 v) { Sc[sidx(k, r, c)] = make_double2(-v.x, -v.y); });
-  }
-  product<MO, false>(A, cz(), Sc, make_double2(1.0, 0.0), N, L, emit);
+  ser_poly2<MO>(P, Y, R, N, L, [](int n) { return inv_factorial(n); },
+                [&](int k, int r, double2 v) { R[sidx(k, r, c)] = v; });
+  if (L.j == 0) R[0] = make_double2(1.0, 0.0);
+  __syncwarp(L.mask);
+}
+
+// log(U) for U with flag 1 (log(const ptSU3&), QCDpt.h:176-198): with
+// X = U - 1, sum_{n<=N} (-1)^{n+1} X^n / n, flag 0.  U, Y and Sc are slots
+// (Y, Sc scratch); emit(k, r, v) receives log_k[r][c].
+template <int MO, class Emit>
+__device__ __forceinline__ void ser_log(const double2 *U, double2 *Y, double2 *Sc, int N,
+                                        const Lane &L, Emit emit) {
+  ser_poly2<MO>(U, Y, Sc, N, L,
+                [](int n) { return n == 0 ? 0.0 : ((n & 1) ? 1.0 : -1.0) / (double)n; }, emit);
 }
 
 // reH on a slot (ptSU3::reH, QCDpt.cc:197-209): per order (M - M^dag)/2
