@@ -734,52 +734,134 @@ void oracle_fa_gauge_fix(oracle_ctx *c, double alpha) {
   free(Wg);
 }
 
-/* stochastic_gauge_fixing, nspt.cc:660-862: sequential lexicographic sweep,
- * in place (periodic boundaries). */
-void oracle_local_gauge_fix(oracle_ctx *c, double alpha) {
+/* One site of stochastic_gauge_fixing (nspt.cc:665-720, OpenMP branch
+ * nspt.cc:731-795): W = sum_mu U_mu(x) - U_mu(x-mu) (the backward link read
+ * through the twisted copy when it crosses a twisted face), W -= W^dag,
+ * Trless, then U_mu(x) <- exp(alpha W) U_mu(x) and U_mu(x-mu) <- U_mu(x-mu)
+ * exp(-alpha W), where a backward link across a twisted face takes
+ * twist_mu(exp(-alpha W)) = Omega W2 Omega^dag per order, flag VACUUM = 1
+ * (nspt.cc:97-160). Scratch: 8 series. */
+static void local_gf_site(oracle_ctx *c, const int *x, double alpha, cx *scr) {
   int N = c->N, n = SER(N);
-  cx *W = (cx *)malloc(sizeof(cx) * n * 8);
-  cx *T = W + n, *D = W + 2 * n, *A = W + 3 * n, *E1 = W + 4 * n,
-     *E2 = W + 5 * n, *B = W + 6 * n, *Bn = W + 7 * n;
-  for (long s = 0; s < c->V; s++) {
-    int x[4];
-    coords_of(c, s, x);
-    s_zero(W, N);
-    for (int mu = 0; mu < 4; mu++) {
-      int y[4];
-      memcpy(y, x, sizeof(y));
-      y[mu] = (y[mu] - 1 + c->L[mu]) % c->L[mu];
-      const cx *a = link_ptr(c->U, c, s, mu);
-      const cx *b = link_ptr(c->U, c, site_of(c, y), mu);
-      for (int k = 0; k < n; k++) T[k] = csub(a[k], b[k]);
-      s_acc(W, T, N);
+  cx *W = scr, *T = scr + n, *D = scr + 2 * n, *A = scr + 3 * n, *E1 = scr + 4 * n,
+     *E2 = scr + 5 * n, *B = scr + 6 * n, *Bn = scr + 7 * n;
+  long s = site_of(c, x);
+  s_zero(W, N);
+  for (int mu = 0; mu < 4; mu++) {
+    int y[4];
+    memcpy(y, x, sizeof(y));
+    y[mu] -= 1;
+    const cx *a = link_ptr(c->U, c, s, mu);
+    fetch_link(c, c->U, y, mu, D);
+    for (int k = 0; k < n; k++) T[k] = csub(a[k], D[k]);
+    s_acc(W, T, N);
+  }
+  s_dag(D, W, N);
+  s_sub_acc(W, D, N);
+  s_trless(W, N);
+  for (int k = 0; k < n; k++) {
+    A[k].re = alpha * W[k].re;
+    A[k].im = alpha * W[k].im;
+  }
+  s_exp(E1, A, N, B, Bn);
+  for (int k = 0; k < n; k++) {
+    A[k].re = -alpha * W[k].re;
+    A[k].im = -alpha * W[k].im;
+  }
+  s_exp(E2, A, N, B, Bn);
+  for (int mu = 0; mu < 4; mu++) {
+    cx *u = link_ptr(c->U, c, s, mu);
+    s_mul(T, E1, u, N);
+    s_copy(u, T, N);
+    int y[4];
+    memcpy(y, x, sizeof(y));
+    const int wrap = y[mu] == 0;
+    y[mu] = (y[mu] - 1 + c->L[mu]) % c->L[mu];
+    cx *v = link_ptr(c->U, c, site_of(c, y), mu);
+    const cx *w2 = E2;
+    if (wrap && ((c->tw >> mu) & 1)) {
+      cx t[9], q[9];
+      for (int k = 0; k < N; k++) {
+        m_mul(t, c->omega[mu], E2 + 1 + 9 * k);
+        m_mul(q, t, c->omegadag[mu]);
+        memcpy(D + 1 + 9 * k, q, sizeof(q));
+      }
+      D[0].re = 1.0;
+      D[0].im = 0.0;
+      w2 = D;
     }
-    s_dag(D, W, N);
-    s_sub_acc(W, D, N);
-    s_trless(W, N);
-    for (int k = 0; k < n; k++) {
-      A[k].re = alpha * W[k].re;
-      A[k].im = alpha * W[k].im;
-    }
-    s_exp(E1, A, N, B, Bn);
-    for (int k = 0; k < n; k++) {
-      A[k].re = -alpha * W[k].re;
-      A[k].im = -alpha * W[k].im;
-    }
-    s_exp(E2, A, N, B, Bn);
-    for (int mu = 0; mu < 4; mu++) {
-      cx *u = link_ptr(c->U, c, s, mu);
-      s_mul(T, E1, u, N);
-      s_copy(u, T, N);
-      int y[4];
-      memcpy(y, x, sizeof(y));
-      y[mu] = (y[mu] - 1 + c->L[mu]) % c->L[mu];
-      cx *v = link_ptr(c->U, c, site_of(c, y), mu);
-      s_mul(T, v, E2, N);
-      s_copy(v, T, N);
+    s_mul(T, v, w2, N);
+    s_copy(v, T, N);
+  }
+}
+
+/* stochastic_gauge_fixing, nspt.cc:660-862, in place, as the reference
+ * built with the OpenMP thread grid grid = {ntt, ntx, nty, ntz}
+ * (choices.h:124-128, blocks set up at Quenched.cc:518-531) runs it: thread
+ * tid owns a block of L_d / n_d sites per direction and walks it
+ * lexicographically; all threads take a barrier after every iteration of the
+ * deepest split direction's loop (nspt.cc:796-815).  Threads between two
+ * barriers touch disjoint links (their sites are >= 2 apart), so the result
+ * is the sequential replay: barrier step by barrier step, thread by thread,
+ * each thread's segment in order.  grid {1,1,1,1} is the plain lexicographic
+ * sweep (nspt.cc:658-720).  Returns -1 if a block is not a whole number of
+ * sites >= 2 in a split direction. */
+int oracle_local_gauge_fix_grid(oracle_ctx *c, double alpha, const int *grid) {
+  int bs[4], dmax = -1;
+  for (int d = 0; d < 4; d++) {
+    if (grid[d] < 1 || c->L[d] % grid[d]) return -1;
+    bs[d] = c->L[d] / grid[d];
+    if (grid[d] > 1) {
+      if (bs[d] < 2) return -1;
+      dmax = d;
     }
   }
-  free(W);
+  const int nthr = grid[0] * grid[1] * grid[2] * grid[3];
+  long steps = 1, seg = 1;
+  for (int d = 0; d < 4; d++) {
+    if (d <= dmax)
+      steps *= bs[d];
+    else
+      seg *= c->L[d];
+  }
+  cx *scr = (cx *)malloc(sizeof(cx) * SER(c->N) * 8);
+  for (long p = 0; p < steps; p++) {
+    int rel[4] = {0, 0, 0, 0};
+    long q = p;
+    for (int d = dmax; d >= 0; d--) {
+      rel[d] = (int)(q % bs[d]);
+      q /= bs[d];
+    }
+    for (int tid = 0; tid < nthr; tid++) {
+      int b[4];
+      b[0] = tid / (grid[1] * grid[2] * grid[3]);
+      b[1] = (tid / (grid[2] * grid[3])) % grid[1];
+      b[2] = (tid / grid[3]) % grid[2];
+      b[3] = tid % grid[3];
+      for (long r = 0; r < seg; r++) {
+        int x[4];
+        long t = r;
+        for (int d = 3; d >= 0; d--) {
+          if (d <= dmax) {
+            x[d] = bs[d] * b[d] + rel[d];
+          } else {
+            x[d] = (int)(t % c->L[d]);
+            t /= c->L[d];
+          }
+        }
+        local_gf_site(c, x, alpha, scr);
+      }
+    }
+  }
+  free(scr);
+  return 0;
+}
+
+/* stochastic_gauge_fixing with the reference's default grid {1,1,1,1}:
+ * the sequential lexicographic sweep. */
+void oracle_local_gauge_fix(oracle_ctx *c, double alpha) {
+  const int one[4] = {1, 1, 1, 1};
+  oracle_local_gauge_fix_grid(c, alpha, one);
 }
 
 /* plaquette_measure, nspt.cc:1316-1406 (OpenMP variant) */

@@ -48,8 +48,11 @@ void oracle_sweep(oracle_ctx *c, double dt, const double *noise, double *plaq,
 void oracle_zero_modes(oracle_ctx *c);
 /* FAstochastic_gauge_fixing, nspt.cc:866-948 (periodic only) */
 void oracle_fa_gauge_fix(oracle_ctx *c, double alpha);
-/* stochastic_gauge_fixing, nspt.cc:660-862: sequential, in place (periodic) */
+/* stochastic_gauge_fixing, nspt.cc:660-862: sequential, in place */
 void oracle_local_gauge_fix(oracle_ctx *c, double alpha);
+/* the same as the reference built with OpenMP thread grid
+ * grid = {ntt, ntx, nty, ntz} runs it; -1 for a grid the reference rejects */
+int oracle_local_gauge_fix_grid(oracle_ctx *c, double alpha, const int *grid);
 /* plaquette_measure, nspt.cc:1316-1406 (OpenMP variant, /72V) */
 void oracle_plaquette(oracle_ctx *c, double *plaq);
 

@@ -49,6 +49,8 @@ def lib():
         L.oracle_zero_modes.argtypes = [P]
         L.oracle_fa_gauge_fix.argtypes = [P, ctypes.c_double]
         L.oracle_local_gauge_fix.argtypes = [P, ctypes.c_double]
+        L.oracle_local_gauge_fix_grid.argtypes = [P, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_local_gauge_fix_grid.restype = ctypes.c_int
         L.oracle_plaquette.argtypes = [P, D]
         for f in ("oracle_ser_mul",):
             getattr(L, f).argtypes = [ctypes.c_int, D, D, D]
@@ -151,8 +153,12 @@ class Oracle:
     def fa_gauge_fix(self, alpha: float):
         lib().oracle_fa_gauge_fix(self._h, float(alpha))
 
-    def local_gauge_fix(self, alpha: float):
-        lib().oracle_local_gauge_fix(self._h, float(alpha))
+    def local_gauge_fix(self, alpha: float, grid=(1, 1, 1, 1)):
+        """stochastic_gauge_fixing as the reference built with the OpenMP
+        thread grid (ntt, ntx, nty, ntz) runs it (nspt.cc:660-862)."""
+        g = (ctypes.c_int * 4)(*grid)
+        if lib().oracle_local_gauge_fix_grid(self._h, float(alpha), g) != 0:
+            raise ValueError("thread grid %r does not tile the lattice" % (tuple(grid),))
 
     def plaquette(self) -> np.ndarray:
         out = np.zeros((self.N + 1, 2))

@@ -51,3 +51,37 @@ def test_oracle_matches_reference_live(oracle_mod, case):
         if case["gf"] == "fa":
             o.fa_gauge_fix(case["alpha"])
     assert per_order_rel(o.links, r["links"], case["N"]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("case", [
+    dict(L=(4, 4, 4, 4), N=4, bc="pbc", grid=(2, 2, 2), zm=True),
+    dict(L=(4, 4, 4, 4), N=5, bc="tw", grid=(1, 1, 1), zm=False),
+    dict(L=(4, 4, 4, 4), N=5, bc="tw", grid=(2, 2, 1), zm=False),
+], ids=["pbc_grid222", "twisted_sequential", "twisted_grid221"])
+def test_oracle_local_gauge_fixing_matches_reference_thread_grid(oracle_mod, case):
+    """stochastic_gauge_fixing as the reference's OpenMP build with thread
+    grid (ntx, nty, ntz) runs it (nspt.cc:723-815), including the twisted
+    boundary updates (nspt.cc:665-720).  dt = 0 makes the sweep an exact
+    identity, so the per-thread noise streams of the OpenMP build do not
+    enter; what is compared is the gauge fixing (and zero modes)."""
+    O = oracle_mod
+    N, grid, alpha, steps = case["N"], case["grid"], -0.08, 2
+    b = O.ref_binary(N, case["bc"], "local", grid)
+    if not os.path.exists(b):
+        if not os.path.exists(os.path.join(REF, "nspt.cc")):
+            pytest.skip("reference sources not available")
+        b = O.build_reference(N, case["bc"], "local", grid)
+    tw = 6 if case["bc"] == "tw" else 0
+    o = O.Oracle(case["L"], N, twist_mask=tw)
+    o.random_start(17, 0.5)
+    with tempfile.TemporaryDirectory() as d:
+        O.write_config(os.path.join(d, "s.dat"), o.links, o.plaquette())
+        r = O.run_reference(b, case["L"], steps, 0.0, alpha, 3, d, start=os.path.join(d, "s.dat"),
+                            noise=False, twist_init=tw != 0)
+    zeros = np.zeros(o.V * 32)
+    for _ in range(steps):
+        o.sweep(0.0, zeros, zero_modes=case["zm"])
+        if case["zm"]:
+            o.zero_modes()
+        o.local_gauge_fix(alpha, grid=(1,) + tuple(grid))
+    assert per_order_rel(o.links, r["links"], N).max() <= 1e-12
