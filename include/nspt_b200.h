@@ -47,6 +47,8 @@ extern "C" {
 #define NSPT_TWIST_T (1u << 3)   /* twisted t boundary (choices.h:49) */
 #define NSPT_ZEROMODE (1u << 4)  /* REMOVE_GLUON_ZEROMOM (choices.h:82-84) */
 #define NSPT_GF_FA (1u << 5)     /* Fourier-accelerated gauge fixing */
+#define NSPT_GF_LOCAL (1u << 6)  /* local stochastic gauge fixing (the reference's
+                                    default without __FA_GAUGE_FIXING__) */
 
 typedef struct nspt_ctx nspt_ctx;
 
@@ -83,7 +85,8 @@ int nspt_seed(nspt_ctx *ctx, uint64_t seed, uint64_t counter);
 /* NsptEvolve (nspt.cc:953-1039) with Beat = nsteps and dt = tau_g of
  * Quench.cfg (before the /(-2 NC) of Quenched.cc:584-589): per step a
  * Jacobi Langevin sweep, then the zero-mode subtraction and the gauge
- * fixing selected at creation.  Twisted boundaries are applied on the fly
+ * fixing (NSPT_GF_FA or NSPT_GF_LOCAL, with the alpha given at creation)
+ * selected at creation.  Twisted boundaries are applied on the fly
  * (no copy sites), so twist_boundary (nspt.cc:163-255) has no separate
  * call.  gf_every > 1 gauge-fixes only every gf_every-th step (0 = never). */
 int nspt_step(nspt_ctx *ctx, double dt, int nsteps, int gf_every);
@@ -95,6 +98,20 @@ int nspt_step(nspt_ctx *ctx, double dt, int nsteps, int gf_every);
 int nspt_gauge_wilson(nspt_ctx *ctx, double dt);
 int nspt_zero_modes_subtraction(nspt_ctx *ctx);
 int nspt_fa_gauge_fixing(nspt_ctx *ctx, double alpha);
+
+/* stochastic_gauge_fixing (nspt.cc:660-862): the local, in-place gauge
+ * transformation site by site, with twisted boundaries where the context has
+ * them.  The result depends on the order of the sites, which the reference
+ * fixes by its OpenMP thread grid (ntt, ntx, nty, ntz of choices.h:124-128,
+ * blocks set up at Quenched.cc:518-531): the engine reproduces the
+ * reference built with the grid set by nspt_set_gf_grid.  The default grid
+ * is the finest one the reference accepts: blocks of 2 sites along every
+ * even extent (1 thread along odd ones).  {1,1,1,1} is the sequential sweep
+ * and runs one site at a time. */
+int nspt_local_gauge_fixing(nspt_ctx *ctx, double alpha);
+/* grid[d] threads along direction d; every L[d] % grid[d] == 0 and
+ * L[d] / grid[d] >= 2 where grid[d] > 1, else NSPT_ERR_ARG. */
+int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]);
 
 /* Observables of the last sweep, normalised as nspt.cc:570-597:
  * plaq[(N+1)*2] (/72V), norm[N] (/12V), trU[4*N*2] (/3V, mu major).

@@ -24,7 +24,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import (NSPT_GF_FA, NSPT_TWIST_T, NSPT_TWIST_Y, NSPT_TWIST_Z, NSPT_ZEROMODE,
+from ._lib import (NSPT_GF_FA, NSPT_GF_LOCAL, NSPT_TWIST_T, NSPT_TWIST_Y, NSPT_TWIST_Z, NSPT_ZEROMODE,
                    NsptError, build as build_library, check, load as load_library)
 
 __all__ = ["NsptEngine", "ptGluon_fld", "SweepObservables", "build", "series_len",
@@ -123,7 +123,7 @@ class NsptEngine:
     """
 
     def __init__(self, L, N: int, twist: str = "", zero_modes: bool = False, fa: bool = False,
-                 alpha: float = 0.0):
+                 alpha: float = 0.0, local_gf: bool = False):
         lib = load_library()
         self.L = tuple(int(x) for x in L)
         if len(self.L) != 4:
@@ -137,6 +137,8 @@ class NsptEngine:
             flags |= NSPT_ZEROMODE
         if fa:
             flags |= NSPT_GF_FA
+        if local_gf:
+            flags |= NSPT_GF_LOCAL
         self.flags = flags
         self.alpha = float(alpha)
         arr = (ctypes.c_int * 4)(*self.L)
@@ -225,6 +227,19 @@ class NsptEngine:
     def FAstochastic_gauge_fixing(self, alpha: float | None = None):
         a = self.alpha if alpha is None else float(alpha)
         self._check(load_library().nspt_fa_gauge_fixing(self._h, a), "nspt_fa_gauge_fixing")
+
+    def stochastic_gauge_fixing(self, alpha: float | None = None):
+        """Local stochastic gauge fixing (nspt.cc:660-862) with the thread grid
+        set by set_gf_grid (default: the finest the reference accepts)."""
+        a = self.alpha if alpha is None else float(alpha)
+        self._check(load_library().nspt_local_gauge_fixing(self._h, a),
+                    "nspt_local_gauge_fixing")
+
+    def set_gf_grid(self, grid):
+        """The reference's OpenMP thread grid (ntt, ntx, nty, ntz), which fixes
+        the order of the local gauge fixing (choices.h:124-128)."""
+        g = (ctypes.c_int * 4)(*[int(x) for x in grid])
+        self._check(load_library().nspt_set_gf_grid(self._h, g), "nspt_set_gf_grid")
 
     def twist_boundary(self):
         """No-op: twisted boundaries are applied inside every neighbour read,

@@ -30,6 +30,7 @@ NSPT_TWIST_Z = 1 << 2
 NSPT_TWIST_T = 1 << 3
 NSPT_ZEROMODE = 1 << 4
 NSPT_GF_FA = 1 << 5
+NSPT_GF_LOCAL = 1 << 6
 
 # every entry point the header declares: name -> (restype, argtypes)
 _P = ctypes.c_void_p
@@ -51,6 +52,8 @@ SIGNATURES = {
     "nspt_gauge_wilson": (_I, [_P, ctypes.c_double]),
     "nspt_zero_modes_subtraction": (_I, [_P]),
     "nspt_fa_gauge_fixing": (_I, [_P, ctypes.c_double]),
+    "nspt_local_gauge_fixing": (_I, [_P, ctypes.c_double]),
+    "nspt_set_gf_grid": (_I, [_P, ctypes.POINTER(ctypes.c_int)]),
     "nspt_observables": (_I, [_P, _D, _D, _D]),
     "nspt_plaquette_measure": (_I, [_P, _D]),
     "nspt_save_config": (_I, [_P, ctypes.c_char_p, _I]),

@@ -47,6 +47,7 @@ struct nspt_ctx {
   double2 *red2;  // [(N+1) + 4N + 4*9N] reduced sums
   double *red1;   // [N]
   double *p2;     // lattice momenta p2hat[4][128] of this context's extents
+  int gf_grid[4]; // local gauge fixing: the reference's thread grid (ntt, ntx, nty, ntz)
   double *noise;  // injected noise
   bool noise_pending;
   bool have_obs;
@@ -259,6 +260,50 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
   return NSPT_OK;
 }
 
+// stochastic_gauge_fixing (nspt.cc:660-862) with the context's thread
+// grid: one launch per barrier step, one group per reference thread.
+static int do_local_gf(nspt_ctx *ctx, double alpha) {
+  LgfGrid gr;
+  gr.dmax = -1;
+  gr.nthr = 1;
+  gr.seg = 1;
+  for (int d = 0; d < 4; d++) {
+    gr.n[d] = ctx->gf_grid[d];
+    gr.bs[d] = ctx->L[d] / gr.n[d];
+    gr.nthr *= gr.n[d];
+    if (gr.n[d] > 1) gr.dmax = d;
+  }
+  long steps = 1;
+  for (int d = 0; d < 4; d++) {
+    if (d <= gr.dmax)
+      steps *= gr.bs[d];
+    else
+      gr.seg *= ctx->L[d];
+  }
+  const int N = ctx->N, SS = ctx->SS;
+  const Geo geo = ctx->geo;
+  cudaStream_t st = ctx->st;
+  double2 *U = ctx->U, *Uf = ctx->Uf;
+  for (long p = 0; p < steps; p++) {
+    int rc = launch_groups(
+        ctx, (const void *)k_local_gf, 4, gr.nthr,
+        [&](unsigned g, dim3 b, size_t sm) {
+          k_local_gf<<<g, b, sm, st>>>(U, Uf, N, SS, geo, alpha, gr, p);
+        },
+        "local gauge fixing");
+    if (rc) return rc;
+  }
+  return NSPT_OK;
+}
+
+static bool grid_ok(const int L[4], const int grid[4]) {
+  for (int d = 0; d < 4; d++) {
+    if (grid[d] < 1 || L[d] % grid[d]) return false;
+    if (grid[d] > 1 && L[d] / grid[d] < 2) return false;
+  }
+  return true;
+}
+
 // ---------------- context ----------------
 
 static int upload_constants(nspt_ctx *ctx) {
@@ -310,8 +355,10 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   if (!out || !L) return NSPT_ERR_ARG;
   *out = nullptr;
   if (N < 1 || N > NSPT_MAX_ORDER) return NSPT_ERR_ORDER;
-  const unsigned known = NSPT_TWIST_Y | NSPT_TWIST_Z | NSPT_TWIST_T | NSPT_ZEROMODE | NSPT_GF_FA;
+  const unsigned known =
+      NSPT_TWIST_Y | NSPT_TWIST_Z | NSPT_TWIST_T | NSPT_ZEROMODE | NSPT_GF_FA | NSPT_GF_LOCAL;
   if (flags & ~known) return NSPT_ERR_ARG;
+  if ((flags & NSPT_GF_FA) && (flags & NSPT_GF_LOCAL)) return NSPT_ERR_ARG;
   long V = 1;
   for (int d = 0; d < 4; d++) {
     if (L[d] < 2 || L[d] > 128) return NSPT_ERR_ARG;
@@ -332,6 +379,8 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->V = V;
   ctx->U = ctx->Uf = ctx->F = ctx->Ff = ctx->Lg = ctx->Wg = ctx->Gx = nullptr;
   ctx->p2 = nullptr;
+  // finest thread grid the reference accepts: blocks of 2 sites where L is even
+  for (int d = 0; d < 4; d++) ctx->gf_grid[d] = (L[d] % 2 == 0) ? L[d] / 2 : 1;
   ctx->obs_tr = ctx->obs_tru = ctx->red2 = nullptr;
   ctx->obs_norm = ctx->red1 = ctx->noise = nullptr;
   ctx->noise_pending = false;
@@ -529,6 +578,20 @@ extern "C" int nspt_fa_gauge_fixing(nspt_ctx *ctx, double alpha) {
   return NSPT_OK;
 }
 
+extern "C" int nspt_local_gauge_fixing(nspt_ctx *ctx, double alpha) {
+  if (!ctx) return NSPT_ERR_ARG;
+  int rc = do_local_gf(ctx, alpha);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->st));
+  return NSPT_OK;
+}
+
+extern "C" int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]) {
+  if (!ctx || !grid || !grid_ok(ctx->L, grid)) return NSPT_ERR_ARG;
+  for (int d = 0; d < 4; d++) ctx->gf_grid[d] = grid[d];
+  return NSPT_OK;
+}
+
 extern "C" int nspt_step(nspt_ctx *ctx, double dt, int nsteps, int gf_every) {
   if (!ctx || nsteps < 0 || !(dt >= 0.0) || gf_every < 0) return NSPT_ERR_ARG;
   CK(cudaEventRecord(ctx->ev0, ctx->st));
@@ -541,6 +604,8 @@ extern "C" int nspt_step(nspt_ctx *ctx, double dt, int nsteps, int gf_every) {
       if ((rc = do_zero_modes(ctx))) return rc;
     if ((ctx->flags & NSPT_GF_FA) && gf_every > 0 && ((ctx->counter % gf_every) == 0))
       if ((rc = do_fa(ctx, ctx->alpha))) return rc;
+    if ((ctx->flags & NSPT_GF_LOCAL) && gf_every > 0 && ((ctx->counter % gf_every) == 0))
+      if ((rc = do_local_gf(ctx, ctx->alpha))) return rc;
   }
   CK(cudaEventRecord(ctx->ev1, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));

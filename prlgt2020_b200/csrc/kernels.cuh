@@ -76,9 +76,16 @@ __device__ __forceinline__ Nb neighbour(const Geo &g, const int *x, int d1, int 
 // Copy link (mu, n.site) from the row-major planes into a column-major slot
 // (DAG: store its dagger), applying the twists of the faces the read crossed.
 // Twisted links get flag 1 (twist_* returns a default flag, nspt.cc:115-121).
-__device__ __forceinline__ void stage(double2 *slot, const double2 *__restrict__ U,
-                                      const double2 *__restrict__ Uf, int mu, Nb n,
-                                      const Geo &g, int N, const Lane &L, bool dag = false) {
+// RW: the field is being updated by the same kernel -- coherent (L2) loads
+// instead of the read-only path.
+template <bool RW>
+__device__ __forceinline__ double2 ld_link(const double2 *p) {
+  return RW ? __ldcg(p) : __ldg(p);
+}
+
+template <bool RW = false>
+__device__ __forceinline__ void stage(double2 *slot, const double2 *U, const double2 *Uf, int mu,
+                                      Nb n, const Geo &g, int N, const Lane &L, bool dag = false) {
   const size_t V = (size_t)g.V;
   const double2 *src = U + (size_t)mu * 9 * N * V + n.site;
   const unsigned tb = n.bwd & g.twist, tf = n.fwd & g.twist;
@@ -87,18 +94,18 @@ __device__ __forceinline__ void stage(double2 *slot, const double2 *__restrict__
     const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
     const int off = dag ? 3 * r + c : 3 * c + r;
     for (int k = 1; k <= N; k++) {
-      const double2 v = __ldg(src + (size_t)(9 * (k - 1) + L.j) * V);
+      const double2 v = ld_link<RW>(src + (size_t)(9 * (k - 1) + L.j) * V);
       slot[1 + 9 * (k - 1) + off] = dag ? cconj(v) : v;
     }
     if (L.j == 0) {
-      const double2 f = __ldg(Uf + (size_t)mu * V + n.site);
+      const double2 f = ld_link<RW>(Uf + (size_t)mu * V + n.site);
       slot[0] = dag ? cconj(f) : f;
     }
   } else {
     for (int k = 1 + L.j; k <= N; k += GROUP) {
       double2 m[9];
 #pragma unroll
-      for (int e = 0; e < 9; e++) m[e] = __ldg(src + (size_t)(9 * (k - 1) + e) * V);
+      for (int e = 0; e < 9; e++) m[e] = ld_link<RW>(src + (size_t)(9 * (k - 1) + e) * V);
       twist3(m, tb, tf);
       double2 *p = slot + 1 + 9 * (k - 1);
 #pragma unroll
@@ -515,6 +522,165 @@ __global__ void __launch_bounds__(256, 1)
     if (valid) dst[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
   });
   if (L.j == 0 && valid) Ff[(size_t)mu * V + site] = cmul(tflag, one);
+}
+
+// ---------------- local stochastic gauge fixing ----------------
+
+// Thread grid of the reference's OpenMP build (choices.h:124-128): n[d]
+// threads along direction d (ntt, ntx, nty, ntz), blocks of bs[d] sites
+// (Quenched.cc:518-531).  Threads take a barrier after every iteration of
+// the deepest split direction dmax (nspt.cc:796-815); between two barriers a
+// thread walks a segment of seg sites.
+struct LgfGrid {
+  int n[4], bs[4];
+  int dmax;   // -1 when no direction is split
+  int nthr;
+  long seg;
+};
+
+// A <- A - A^dag, then Trless (W -= dag(W); W.Trless(), nspt.cc:679-682,
+// QCDpt.cc:124-136 and 185-194): flag 0.  Lanes split the orders.
+__device__ __forceinline__ void ser_aherm_trless(double2 *P, int N, const Lane &L) {
+  const double D3 = 1.0 / 3.0;
+  for (int k = 1 + L.j; k <= N; k += GROUP) {
+    double2 *m = P + 1 + 9 * (k - 1);
+    double2 a[9], b[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) a[e] = m[e];
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int q = 0; q < 3; q++) b[3 * r + q] = csub(a[3 * r + q], cconj(a[3 * q + r]));
+    const double2 tr = cadd(cadd(b[0], b[4]), b[8]);
+    const double2 z = make_double2(D3 * tr.x, D3 * tr.y);
+    b[0] = csub(b[0], z);
+    b[4] = csub(b[4], z);
+    b[8] = csub(b[8], z);
+#pragma unroll
+    for (int e = 0; e < 9; e++) m[e] = b[e];
+  }
+  if (L.j == 0) P[0] = cz();
+  __syncwarp(L.mask);
+}
+
+// One barrier step of stochastic_gauge_fixing (nspt.cc:660-862), in place:
+// one group per reference thread, walking its segment site by site.  Sites
+// of different groups are >= 2 apart and share no link, so the result is
+// the reference's with the same thread grid.  Per site: W = sum_mu U_mu(x) -
+// U_mu(x-mu) (twisted read across a twisted face), W -= W^dag, Trless,
+// U_mu(x) <- exp(alpha W) U_mu(x), U_mu(x-mu) <- U_mu(x-mu) exp(-alpha W)
+// (twist_mu(exp(-alpha W)) = Omega W2 Omega^dag when x-mu wraps a twisted
+// face, nspt.cc:690-719).  Four slots per group.
+__global__ void __launch_bounds__(256, 1)
+    k_local_gf(double2 *U, double2 *Uf, int N, int SS, Geo geo, double alpha, LgfGrid gr,
+               long step) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long tid = ((long)blockIdx.x * nw + warp) * LPW + g;
+  if (tid >= gr.nthr) return;
+  double2 *A = sm + (size_t)(warp * LPW + g) * 4 * SS, *Y2 = A + SS, *E1 = Y2 + SS, *E2 = E1 + SS;
+  const size_t V = (size_t)geo.V;
+  const size_t plane = (size_t)9 * N * V;
+  const int c = L.c;
+  const double2 one = make_double2(1.0, 0.0);
+  int b[4];
+  b[0] = (int)(tid / ((long)gr.n[1] * gr.n[2] * gr.n[3]));
+  b[1] = (int)((tid / ((long)gr.n[2] * gr.n[3])) % gr.n[1]);
+  b[2] = (int)((tid / gr.n[3]) % gr.n[2]);
+  b[3] = (int)(tid % gr.n[3]);
+  int rel[4] = {0, 0, 0, 0};
+  {
+    long q = step;
+    for (int d = gr.dmax; d >= 0; d--) {
+      rel[d] = (int)(q % gr.bs[d]);
+      q /= gr.bs[d];
+    }
+  }
+  for (long r = 0; r < gr.seg; r++) {
+    int x[4];
+    long t = r;
+    for (int d = 3; d >= 0; d--) {
+      if (d <= gr.dmax) {
+        x[d] = gr.bs[d] * b[d] + rel[d];
+      } else {
+        x[d] = (int)(t % geo.L[d]);
+        t /= geo.L[d];
+      }
+    }
+    Nb self;
+    self.site = x[0] * geo.s0 + x[1] * geo.s1 + x[2] * geo.s2 + x[3];
+    self.fwd = self.bwd = 0;
+    // W = sum_mu U_mu(x) - U_mu(x-mu)  (nspt.cc:672-675)
+    for (int mu = 0; mu < 4; mu++) {
+      stage<true>(Y2, U, Uf, mu, self, geo, N, L);
+      stage<true>(E1, U, Uf, mu, neighbour(geo, x, mu, -1), geo, N, L);
+      for (int e = L.j; e < 1 + 9 * N; e += GROUP)
+        A[e] = cadd(mu == 0 ? cz() : A[e], csub(Y2[e], E1[e]));
+      __syncwarp(L.mask);
+    }
+    ser_aherm_trless(A, N, L);
+    for (int e = L.j; e < 1 + 9 * N; e += GROUP) A[e] = cscale(A[e], alpha);
+    __syncwarp(L.mask);
+    // E1 = exp(alpha W), E2 = exp(-alpha W), sharing (alpha W)^2
+    ser_square<MO>(A, Y2, N, L);
+    ser_horner2<MO>(A, Y2, E1, N, L, [](int n) { return inv_factorial(n); },
+                    [&](int k, int rr, double2 v) { E1[sidx(k, rr, c)] = v; });
+    ser_horner2<MO>(A, Y2, E2, N, L,
+                    [](int n) { return (n & 1) ? -inv_factorial(n) : inv_factorial(n); },
+                    [&](int k, int rr, double2 v) { E2[sidx(k, rr, c)] = v; });
+    if (L.j == 0) E1[0] = E2[0] = one;
+    __syncwarp(L.mask);
+    for (int mu = 0; mu < 4; mu++) {
+      // U_mu(x) <- E1 U_mu(x)
+      stage<true>(Y2, U, Uf, mu, self, geo, N, L);
+      {
+        double2 *dst = U + mu * plane + self.site;
+        const double2 yf = Y2[0];
+        product<MO, false>(LeftS{E1}, one, Y2, yf, N, L, [&](int k, int rr, double2 v) {
+          dst[(size_t)(9 * (k - 1) + 3 * rr + c) * V] = v;
+        });
+        if (L.j == 0) Uf[(size_t)mu * V + self.site] = flag_mul(one, yf);
+      }
+      // U_mu(x-mu) <- U_mu(x-mu) E2
+      const Nb back = neighbour(geo, x, mu, -1);
+      Nb at;
+      at.site = back.site;
+      at.fwd = at.bwd = 0;
+      stage<true>(A, U, Uf, mu, at, geo, N, L);
+      const double2 *R = E2;
+      if ((back.bwd & geo.twist) >> mu & 1u) {
+        for (int k = 1 + L.j; k <= N; k += GROUP) {
+          const double2 *src = E2 + 1 + 9 * (k - 1);
+          double2 m[9];
+#pragma unroll
+          for (int rr = 0; rr < 3; rr++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) m[3 * rr + q] = src[3 * q + rr];
+          twist3(m, 0u, 1u << mu);
+          double2 *o = Y2 + 1 + 9 * (k - 1);
+#pragma unroll
+          for (int rr = 0; rr < 3; rr++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) o[3 * q + rr] = m[3 * rr + q];
+        }
+        if (L.j == 0) Y2[0] = one;  // twist_* returns flag VACUUM
+        __syncwarp(L.mask);
+        R = Y2;
+      }
+      {
+        double2 *dst = U + mu * plane + back.site;
+        const double2 af = A[0], rf = R[0];
+        product<MO, false>(LeftS{A}, af, R, rf, N, L, [&](int k, int rr, double2 v) {
+          dst[(size_t)(9 * (k - 1) + 3 * rr + c) * V] = v;
+        });
+        if (L.j == 0) Uf[(size_t)mu * V + back.site] = flag_mul(af, rf);
+      }
+      __syncwarp(L.mask);
+    }
+  }
 }
 
 // Wg(x) = sum_mu [log U_mu(x) - log U_mu(x-mu)]  (nspt.cc:871-877)

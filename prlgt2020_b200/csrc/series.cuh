@@ -254,13 +254,19 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
 // 1 + N/2 series products of sizes 2, 4, ..., N instead of N products of
 // sizes 1..N (1354 instead of 2300 3x3 products at N = 24).  The last step
 // goes to last(k, r, v) instead of S.  X, Y and S are slots.
-template <int MO, class Coef, class Last>
-__device__ __forceinline__ void ser_poly2(const double2 *X, double2 *Y, double2 *S, int N,
-                                          const Lane &L, Coef coef, Last last) {
+template <int MO>
+__device__ __forceinline__ void ser_square(const double2 *X, double2 *Y, int N, const Lane &L) {
   const int c = L.c;
   // Y = X X (order 1 comes out as an exact zero)
   product<MO, false>(LeftS{X}, cz(), X, cz(), N, L,
                      [&](int k, int r, double2 v) { Y[sidx(k, r, c)] = v; });
+}
+
+// The Horner part of ser_poly2, for a Y = X^2 already formed.
+template <int MO, class Coef, class Last>
+__device__ __forceinline__ void ser_horner2(const double2 *X, const double2 *Y, double2 *S, int N,
+                                            const Lane &L, Coef coef, Last last) {
+  const int c = L.c;
   const int J = N / 2;
   // S_J = coef(2J) + coef(2J+1) X to order N - 2J; higher orders zero (they
   // meet Y's zero order-1 coefficient and must be finite)
@@ -299,6 +305,13 @@ __device__ __forceinline__ void ser_poly2(const double2 *X, double2 *Y, double2 
       });
     }
   }
+}
+
+template <int MO, class Coef, class Last>
+__device__ __forceinline__ void ser_poly2(const double2 *X, double2 *Y, double2 *S, int N,
+                                          const Lane &L, Coef coef, Last last) {
+  ser_square<MO>(X, Y, N, L);
+  ser_horner2<MO>(X, Y, S, N, L, coef, last);
 }
 
 __device__ __forceinline__ double inv_factorial(int n) {

@@ -136,8 +136,7 @@ def test_twisted_boundaries(engine_mod, oracle_mod, twist, N):
 def test_reference_golden_fixture(engine_mod, oracle_mod, path):
     """The engine replays each fixture the reference's own code produced."""
     g = np.load(path)
-    if bool(g["local_gf"]):
-        pytest.skip("sequential local gauge fixing has no parallel counterpart")
+    local_gf = bool(g["local_gf"])
     L = tuple(int(x) for x in g["L"])
     N = int(g["N"])
     twist = "yz" if bool(g["twisted"]) else ""
@@ -146,6 +145,8 @@ def test_reference_golden_fixture(engine_mod, oracle_mod, path):
                      start=int(g["start"]) if int(g["start"]) >= 0 else None)
     ok, w = obs_close(e.plaquette_measure(), g["plaq0"], 1e-12)
     assert ok, ("start plaquette", w)
+    if local_gf:
+        e.set_gf_grid((1, 1, 1, 1))  # the fixture's reference build runs one thread
     rng = oracle_mod.Rand55(int(g["seed"]))
     for s in range(int(g["steps"])):
         nz = rng.gauss(o.V * 32)
@@ -158,6 +159,8 @@ def test_reference_golden_fixture(engine_mod, oracle_mod, path):
             e.zero_modes_subtraction()
         if fa:
             e.FAstochastic_gauge_fixing(alpha)
+        if local_gf:
+            e.stochastic_gauge_fixing(alpha)
     rel = per_order_rel(e.download()[: g["links"].shape[0]], g["links"], N)
     bound = cold_bound(N, 1e-11) if (zm and int(g["start"]) < 0) else 1e-11
     assert np.all(rel <= bound), rel
@@ -239,3 +242,56 @@ def test_two_contexts_with_different_extents_interleaved(engine_mod, oracle_mod)
             check_obs(eo, oo, 1e-11)
     for (e, o), (L, N, _, _) in zip(pairs, cases):
         assert per_order_rel(e.download(), o.links, N).max() <= 1e-11
+
+
+@pytest.mark.parametrize("L,N,twist,grid", [
+    ((4, 4, 4, 4), 4, "", (1, 1, 1, 1)),
+    ((4, 4, 4, 4), 6, "", (2, 2, 2, 2)),
+    ((4, 6, 4, 4), 5, "", (1, 3, 1, 2)),
+    ((4, 4, 4, 4), 5, "yz", (1, 2, 2, 1)),
+    ((4, 4, 4, 4), 12, "yzt", (2, 1, 2, 2)),
+], ids=["sequential", "grid2222", "grid1312_6x", "twisted_yz_grid1221", "twisted_yzt_n12"])
+def test_local_gauge_fixing_matches_oracle_thread_grid(engine_mod, oracle_mod, L, N, twist, grid):
+    """stochastic_gauge_fixing in the order the reference's OpenMP thread grid
+    fixes (the oracle is pinned to the reference's builds of those grids)."""
+    e, o = make_pair(engine_mod, oracle_mod, L, N, twist=twist, start=61)
+    alpha = -0.08
+    e.set_gf_grid(grid)
+    for _ in range(2):
+        e.stochastic_gauge_fixing(alpha)
+        o.local_gauge_fix(alpha, grid=grid)
+    rel = per_order_rel(e.download(), o.links, N)
+    assert rel.max() <= 1e-12, rel
+    assert flag_diff(e.download(), o.links, N) == 0.0
+
+
+def test_local_gauge_fixing_in_the_step_with_default_grid(engine_mod, oracle_mod):
+    """nspt_step with NSPT_GF_LOCAL: sweep, zero modes, local gauge fixing;
+    the default grid is the finest the reference accepts (blocks of 2)."""
+    P, O = engine_mod, oracle_mod
+    L, N, alpha = (4, 4, 2, 4), 6, -0.05
+    o = O.Oracle(L, N)
+    o.random_start(71, 0.5)
+    e = P.NsptEngine(L, N, zero_modes=True, local_gf=True, alpha=alpha)
+    e.upload(o.links)
+    rng = O.Rand55(5)
+    for _ in range(2):
+        nz = rng.gauss(o.V * 32)
+        e.set_noise(nz)
+        e.NsptEvolve(0.01, 1, 1)
+        oo = o.sweep(0.01, nz, zero_modes=True)
+        o.zero_modes()
+        o.local_gauge_fix(alpha, grid=(2, 2, 1, 2))
+        check_obs(e.observables(), oo, 1e-11)
+    assert per_order_rel(e.download(), o.links, N).max() <= 1e-11
+
+
+def test_gf_grid_rejects_what_the_reference_rejects(engine_mod):
+    P = engine_mod
+    with P.NsptEngine((4, 6, 4, 4), 3) as e:
+        for bad in [(3, 1, 1, 1), (1, 6, 1, 1), (0, 1, 1, 1)]:
+            with pytest.raises(P.NsptError):
+                e.set_gf_grid(bad)
+        e.set_gf_grid((2, 3, 2, 2))
+    with pytest.raises(P.NsptError):
+        P.NsptEngine((4, 4, 4, 4), 3, fa=True, local_gf=True)
