@@ -32,6 +32,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "Langevin sweeps/s at 32^4 x 24 orders (FP64, twisted y,z)"
+GF_ALPHA = -0.05
 
 
 def canonical_flops_per_link(N: int) -> float:
@@ -258,7 +259,9 @@ def run_ours(args, world, rank, local):
     lib = _lib.load()
     peak = P.fp64_peak_tflops()
 
-    eng = P.NsptEngine(L, N, twist="yz")
+    # local gauge fixing (the reference's default with twisted boundaries) is
+    # enabled for the secondary "with_gf" figure; the headline sweeps skip it
+    eng = P.NsptEngine(L, N, twist="yz", local_gf=True, alpha=GF_ALPHA)
     eng.seed(replica_seed(1000, rank), 0)
     eng.cold_start()
 
@@ -268,15 +271,31 @@ def run_ours(args, world, rank, local):
     with ClockSampler(local) as clk:
         eng.NsptEvolve(args.dt, args.steps, 0)
         ms = eng.last_step_ms()
+        kernel_ms = eng.last_kernel_ms()
     barrier(world)
     clocks = clk.summary()
     ms_max = max_over_ranks(ms)
     ms_step = ms_max / args.steps
     value = whole_job_rate(args.steps, world, ms_max * 1e-3)
 
-    # roofline of the dominant kernel (the sweep): canonical flops / sweep time
+    # roofline of the dominant kernel (the sweep): canonical flops / the
+    # average duration of one sweep-kernel launch (CUDA events on its stream)
     flops = canonical_flops_per_link(N) * 4 * V
-    achieved = flops / (ms_step * 1e-3) / 1e12
+    kernel_ms = max_over_ranks(kernel_ms)
+    achieved = flops / (kernel_ms * 1e-3) / 1e12
+
+    # the workload's full step: local gauge fixing every 10 sweeps
+    if args.no_gf:
+        with_gf = None
+    else:
+        barrier(world)
+        eng.NsptEvolve(args.dt, 10, 10)
+        gf_ms = max_over_ranks(eng.last_step_ms())
+        eng.stochastic_gauge_fixing()
+        pass_ms = max_over_ranks(eng.last_step_ms())
+        with_gf = {"value": whole_job_rate(10, world, gf_ms * 1e-3), "unit": "sweeps/s",
+                   "gf_every": 10, "gf": "local stochastic (nspt.cc:660-862), finest thread grid",
+                   "alpha": GF_ALPHA, "ms_per_10_steps": gf_ms, "gf_pass_ms": pass_ms}
 
     # end to end through the C ABI with the configuration on the host
     field_bytes = V * 4 * P.series_len(N) * 8
@@ -304,6 +323,7 @@ def run_ours(args, world, rank, local):
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": read_profile_traffic(),
+                         "kernel": "k_sweep", "kernel_ms": kernel_ms,
                          "peak_source": "FP64 FMA microbenchmark on this GPU "
                                         "(nspt_measure_fp64_peak); MEASURED_PEAKS.json has no FP64 entry",
                          "flops_per_sweep": flops,
@@ -311,6 +331,7 @@ def run_ours(args, world, rank, local):
                          "hbm_gbs_equiv": algorithmic_bytes_per_sweep(V, N) / (ms_step * 1e-3) / 1e9},
             "clocks": clocks,
             "e2e": e2e,
+            "with_gf": with_gf,
             "gpu_launches": 4 * args.steps,
             "cpu_baseline": cpu,
         }
@@ -320,6 +341,69 @@ def run_ours(args, world, rank, local):
         import torch.distributed as dist
         dist.barrier()
         dist.destroy_process_group()
+
+
+def run_c2(args, world, rank, local):
+    """16^4 x 20 orders, periodic, every step: sweep (with the per-link log
+    the zero modes need), zero-mode subtraction, FA gauge fixing.  Each pass
+    is timed on the device and set against its own roofline: canonical
+    FP64 work for the series passes (the per-link log is in the sweep, one
+    exp per link in the zero modes, a log, 1/4 exp and 2 products per link
+    plus the FFTs in FA), HBM bytes for the FFT-dominated FA pass."""
+    import numpy as np
+    import torch
+
+    import prlgt2020_b200 as P
+    from prlgt2020_b200.replicas import max_over_ranks, replica_seed, whole_job_rate
+    torch.cuda.set_device(local)
+    L, N, alpha, dt = (16, 16, 16, 16), 20, -0.05, 0.01
+    V = int(np.prod(L))
+    peak = P.fp64_peak_tflops()
+    eng = P.NsptEngine(L, N, zero_modes=True, fa=True, alpha=alpha)
+    eng.seed(replica_seed(2000, rank), 0)
+    eng.NsptEvolve(dt, args.warmup, 1)
+    sweep = zm = fa = kern = 0.0
+    for _ in range(args.steps):
+        eng.gauge_wilson(dt)
+        sweep += eng.last_step_ms()
+        kern += eng.last_kernel_ms()
+        eng.zero_modes_subtraction()
+        zm += eng.last_step_ms()
+        eng.FAstochastic_gauge_fixing(alpha)
+        fa += eng.last_step_ms()
+    eng.NsptEvolve(dt, args.steps, 1)
+    step_ms = max_over_ranks(eng.last_step_ms()) / args.steps
+    K = args.steps
+    sweep, zm, fa, kern = (max_over_ranks(x) / K for x in (sweep, zm, fa, kern))
+    Pn = N * (N - 1) // 2
+    E = (N - 1) * N * (N + 1) // 6
+    f_sweep = (14 * Pn + 2 * E) * 216.0 * 4 * V          # + the per-link log
+    f_zm = E * 216.0 * 4 * V
+    f_fa = (E + 0.25 * E + 2 * Pn) * 216.0 * 4 * V
+    fft_flops = 2 * (9 * N + 1) * 5 * V * np.log2(V)
+    fft_bytes = 2 * 4 * (9 * N + 1) * 16 * V              # 2 FFTs x 4 axis passes, read + write
+    if rank == 0:
+        tf = lambda f, ms: f / (ms * 1e-3) / 1e12
+        line = {
+            "metric": "Langevin steps/s at 16^4 x 20 orders (FP64, ZM + FA every step)",
+            "value": whole_job_rate(1, world, step_ms * 1e-3), "unit": "steps/s",
+            "n_gpus": world, "steps": K, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (cold start + warm-up sweeps, device Philox noise)",
+            "config": {"workload": "c2_16^4_N20_zm_fa", "L": list(L), "N": N, "dt": dt,
+                       "alpha": alpha, "bc": "periodic"},
+            "passes": {
+                "sweep": {"ms": sweep, "kernel_ms": kern, "tflops": tf(f_sweep, kern),
+                          "frac_fp64": tf(f_sweep, kern) / peak},
+                "zero_modes": {"ms": zm, "tflops": tf(f_zm, zm), "frac_fp64": tf(f_zm, zm) / peak},
+                "fa_gauge_fixing": {"ms": fa, "tflops": tf(f_fa + fft_flops, fa),
+                                    "frac_fp64": tf(f_fa + fft_flops, fa) / peak,
+                                    "fft_hbm_gbs_equiv": fft_bytes / (fa * 1e-3) / 1e9},
+            },
+            "fp64_peak_tflops": peak,
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
 
 
 def main():
@@ -333,10 +417,17 @@ def main():
     ap.add_argument("--dt", type=float, default=0.005)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--no-gf", action="store_true", help="skip the gauge-fixing figure")
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "c2"],
+                    help="sweep: 32^4 x 24 twisted (the headline); c2: 16^4 x 20 periodic "
+                         "with zero modes and FA gauge fixing every step, per pass")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference_arm(args, world, rank)
+        return
+    if args.workload == "c2":
+        run_c2(args, world, rank, local)
         return
     run_ours(args, world, rank, local)
 

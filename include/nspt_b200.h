@@ -129,9 +129,15 @@ int nspt_save_config(nspt_ctx *ctx, const char *path, int allocORD);
 int nspt_load_config(nspt_ctx *ctx, const char *path, int allocORD,
                      double *plaq_trailer);
 
-/* Wall time of the last nspt_step / sweep call on the device (CUDA events on
- * the context's stream), milliseconds. */
+/* Device time of the last nspt_step, nspt_gauge_wilson,
+ * nspt_zero_modes_subtraction, nspt_fa_gauge_fixing or
+ * nspt_local_gauge_fixing call (CUDA events on the context's stream around
+ * all of its launches), milliseconds. */
 double nspt_last_step_ms(const nspt_ctx *ctx);
+/* Average device time of one sweep-kernel launch in the last nspt_step or
+ * nspt_gauge_wilson call (CUDA events around each of the first 64
+ * launches), milliseconds: the duration the sweep's roofline divides by. */
+double nspt_last_kernel_ms(const nspt_ctx *ctx);
 
 /* Measured FP64 FMA throughput of the current device (independent FMA
  * chains on every SM), TFLOP/s.  Roofline denominator for the sweep. */

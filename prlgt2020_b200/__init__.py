@@ -266,4 +266,9 @@ class NsptEngine:
         return SweepObservables(plaq, norm, tru)
 
     def last_step_ms(self) -> float:
+        """Device time of the last step / sweep / zero-mode / gauge-fixing call."""
         return float(load_library().nspt_last_step_ms(self._h))
+
+    def last_kernel_ms(self) -> float:
+        """Average sweep-kernel launch of the last NsptEvolve / gauge_wilson."""
+        return float(load_library().nspt_last_kernel_ms(self._h))

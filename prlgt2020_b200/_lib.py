@@ -59,6 +59,7 @@ SIGNATURES = {
     "nspt_save_config": (_I, [_P, ctypes.c_char_p, _I]),
     "nspt_load_config": (_I, [_P, ctypes.c_char_p, _I, _D]),
     "nspt_last_step_ms": (ctypes.c_double, [_P]),
+    "nspt_last_kernel_ms": (ctypes.c_double, [_P]),
     "nspt_measure_fp64_peak": (_I, [_D]),
     "nspt_plaquette_measure_noalloc": (_I, [ctypes.c_void_p, _I, ctypes.POINTER(ctypes.c_int), _I,
                                            ctypes.c_uint, _D, ctypes.c_void_p]),

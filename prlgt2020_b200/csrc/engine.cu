@@ -37,6 +37,11 @@ struct nspt_ctx {
   cudaStream_t st;
   cudaEvent_t ev0, ev1;
   float last_ms;
+  // CUDA events around the first KEV sweep-kernel launches of a call
+  static constexpr int KEV = 64;
+  cudaEvent_t kev[2 * KEV];
+  int kcount;
+  double last_kernel_ms;  // average sweep-kernel launch of the last call
   Geo geo;
   int SS;  // slot stride (double2)
   double2 *U, *Uf, *F, *Ff;
@@ -173,8 +178,14 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   a.N = ctx->N;
   a.SS = ctx->SS;
   a.g = ctx->geo;
+  const bool timed = ctx->kcount < nspt_ctx::KEV;
+  if (timed) CK(cudaEventRecord(ctx->kev[2 * ctx->kcount], ctx->st));
   int rc = launch_sweep(ctx, a, false);
   if (rc) return rc;
+  if (timed) {
+    CK(cudaEventRecord(ctx->kev[2 * ctx->kcount + 1], ctx->st));
+    ctx->kcount++;
+  }
   rc = reduce_sweep_obs(ctx);
   if (rc) return rc;
   std::swap(ctx->U, ctx->F);
@@ -417,6 +428,9 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return fail(NSPT_ERR_CUDA);
   cudaEventCreate(&ctx->ev0);
   cudaEventCreate(&ctx->ev1);
+  for (int i = 0; i < 2 * nspt_ctx::KEV; i++) cudaEventCreate(&ctx->kev[i]);
+  ctx->kcount = 0;
+  ctx->last_kernel_ms = 0.0;
   const size_t field = (size_t)4 * 9 * N * V * sizeof(double2);
   const size_t flagb = (size_t)4 * V * sizeof(double2);
   const size_t nl = (size_t)4 * V;
@@ -452,6 +466,7 @@ extern "C" int nspt_destroy(nspt_ctx *ctx) {
   free_all(ctx);
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
+  for (int i = 0; i < 2 * nspt_ctx::KEV; i++) cudaEventDestroy(ctx->kev[i]);
   cudaStreamDestroy(ctx->st);
   delete ctx;
   return NSPT_OK;
@@ -547,43 +562,58 @@ extern "C" int nspt_seed(nspt_ctx *ctx, uint64_t seed, uint64_t counter) {
   return NSPT_OK;
 }
 
-extern "C" int nspt_gauge_wilson(nspt_ctx *ctx, double dt) {
-  if (!ctx || !(dt >= 0.0)) return NSPT_ERR_ARG;
+// Device time of a call: events on the context's stream around its launches.
+static int timed_begin(nspt_ctx *ctx) {
+  ctx->kcount = 0;
   CK(cudaEventRecord(ctx->ev0, ctx->st));
-  const bool use = ctx->noise_pending;
-  int rc = do_sweep(ctx, dt, use);
-  ctx->noise_pending = false;
-  if (rc) return rc;
+  return NSPT_OK;
+}
+static int timed_end(nspt_ctx *ctx) {
   CK(cudaEventRecord(ctx->ev1, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
   cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1);
+  double sum = 0.0;
+  for (int i = 0; i < ctx->kcount; i++) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, ctx->kev[2 * i], ctx->kev[2 * i + 1]);
+    sum += ms;
+  }
+  ctx->last_kernel_ms = ctx->kcount ? sum / ctx->kcount : 0.0;
   return NSPT_OK;
+}
+
+extern "C" int nspt_gauge_wilson(nspt_ctx *ctx, double dt) {
+  if (!ctx || !(dt >= 0.0)) return NSPT_ERR_ARG;
+  int rc = timed_begin(ctx);
+  if (rc) return rc;
+  const bool use = ctx->noise_pending;
+  rc = do_sweep(ctx, dt, use);
+  ctx->noise_pending = false;
+  if (rc) return rc;
+  return timed_end(ctx);
 }
 
 extern "C" int nspt_zero_modes_subtraction(nspt_ctx *ctx) {
   if (!ctx) return NSPT_ERR_ARG;
   if (!(ctx->flags & NSPT_ZEROMODE) || !ctx->have_obs) return NSPT_ERR_STATE;
-  int rc = do_zero_modes(ctx);
-  if (rc) return rc;
-  CK(cudaStreamSynchronize(ctx->st));
-  return NSPT_OK;
+  int rc = timed_begin(ctx);
+  if (rc || (rc = do_zero_modes(ctx))) return rc;
+  return timed_end(ctx);
 }
 
 extern "C" int nspt_fa_gauge_fixing(nspt_ctx *ctx, double alpha) {
   if (!ctx) return NSPT_ERR_ARG;
   if (!(ctx->flags & NSPT_GF_FA)) return NSPT_ERR_STATE;
-  int rc = do_fa(ctx, alpha);
-  if (rc) return rc;
-  CK(cudaStreamSynchronize(ctx->st));
-  return NSPT_OK;
+  int rc = timed_begin(ctx);
+  if (rc || (rc = do_fa(ctx, alpha))) return rc;
+  return timed_end(ctx);
 }
 
 extern "C" int nspt_local_gauge_fixing(nspt_ctx *ctx, double alpha) {
   if (!ctx) return NSPT_ERR_ARG;
-  int rc = do_local_gf(ctx, alpha);
-  if (rc) return rc;
-  CK(cudaStreamSynchronize(ctx->st));
-  return NSPT_OK;
+  int rc = timed_begin(ctx);
+  if (rc || (rc = do_local_gf(ctx, alpha))) return rc;
+  return timed_end(ctx);
 }
 
 extern "C" int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]) {
@@ -594,7 +624,8 @@ extern "C" int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]) {
 
 extern "C" int nspt_step(nspt_ctx *ctx, double dt, int nsteps, int gf_every) {
   if (!ctx || nsteps < 0 || !(dt >= 0.0) || gf_every < 0) return NSPT_ERR_ARG;
-  CK(cudaEventRecord(ctx->ev0, ctx->st));
+  int rc0 = timed_begin(ctx);
+  if (rc0) return rc0;
   for (int s = 0; s < nsteps; s++) {
     const bool use = ctx->noise_pending;
     int rc = do_sweep(ctx, dt, use);
@@ -607,13 +638,13 @@ extern "C" int nspt_step(nspt_ctx *ctx, double dt, int nsteps, int gf_every) {
     if ((ctx->flags & NSPT_GF_LOCAL) && gf_every > 0 && ((ctx->counter % gf_every) == 0))
       if ((rc = do_local_gf(ctx, ctx->alpha))) return rc;
   }
-  CK(cudaEventRecord(ctx->ev1, ctx->st));
-  CK(cudaStreamSynchronize(ctx->st));
-  cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1);
-  return NSPT_OK;
+  return timed_end(ctx);
 }
 
 extern "C" double nspt_last_step_ms(const nspt_ctx *ctx) { return ctx ? ctx->last_ms : 0.0; }
+extern "C" double nspt_last_kernel_ms(const nspt_ctx *ctx) {
+  return ctx ? ctx->last_kernel_ms : 0.0;
+}
 
 extern "C" int nspt_observables(nspt_ctx *ctx, double *plaq, double *norm, double *trU) {
   if (!ctx) return NSPT_ERR_ARG;
