@@ -406,6 +406,84 @@ def run_c2(args, world, rank, local):
     eng.close()
 
 
+def run_c4(args, world, rank, local):
+    """64 independent replicas, 12 orders, periodic, zero modes + FA gauge
+    fixing every step: replica r has L = {6,8,10}[r mod 3]^4, dt =
+    {0.005,0.01,0.02}[(r/3) mod 3], seed = 3000 + r.  Batched: all replicas
+    in one CUDA graph per 2 steps (nspt_batch_step), sweep shape picked by
+    the autotuner.  Plain: the same replicas advanced one after the other
+    with nspt_step, as one process per lattice would.  The unit is replica
+    steps per second; the plaquette series are averaged per dt for the
+    dt -> 0 extrapolation."""
+    import numpy as np
+    import torch
+
+    import prlgt2020_b200 as P
+    from prlgt2020_b200.replicas import max_over_ranks, replica_seed, whole_job_rate
+    torch.cuda.set_device(local)
+    nrep, N, alpha = 64, 12, -0.05
+    Ls = [(v,) * 4 for v in (6, 8, 10) for _ in range(1)]
+    L = [Ls[r % 3] for r in range(nrep)]
+    dts = [(0.005, 0.01, 0.02)[(r // 3) % 3] for r in range(nrep)]
+    seeds = [replica_seed(3000 + r, rank) for r in range(nrep)]
+    K = max(2, args.steps - args.steps % 2)
+    kw = dict(zero_modes=True, fa=True, alpha=alpha)
+    # plain: one replica after another, each its own launches and syncs
+    plain = [P.NsptEngine(l, N, **kw) for l in L]
+    for e, sd, dt in zip(plain, seeds, dts):
+        e.seed(sd, 0)
+        e.NsptEvolve(dt, args.warmup, 1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for e, dt in zip(plain, dts):
+        e.NsptEvolve(dt, K, 1)
+    torch.cuda.synchronize()
+    plain_s = max_over_ranks(time.perf_counter() - t0)
+    for e in plain:
+        e.close()
+    # batched
+    b = P.NsptBatch(L, N, dts, seeds, **kw)
+    warps = b.tune(1)
+    b.step(max(2, args.warmup - args.warmup % 2), 1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.step(K, 1)
+    torch.cuda.synchronize()
+    batch_s = max_over_ranks(time.perf_counter() - t0)
+    batch_dev_ms = max_over_ranks(b.last_step_ms())
+    plaq = b.plaquettes()
+    b.close()
+    Pn = N * (N - 1) // 2
+    E = (N - 1) * N * (N + 1) // 6
+    links = sum(4 * int(np.prod(l)) for l in L)
+    flops = (14 * Pn + 2 * E + E + 1.25 * E + 2 * Pn) * 216.0 * links * K
+    peak = P.fp64_peak_tflops()
+    if rank == 0:
+        series = {}
+        for dt in (0.005, 0.01, 0.02):
+            idx = [r for r in range(nrep) if dts[r] == dt]
+            series[str(dt)] = plaq[idx, :, 0].mean(axis=0).tolist()
+        line = {
+            "metric": "replica Langevin steps/s, 64 replicas of 6^4/8^4/10^4 x 12 orders "
+                      "(FP64, ZM + FA every step)",
+            "value": whole_job_rate(nrep * K, world, batch_s), "unit": "replica steps/s",
+            "n_gpus": world, "steps": K, "warmup": args.warmup,
+            "ms_per_step": batch_s * 1e3 / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (cold start + warm-up, device Philox noise per replica)",
+            "config": {"workload": "c4_batch_64x{6,8,10}^4_N12", "nrep": nrep, "N": N,
+                       "dt": [0.005, 0.01, 0.02], "alpha": alpha, "gf_every": 1},
+            "plain": {"value": whole_job_rate(nrep * K, world, plain_s), "unit": "replica steps/s",
+                      "how": "replicas one after another, nspt_step each"},
+            "batched_over_plain": plain_s / batch_s,
+            "batched_device_ms": batch_dev_ms, "tuned_warps": warps,
+            "roofline": {"bound": "fp64", "achieved": flops / batch_s / 1e12, "peak": peak,
+                         "unit": "TFLOP/s", "frac": flops / batch_s / 1e12 / peak},
+            "plaquette_per_dt": series,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -418,9 +496,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-gf", action="store_true", help="skip the gauge-fixing figure")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "c2"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "c2", "c4"],
                     help="sweep: 32^4 x 24 twisted (the headline); c2: 16^4 x 20 periodic "
-                         "with zero modes and FA gauge fixing every step, per pass")
+                         "with zero modes and FA gauge fixing every step, per pass; c4: 64 "
+                         "replicas of 6^4..10^4 x 12, batched in one CUDA graph vs plain")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -428,6 +507,9 @@ def main():
         return
     if args.workload == "c2":
         run_c2(args, world, rank, local)
+        return
+    if args.workload == "c4":
+        run_c4(args, world, rank, local)
         return
     run_ours(args, world, rank, local)
 

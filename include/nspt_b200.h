@@ -143,6 +143,37 @@ double nspt_last_kernel_ms(const nspt_ctx *ctx);
  * chains on every SM), TFLOP/s.  Roofline denominator for the sweep. */
 int nspt_measure_fp64_peak(double *tflops);
 
+/* ---- batches of independent replicas ----
+ * The reference runs one lattice per process; studies such as the dt -> 0
+ * extrapolation run many (seeds x time steps x volumes).  A batch holds nrep
+ * replicas -- each an ordinary context: extents L[4r..4r+3], its own time
+ * step dt[r] and noise seed seeds[r] (Philox counter 0), the same N, flags
+ * and alpha -- and advances all of them per step with one CUDA graph in
+ * which the replicas' kernels run side by side.  Replica r after k batch
+ * steps is bit-identical to a context created and seeded alike and advanced
+ * by nspt_step(ctx, dt[r], k, gf_every). */
+typedef struct nspt_batch nspt_batch;
+int nspt_batch_create(int nrep, const int *L, int N, unsigned flags, double alpha,
+                      const double *dt, const uint64_t *seeds, nspt_batch **out);
+int nspt_batch_destroy(nspt_batch *b);
+/* Replica r's context, owned by the batch (upload, download, observables,
+ * plaquette, save/load all apply; do not destroy it). */
+int nspt_batch_context(nspt_batch *b, int r, nspt_ctx **ctx);
+/* nsteps Langevin steps of every replica (nspt_step's body, device noise):
+ * nsteps must be a multiple of the graph length, 2 for gf_every <= 1, else
+ * the even multiple of gf_every (gf_every, or 2 gf_every when odd).  The
+ * first call captures the graph; later calls replay it.  NSPT_ERR_STATE if
+ * a replica has injected noise pending. */
+int nspt_batch_step(nspt_batch *b, int nsteps, int gf_every);
+/* Device time of the last nspt_batch_step (CUDA events), milliseconds. */
+double nspt_batch_last_step_ms(const nspt_batch *b);
+/* Plaquette series of every replica's last sweep: plaq[nrep][(N+1)*2]. */
+int nspt_batch_observables(nspt_batch *b, double *plaq);
+/* Autotuner: times the batch step for every sweep shape (warps per CTA)
+ * and keeps the fastest in *warps_out; the trial steps are undone (every
+ * replica back to a cold start with its seed).  Call before stepping. */
+int nspt_batch_tune(nspt_batch *b, int gf_every, int *warps_out);
+
 /* Static plaquette of a field the caller already holds in device memory,
  * without a context and without allocating anything.  This entry point has
  * no counterpart in the reference.  It computes what nspt_plaquette_measure

@@ -28,7 +28,7 @@ from ._lib import (NSPT_GF_FA, NSPT_GF_LOCAL, NSPT_TWIST_T, NSPT_TWIST_Y, NSPT_T
                    NsptError, build as build_library, check, load as load_library)
 
 __all__ = ["NsptEngine", "ptGluon_fld", "SweepObservables", "build", "series_len",
-           "NsptError", "fp64_peak_tflops"]
+           "NsptError", "fp64_peak_tflops", "NsptBatch"]
 
 _DIRS = {"x": 0, "y": 1, "z": 2, "t": 3}
 
@@ -145,11 +145,22 @@ class NsptEngine:
         h = ctypes.c_void_p()
         check(lib.nspt_create(arr, self.N, flags, self.alpha, ctypes.byref(h)), "nspt_create")
         self._h = h
+        self._owned = True
+
+    @classmethod
+    def _view(cls, h, L, N, flags, alpha):
+        """A context owned elsewhere (a replica of an NsptBatch)."""
+        e = cls.__new__(cls)
+        e.L, e.N, e.V = tuple(L), int(N), int(np.prod(L))
+        e.flags, e.alpha = flags, float(alpha)
+        e._h, e._owned = h, False
+        return e
 
     # -- lifetime -------------------------------------------------------
     def close(self):
         if getattr(self, "_h", None):
-            load_library().nspt_destroy(self._h)
+            if getattr(self, "_owned", True):
+                load_library().nspt_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -272,3 +283,71 @@ class NsptEngine:
     def last_kernel_ms(self) -> float:
         """Average sweep-kernel launch of the last NsptEvolve / gauge_wilson."""
         return float(load_library().nspt_last_kernel_ms(self._h))
+
+
+class NsptBatch:
+    """Independent replicas advanced together in one CUDA graph
+    (nspt_batch_* in include/nspt_b200.h): replica r has extents L[r], time
+    step dt[r] and noise seed seeds[r]; all share N, the flags and alpha."""
+
+    def __init__(self, L, N: int, dt, seeds, zero_modes: bool = False, fa: bool = False,
+                 local_gf: bool = False, alpha: float = 0.0, twist: str = ""):
+        lib = load_library()
+        L = [tuple(int(x) for x in l) for l in L]
+        n = len(L)
+        if len(dt) != n or len(seeds) != n:
+            raise ValueError("L, dt and seeds need one entry per replica")
+        flags = 0
+        for d in twist:
+            flags |= {"y": NSPT_TWIST_Y, "z": NSPT_TWIST_Z, "t": NSPT_TWIST_T}[d]
+        flags |= (NSPT_ZEROMODE if zero_modes else 0) | (NSPT_GF_FA if fa else 0)
+        flags |= NSPT_GF_LOCAL if local_gf else 0
+        self.N, self.n = int(N), n
+        Ls = (ctypes.c_int * (4 * n))(*[x for l in L for x in l])
+        dts = (ctypes.c_double * n)(*[float(x) for x in dt])
+        sds = (ctypes.c_uint64 * n)(*[int(x) for x in seeds])
+        h = ctypes.c_void_p()
+        check(lib.nspt_batch_create(n, Ls, self.N, flags, float(alpha), dts, sds, ctypes.byref(h)),
+              "nspt_batch_create")
+        self._h = h
+        self.replicas = []
+        for r in range(n):
+            c = ctypes.c_void_p()
+            check(lib.nspt_batch_context(h, r, ctypes.byref(c)), "nspt_batch_context")
+            self.replicas.append(NsptEngine._view(c, L[r], self.N, flags, alpha))
+
+    def step(self, nsteps: int, gf_every: int = 1):
+        check(load_library().nspt_batch_step(self._h, int(nsteps), int(gf_every)), "nspt_batch_step")
+
+    def last_step_ms(self) -> float:
+        return float(load_library().nspt_batch_last_step_ms(self._h))
+
+    def plaquettes(self) -> np.ndarray:
+        out = np.zeros((self.n, self.N + 1, 2))
+        check(load_library().nspt_batch_observables(self._h, _dp(out)), "nspt_batch_observables")
+        return out
+
+    def tune(self, gf_every: int = 1) -> int:
+        w = ctypes.c_int()
+        check(load_library().nspt_batch_tune(self._h, int(gf_every), ctypes.byref(w)),
+              "nspt_batch_tune")
+        return w.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for e in self.replicas:
+                e._h = None
+            load_library().nspt_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

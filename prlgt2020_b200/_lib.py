@@ -61,6 +61,14 @@ SIGNATURES = {
     "nspt_last_step_ms": (ctypes.c_double, [_P]),
     "nspt_last_kernel_ms": (ctypes.c_double, [_P]),
     "nspt_measure_fp64_peak": (_I, [_D]),
+    "nspt_batch_create": (_I, [_I, ctypes.POINTER(ctypes.c_int), _I, ctypes.c_uint, ctypes.c_double,
+                               _D, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(_P)]),
+    "nspt_batch_destroy": (_I, [_P]),
+    "nspt_batch_context": (_I, [_P, _I, ctypes.POINTER(_P)]),
+    "nspt_batch_step": (_I, [_P, _I, _I]),
+    "nspt_batch_last_step_ms": (ctypes.c_double, [_P]),
+    "nspt_batch_observables": (_I, [_P, _D]),
+    "nspt_batch_tune": (_I, [_P, _I, ctypes.POINTER(_I)]),
     "nspt_plaquette_measure_noalloc": (_I, [ctypes.c_void_p, _I, ctypes.POINTER(ctypes.c_int), _I,
                                            ctypes.c_uint, _D, ctypes.c_void_p]),
 }

@@ -53,6 +53,8 @@ struct nspt_ctx {
   double *red1;   // [N]
   double *p2;     // lattice momenta p2hat[4][128] of this context's extents
   int gf_grid[4]; // local gauge fixing: the reference's thread grid (ntt, ntx, nty, ntz)
+  unsigned long long *dcounter;  // Philox step counter on the device (advanced by k_inc)
+  int sweep_warps;               // warps per CTA of the sweep, 0 = as many as fit
   double *noise;  // injected noise
   bool noise_pending;
   bool have_obs;
@@ -110,7 +112,9 @@ static KernelShape choose_shape(const nspt_ctx *ctx, int slots, long units, int 
 
 static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
   const long nl = 4 * ctx->V;
-  KernelShape k = choose_shape(ctx, SWEEP_SLOTS, nl, RING, SWEEP_THREADS / 32);
+  KernelShape k = choose_shape(ctx, SWEEP_SLOTS, nl, RING,
+                               ctx->sweep_warps > 0 ? std::min(ctx->sweep_warps, SWEEP_THREADS / 32)
+                                                    : SWEEP_THREADS / 32);
   const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, SWEEP_SLOTS, RING);
   const long per_cta = (long)k.warps * LPW;
   const unsigned grid = (unsigned)((nl + per_cta - 1) / per_cta);
@@ -170,6 +174,7 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   a.noise = use_noise ? ctx->noise : nullptr;
   a.seed = ctx->seed;
   a.step = ctx->counter;
+  a.stepp = ctx->dcounter;
   // QuenchedAllocate: stau = sqrt(tau_g); tau_g /= -(2 NC)  (Quenched.cc:584-589)
   a.stau = sqrt(dt);
   double tg = dt;
@@ -188,6 +193,8 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   }
   rc = reduce_sweep_obs(ctx);
   if (rc) return rc;
+  k_inc<<<1, 1, 0, ctx->st>>>(ctx->dcounter);
+  CK(cudaGetLastError());
   std::swap(ctx->U, ctx->F);
   std::swap(ctx->Uf, ctx->Ff);
   ctx->counter++;
@@ -355,7 +362,7 @@ static int upload_constants(nspt_ctx *ctx) {
 }
 
 static void free_all(nspt_ctx *ctx) {
-  void *ptrs[] = {ctx->U, ctx->Uf, ctx->F, ctx->Ff, ctx->Lg, ctx->Wg, ctx->Gx, ctx->p2,
+  void *ptrs[] = {ctx->U, ctx->Uf, ctx->F, ctx->Ff, ctx->Lg, ctx->Wg, ctx->Gx, ctx->p2, ctx->dcounter,
                   ctx->obs_tr, ctx->obs_tru, ctx->obs_norm, ctx->red2, ctx->red1, ctx->noise};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -390,6 +397,8 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->V = V;
   ctx->U = ctx->Uf = ctx->F = ctx->Ff = ctx->Lg = ctx->Wg = ctx->Gx = nullptr;
   ctx->p2 = nullptr;
+  ctx->dcounter = nullptr;
+  ctx->sweep_warps = 0;
   // finest thread grid the reference accepts: blocks of 2 sites where L is even
   for (int d = 0; d < 4; d++) ctx->gf_grid[d] = (L[d] % 2 == 0) ? L[d] / 2 : 1;
   ctx->obs_tr = ctx->obs_tru = ctx->red2 = nullptr;
@@ -446,7 +455,8 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
             alloc((void **)&ctx->obs_norm, N * nl * sizeof(double)) &&
             alloc((void **)&ctx->red2, ((N + 1) + 4 * N + 36 * N) * sizeof(double2)) &&
             alloc((void **)&ctx->red1, N * sizeof(double)) &&
-            alloc((void **)&ctx->p2, 4 * 128 * sizeof(double));
+            alloc((void **)&ctx->p2, 4 * 128 * sizeof(double)) &&
+            alloc((void **)&ctx->dcounter, sizeof(unsigned long long));
   if (ok && (flags & (NSPT_ZEROMODE | NSPT_GF_FA))) ok = alloc((void **)&ctx->Lg, field);
   if (ok && (flags & NSPT_GF_FA))
     ok = alloc((void **)&ctx->Wg, field / 4) && alloc((void **)&ctx->Gx, field / 4);
@@ -456,6 +466,10 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
     return fail(NSPT_ERR_NOMEM);
   }
   if (upload_constants(ctx) != NSPT_OK) return fail(NSPT_ERR_CUDA);
+  if (cudaMemsetAsync(ctx->dcounter, 0, sizeof(unsigned long long), ctx->st) != cudaSuccess) {
+    cudaStreamDestroy(ctx->st);
+    return fail(NSPT_ERR_CUDA);
+  }
   *out = ctx;
   return nspt_cold_start(ctx);
 }
@@ -559,6 +573,9 @@ extern "C" int nspt_seed(nspt_ctx *ctx, uint64_t seed, uint64_t counter) {
   if (!ctx) return NSPT_ERR_ARG;
   ctx->seed = seed;
   ctx->counter = counter;
+  const unsigned long long c = counter;
+  CK(cudaMemcpyAsync(ctx->dcounter, &c, sizeof(c), cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
   return NSPT_OK;
 }
 
@@ -770,3 +787,6 @@ extern "C" int nspt_measure_fp64_peak(double *tflops) {
 
 // allocation-free plaquette of a caller-owned device field
 #include "noalloc.cuh"
+
+// batches of replicas in one CUDA graph
+#include "batch.cuh"

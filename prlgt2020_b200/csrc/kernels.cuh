@@ -199,6 +199,7 @@ struct SweepArgs {
   double2 *obs_tru;    // [N][4V]     Tr U_k
   const double *noise; // [V][4][8] injected, or null (Philox)
   uint64_t seed, step;
+  const unsigned long long *stepp;  // device step counter (Philox), or null: use step
   double tau_g, stau;  // -dt/6, sqrt(dt)  (Quenched.cc:584-589)
   int N, SS;
   Geo g;
@@ -357,7 +358,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
 #pragma unroll
         for (int q = 0; q < 8; q++) gz[q] = __ldg(a.noise + ((size_t)site * 4 + mu) * 8 + q);
       } else {
-        philox_gauss8(a.seed, a.step, (uint32_t)link, gz);
+        philox_gauss8(a.seed, a.stepp ? *a.stepp : a.step, (uint32_t)link, gz);
       }
     }
     for (int k = 1 + L.j; k <= N; k += GROUP) {
@@ -396,6 +397,10 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
     Lo[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
   });
 }
+
+// Advance a device step counter by one (a kernel, so that it replays
+// inside a captured CUDA graph).
+__global__ void k_inc(unsigned long long *c) { *c += 1ull; }
 
 // U = exp(reH(log U - MM[mu]/V)) per link: zero_modes_subtraction,
 // nspt.cc:605-654 (log U is the per-link log stored by the sweep).
