@@ -1,0 +1,329 @@
+// nspt_quenched -- the reference's quenched NSPT program (Quenched.cc) on
+// the B200 engine.
+//
+// The same inputs and outputs as the reference's executable:
+//   * Quench.cfg in the working directory, read key by key in the
+//     reference's order (Quenched.cc:158-172): "taglia L0 L1 L2 L3", SWEEP,
+//     BEAT, tau_g, alpha, init_status, plaq_out, last_conf, PTORD, seed;
+//   * the same command-line overrides (-l -s -b -r -g -a -t -p -c -d -n -h,
+//     Quenched.cc:182-236; -a sets alpha = -value as there);
+//   * damocle.dag, re-read after every BEAT steps for SWEEP, BEAT, tau_g,
+//     alpha, save_config and kill_run (AggiornaParametri, Quenched.cc:662-713);
+//   * output files named as the reference names them (Quenched.cc:376-407):
+//     the plaquette series <plaq_out>_SU3_wil_nf0_<L>_a<alpha>_tg<tau>_o<N>.txt
+//     (appended, 30 digits), .nor, .trU, .log, and the final configuration
+//     <last_conf>SU3_wil_nf0_..._o<N> in the reference's binary format
+//     (checkpoints add _<k>.dat), one line per order per step as
+//     gauge_wilson writes them (nspt.cc:570-597).
+// The reference fixes some choices at compile time (choices.h); here they are
+// options: -T <dirs> twisted boundaries in y/z/t (TWISTED_BC, _TWIST_*),
+// -F Fourier-accelerated gauge fixing (__FA_GAUGE_FIXING__, periodic only),
+// -G ntt,ntx,nty,ntz the thread grid whose order the local gauge fixing
+// reproduces (choices.h:124-128; default: the finest the reference accepts),
+// -Z 0|1 zero-mode subtraction (default: on with periodic boundaries, as
+// REMOVE_GLUON_ZEROMOM), -P device Philox noise instead of the reference's
+// rand55 stream.  The update is the Jacobi one (UPDATE_ONTHEFLY off).
+// Not reproduced: the Wilson-loop files of __MANY_LOOP__ / __WILLOOP_2x2__.
+#include <getopt.h>
+#include <unistd.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <ctime>
+#include <string>
+#include <vector>
+
+#include "../../include/nspt_b200.h"
+#include "rand55.h"
+
+namespace {
+
+struct Params {
+  int L[4] = {0, 0, 0, 0};
+  int sweep = 0, beat = 0, init = 0, N = 0;
+  double tau_g = 0.0, alpha = 0.0;
+  long seed = 0;
+  std::string plaqn, confn, damon = "damocle.dag";
+  unsigned twist = 0;
+  bool fa = false, philox = false;
+  int zm = -1;  // -1: as the boundary conditions imply
+  int grid[4] = {0, 0, 0, 0};
+};
+
+// get_val (Quenched.cc:97-114): the next word must be `key`, then a value.
+bool get_word(FILE *fp, const char *key, char *val, size_t n) {
+  char w[128];
+  if (fscanf(fp, "%127s", w) != 1 || strcmp(w, key) != 0) {
+    fprintf(stderr, "Error reading input file: expected %s\n", key);
+    return false;
+  }
+  char fmt[16];
+  snprintf(fmt, sizeof(fmt), "%%%zus", n - 1);
+  if (fscanf(fp, fmt, val) != 1) {
+    fprintf(stderr, "Error reading input file at %s\n", key);
+    return false;
+  }
+  return true;
+}
+bool get_int(FILE *fp, const char *key, int *v) {
+  char s[128];
+  if (!get_word(fp, key, s, sizeof(s))) return false;
+  *v = atoi(s);
+  return true;
+}
+bool get_double(FILE *fp, const char *key, double *v) {
+  char s[128];
+  if (!get_word(fp, key, s, sizeof(s))) return false;
+  *v = atof(s);
+  return true;
+}
+
+bool read_cfg(Params &p) {
+  FILE *fp = fopen("Quench.cfg", "r");
+  if (!fp) {
+    fprintf(stderr, "Errore: impossibile leggere il file di configurazione.\n");
+    return false;
+  }
+  bool ok = fscanf(fp, " taglia %d %d %d %d", &p.L[0], &p.L[1], &p.L[2], &p.L[3]) == 4;
+  char s[128];
+  ok = ok && get_int(fp, "SWEEP", &p.sweep) && get_int(fp, "BEAT", &p.beat) &&
+       get_double(fp, "tau_g", &p.tau_g) && get_double(fp, "alpha", &p.alpha) &&
+       get_int(fp, "init_status", &p.init);
+  if (ok && (ok = get_word(fp, "plaq_out", s, sizeof(s)))) p.plaqn = s;
+  if (ok && (ok = get_word(fp, "last_conf", s, sizeof(s)))) p.confn = s;
+  ok = ok && get_int(fp, "PTORD", &p.N);
+  if (ok && (ok = get_word(fp, "seed", s, sizeof(s)))) p.seed = atol(s);
+  fclose(fp);
+  if (!ok) fprintf(stderr, "Errore: Quench.cfg non valido.\n");
+  return ok;
+}
+
+void usage() {
+  printf("\n"
+         "-l\t\ttaglia (reticolo t==x==y==z)\n"
+         "-s\t\tnumero iterazioni (SWEEP)\n"
+         "-b\t\titerazioni tra letture damocle (BEAT)\n"
+         "-r\t\tseed generatore random\n"
+         "-g\t\ttau gluoni\n"
+         "-a\t\talpha\n"
+         "-t\t\tstato iniziale: 1)da configurazione; 0)freddo\n"
+         "-p\t\tnome file placchetta\n"
+         "-c\t\tnome configurazione salvata\n"
+         "-d\t\tnome file damocle\n"
+         "-n\t\tordine pt\n"
+         "-T dirs\t\ttwisted boundaries in the directions dirs (y, z, t)\n"
+         "-F\t\tFourier-accelerated gauge fixing (periodic boundaries)\n"
+         "-G a,b,c,d\tthread grid (ntt,ntx,nty,ntz) of the local gauge fixing\n"
+         "-Z 0|1\t\tzero-mode subtraction off/on\n"
+         "-P\t\tdevice Philox noise instead of the reference's generator\n\n");
+}
+
+// AggiornaParametri's damocle.dag read (Quenched.cc:677-685)
+bool read_damocle(const std::string &path, int &sweep, int &beat, double &tau_g, double &alpha,
+                  int &save, int &kill) {
+  FILE *df = fopen(path.c_str(), "r");
+  if (!df) {
+    fprintf(stderr, "Errore, impossibile trovare file damocle.\n");
+    return false;
+  }
+  const bool ok = get_int(df, "SWEEP", &sweep) && get_int(df, "BEAT", &beat) &&
+                  get_double(df, "tau_g", &tau_g) && get_double(df, "alpha", &alpha) &&
+                  get_int(df, "save_config", &save) && get_int(df, "kill_run", &kill);
+  fclose(df);
+  return ok;
+}
+
+std::string stem(const Params &p, const char *type) {
+  char buf[256];
+  snprintf(buf, sizeof(buf), "%s_nf0_%dx%dx%dx%d_a%2.2f_tg%3.3f_o%d", type, p.L[0], p.L[1], p.L[2],
+           p.L[3], std::fabs(p.alpha), p.tau_g, p.N);
+  return buf;
+}
+
+void stamp(FILE *log, const char *what) {
+  time_t t = time(nullptr);
+  fprintf(log, "%s\t\t%s\n", what, ctime(&t));
+}
+
+int fail(nspt_ctx *ctx, int rc, const char *where) {
+  fprintf(stderr, "nspt_quenched: %s: %s (%s)\n", where, nspt_error_string(rc),
+          ctx ? nspt_last_error(ctx) : "");
+  return 2;
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  Params p;
+  for (int i = 1; i < argc; i++)
+    if (!strcmp(argv[i], "-h")) {
+      usage();
+      return 0;
+    }
+  if (!read_cfg(p)) return 1;
+  int opt;
+  while ((opt = getopt(argc, argv, "l:s:b:d:r:g:a:t:p:c:n:hT:FG:Z:P")) != -1) {
+    switch (opt) {
+      case 'l': p.L[0] = p.L[1] = p.L[2] = p.L[3] = atoi(optarg); break;
+      case 's': p.sweep = atoi(optarg); break;
+      case 'b': p.beat = atoi(optarg); break;
+      case 'r': p.seed = atol(optarg); break;
+      case 'n': p.N = atoi(optarg); break;
+      case 'g': p.tau_g = atof(optarg); break;
+      case 'a': p.alpha = -atof(optarg); break;
+      case 't': p.init = atoi(optarg); break;
+      case 'p': p.plaqn = optarg; break;
+      case 'c': p.confn = optarg; break;
+      case 'd': p.damon = optarg; break;
+      case 'T':
+        for (const char *c = optarg; *c; c++) {
+          if (*c == 'y') p.twist |= NSPT_TWIST_Y;
+          else if (*c == 'z') p.twist |= NSPT_TWIST_Z;
+          else if (*c == 't') p.twist |= NSPT_TWIST_T;
+          else {
+            fprintf(stderr, "nspt_quenched: -T takes y, z and t\n");
+            return 1;
+          }
+        }
+        break;
+      case 'F': p.fa = true; break;
+      case 'G':
+        if (sscanf(optarg, "%d,%d,%d,%d", &p.grid[0], &p.grid[1], &p.grid[2], &p.grid[3]) != 4) {
+          fprintf(stderr, "nspt_quenched: -G takes ntt,ntx,nty,ntz\n");
+          return 1;
+        }
+        break;
+      case 'Z': p.zm = atoi(optarg); break;
+      case 'P': p.philox = true; break;
+      default: usage(); return 1;
+    }
+  }
+  {
+    FILE *df = fopen(p.damon.c_str(), "r");
+    if (!df) {
+      fprintf(stderr, "Errore, impossibile trovare file damocle.\n");
+      return 1;
+    }
+    fclose(df);
+  }
+  if (p.beat < 1 || p.N < 1) {
+    fprintf(stderr, "nspt_quenched: BEAT and PTORD must be positive\n");
+    return 1;
+  }
+  const bool periodic = p.twist == 0;
+  const bool zm = p.zm < 0 ? periodic : p.zm != 0;
+  unsigned flags = p.twist | (zm ? NSPT_ZEROMODE : 0u) | (p.fa ? NSPT_GF_FA : NSPT_GF_LOCAL);
+
+  // file names (Quenched.cc:376-407)
+  const char *type = "SU3_wil";
+  const std::string plaq_name = p.plaqn + "_" + stem(p, type) + ".txt";
+  const std::string conf_name = p.confn + stem(p, type);
+  const std::string log_name = stem(p, type) + ".log";
+  const std::string norm_name = stem(p, type) + ".nor";
+  const std::string tru_name = stem(p, type) + ".trU";
+  FILE *plaqf = fopen(plaq_name.c_str(), "a");
+  FILE *normf = fopen(norm_name.c_str(), "w");
+  FILE *truf = fopen(tru_name.c_str(), "w");
+  FILE *logf = fopen(log_name.c_str(), "w");
+  if (!plaqf || !normf || !truf || !logf) {
+    fprintf(stderr, "nspt_quenched: cannot open the output files\n");
+    return 1;
+  }
+  fprintf(logf, "Gauge group\t\tSU3\n\tgauge field update not \"on the fly\"\n");
+  fprintf(logf, "Gauge field boundary conditions\t\t%s\n", periodic ? "PERIODIC" : "TWISTED");
+  fprintf(logf,
+          "Taglia\t\t%d %d %d %d\nSweep\t\t%d\nBeat\t\t%d\nTau_g\t\t%g\nAlpha\t\t%g\n"
+          "Init status\t%d\nOrdine\t\t%d\n\nPlacchetta\t%s\nConfigurazione\t%s\nDamocle\t\t%s\n"
+          "Norma\t\t%s\nTr(U)\t\t%s\n\n",
+          p.L[0], p.L[1], p.L[2], p.L[3], p.sweep, p.beat, p.tau_g, p.alpha, p.init, p.N,
+          plaq_name.c_str(), conf_name.c_str(), p.damon.c_str(), norm_name.c_str(),
+          tru_name.c_str());
+
+  nspt_ctx *ctx = nullptr;
+  int rc = nspt_create(p.L, p.N, flags, p.alpha, &ctx);
+  if (rc) return fail(nullptr, rc, "nspt_create");
+  if (p.grid[0] && (rc = nspt_set_gf_grid(ctx, p.grid))) return fail(ctx, rc, "thread grid");
+  const int N = p.N;
+  std::vector<double> plaq(2 * (N + 1)), w(2 * (N + 1)), norm(N), tru(8 * N);
+  if (p.init) {  // hot start from the saved configuration (Quenched.cc:612-637)
+    if ((rc = nspt_load_config(ctx, conf_name.c_str(), N, w.data())))
+      return fail(ctx, rc, "Errore nella lettura della configurazione");
+    if ((rc = nspt_plaquette_measure(ctx, plaq.data()))) return fail(ctx, rc, "plaquette");
+    bool same = true;  // plaquette_check (nspt.cc:1042-1052)
+    for (int k = 0; k <= N; k++)
+      if (std::hypot(plaq[2 * k] - w[2 * k], plaq[2 * k + 1] - w[2 * k + 1]) > 1e-7) same = false;
+    if (!same) printf("La misura della placchetta non corrisponde.\n");
+    printf("\nMisura della placchetta:\n");
+    for (int k = 0; k <= N; k++) printf("%e %e\n", plaq[2 * k], plaq[2 * k + 1]);
+  }
+  Rand55 rng(p.seed);
+  if (p.philox && (rc = nspt_seed(ctx, (uint64_t)p.seed, 0))) return fail(ctx, rc, "seed");
+  std::vector<double> eta;
+  if (!p.philox) eta.resize((size_t)p.L[0] * p.L[1] * p.L[2] * p.L[3] * 32);
+  stamp(logf, "Inizio run");
+
+  int t1 = 0, done = 0, config_counter = 0;
+  while (t1 < p.sweep) {
+    t1 += p.beat;
+    for (int t2 = 0; t2 < p.beat; t2++) {  // NsptEvolve (nspt.cc:963-1036)
+      if (!p.philox) {
+        rng.fill(eta.data(), (long)eta.size());
+        if ((rc = nspt_set_noise(ctx, eta.data()))) return fail(ctx, rc, "noise");
+      }
+      if ((rc = nspt_gauge_wilson(ctx, p.tau_g))) return fail(ctx, rc, "gauge_wilson");
+      if ((rc = nspt_observables(ctx, plaq.data(), norm.data(), tru.data())))
+        return fail(ctx, rc, "observables");
+      for (int k = 0; k < N; k++) {  // nspt.cc:576-591
+        fprintf(plaqf, "%.30e\t%.30e\n", plaq[2 * k], plaq[2 * k + 1]);
+        fprintf(normf, "%g\n", norm[k]);
+        for (int mu = 0; mu < 4; mu++)
+          fprintf(truf, "%g\t%g\t", tru[2 * (mu * N + k)], tru[2 * (mu * N + k) + 1]);
+        fprintf(truf, "\n");
+      }
+      fprintf(plaqf, "%.30e\t%.30e\n", plaq[2 * N], plaq[2 * N + 1]);
+      if (zm && (rc = nspt_zero_modes_subtraction(ctx))) return fail(ctx, rc, "zero modes");
+      if (p.fa)
+        rc = nspt_fa_gauge_fixing(ctx, p.alpha);
+      else
+        rc = nspt_local_gauge_fixing(ctx, p.alpha);
+      if (rc) return fail(ctx, rc, "gauge fixing");
+      done++;
+    }
+    fflush(plaqf);
+    fflush(normf);
+    fflush(truf);
+    // AggiornaParametri (Quenched.cc:662-713)
+    fprintf(logf, "______________________________________\n\n");
+    stamp(logf, "Damocle Update");
+    fprintf(logf, "# Iterazioni\t\t%d\n", done);
+    int save = 0, kill = 0;
+    if (!read_damocle(p.damon, p.sweep, p.beat, p.tau_g, p.alpha, save, kill)) return 1;
+    fprintf(logf, "Tau_g\t\t\t%g\n\n", p.tau_g);
+    fflush(logf);
+    if (p.beat < 1) {
+      fprintf(stderr, "nspt_quenched: BEAT must be positive\n");
+      return 1;
+    }
+    if (save == 1) {
+      const std::string name = conf_name + "_" + std::to_string(++config_counter) + ".dat";
+      if ((rc = nspt_save_config(ctx, name.c_str(), N))) return fail(ctx, rc, "checkpoint");
+    }
+    if (kill == 1) p.sweep = 0;
+  }
+  // NsptFinalize (Quenched.cc:718-757)
+  fprintf(logf, "__________________________________\n");
+  stamp(logf, "Termine simulazione");
+  fprintf(logf, "# Iterazioni\t\t%d\n", t1);
+  if ((rc = nspt_plaquette_measure(ctx, plaq.data()))) return fail(ctx, rc, "plaquette");
+  printf("Misura della placchetta:\n");
+  for (int k = 0; k <= N; k++) printf("%e\t%e\n", plaq[2 * k], plaq[2 * k + 1]);
+  if ((rc = nspt_save_config(ctx, conf_name.c_str(), N))) return fail(ctx, rc, "save");
+  fclose(plaqf);
+  fclose(normf);
+  fclose(truf);
+  fclose(logf);
+  nspt_destroy(ctx);
+  return 0;
+}

@@ -1,0 +1,108 @@
+"""The C++ host driver (prlgt2020_b200/lib/nspt_quenched), run like the
+reference's own program: Quench.cfg and damocle.dag in the working directory,
+output files named and formatted as Quenched.cc / nspt.cc write them.
+
+The GPU tests replay every reference fixture in tests/golden through the
+driver, with the reference's own noise stream (the driver's host rand55),
+and compare the plaquette and norm series it writes, and the configuration
+it saves, with what the reference wrote.  Tolerances as in
+test_gpu_parity.py; the .nor file carries 6 significant digits (the
+reference's default stream precision), so it is held to 1e-5.
+"""
+import glob
+import math
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import obs_close, per_order_rel
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+@pytest.fixture(scope="module")
+def driver():
+    from prlgt2020_b200 import _lib
+    _lib.build()
+    path = os.path.join(os.path.dirname(_lib.LIB_PATH), "nspt_quenched")
+    assert os.path.exists(path)
+    return path
+
+
+def write_cfg(d, L, sweep, beat, tau_g, alpha, init, N, seed, plaq="plaq", conf="conf"):
+    with open(os.path.join(d, "Quench.cfg"), "w") as f:
+        f.write("taglia %d %d %d %d\n" % tuple(L))
+        f.write("SWEEP %d\nBEAT %d\ntau_g %r\nalpha %r\ninit_status %d\n" % (sweep, beat, tau_g, alpha,
+                                                                             init))
+        f.write("plaq_out %s\nlast_conf %s\nPTORD %d\nseed %d\n" % (plaq, conf, N, seed))
+
+
+def write_damocle(d, tau_g, alpha, sweep=0, beat=1, save=0, kill=0):
+    with open(os.path.join(d, "damocle.dag"), "w") as f:
+        f.write("SWEEP %d\nBEAT %d\ntau_g %r\nalpha %r\nsave_config %d\nkill_run %d\n"
+                % (sweep, beat, tau_g, alpha, save, kill))
+
+
+def stem(L, alpha, tau_g, N):
+    return "SU3_wil_nf0_%dx%dx%dx%d_a%.2f_tg%.3f_o%d" % (tuple(L) + (abs(alpha), tau_g, N))
+
+
+def test_driver_reports_missing_inputs(driver, tmp_path):
+    r = subprocess.run([driver], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 1 and "configurazione" in r.stderr
+    r = subprocess.run([driver, "-h"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0 and "SWEEP" in r.stdout
+    write_cfg(tmp_path, (4, 4, 4, 4), 2, 1, 0.01, 0.0, 0, 3, 1)
+    r = subprocess.run([driver], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 1 and "damocle" in r.stderr
+    with open(tmp_path / "Quench.cfg", "w") as f:
+        f.write("taglia 4 4 4 4\nSWEEP 2\nBEEP 1\n")
+    write_damocle(tmp_path, 0.01, 0.0)
+    r = subprocess.run([driver], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 1 and "BEAT" in r.stderr
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))),
+                         ids=lambda p: os.path.basename(p)[:-4])
+def test_driver_replays_reference_fixture(driver, oracle_mod, tmp_path, path):
+    O = oracle_mod
+    g = np.load(path)
+    L = tuple(int(x) for x in g["L"])
+    N, steps, dt = int(g["N"]), int(g["steps"]), float(g["dt"])
+    alpha, seed, start = float(g["alpha"]), int(g["seed"]), int(g["start"])
+    twisted, fa, zm = bool(g["twisted"]), bool(g["fa"]), bool(g["zm"])
+    V = int(np.prod(L))
+    name = stem(L, alpha, dt, N)
+    write_cfg(tmp_path, L, steps, steps, dt, alpha, 1 if start >= 0 else 0, N, seed)
+    write_damocle(tmp_path, dt, alpha)
+    if start >= 0:
+        o = O.Oracle(L, N, twist_mask=6 if twisted else 0)
+        o.random_start(start, 0.5)
+        O.write_config(str(tmp_path / ("conf" + name)), o.links, o.plaquette())
+    args = [driver, "-G", "1,1,1,1"]  # the fixtures' reference builds run one thread
+    if twisted:
+        args += ["-T", "yz"]
+    if fa:
+        args += ["-F"]
+    if not zm:
+        args += ["-Z", "0"]
+    r = subprocess.run(args, cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    plaq = np.loadtxt(tmp_path / ("plaq_" + name + ".txt")).reshape(steps, N + 1, 2)
+    norm = np.loadtxt(tmp_path / (name + ".nor")).reshape(steps, N)
+    for s in range(steps):
+        ok, w = obs_close(plaq[s], g["plaq"][s], 1e-11)
+        assert ok, ("plaq", s, w)
+        ok, w = obs_close(norm[s], g["norm"][s], 1e-5)
+        assert ok, ("norm", s, w)
+    links, trailer = O.read_config(str(tmp_path / ("conf" + name)), V, N)
+    rel = per_order_rel(links[: g["links"].shape[0]], g["links"], N)
+    bound = (np.array([max(1e-11, 1e-15 * math.factorial(k)) for k in range(1, N + 1)])
+             if (zm and start < 0) else 1e-11)
+    assert np.all(rel <= bound), rel
+    ok, w = obs_close(trailer, g["plaq_final"][: N + 1], 1e-11)
+    assert ok, ("saved plaquette", w)
