@@ -864,6 +864,120 @@ void oracle_local_gauge_fix(oracle_ctx *c, double alpha) {
   oracle_local_gauge_fix_grid(c, alpha, one);
 }
 
+/* ComputeLoops, nspt.cc:1148-1312 (periodic boundaries): per plane mu < nu
+ * and site x the 1x2 (both orientations), 2x2, 2x4 (both) and 4x4 Wilson
+ * loops as series, summed in the reference's order, then traced.  out holds
+ * 4 x (N+1) complex traces, already normalised as the reference prints them
+ * (loopNorm = 1/(3*2*3*V), with the extra 1/2 for 1x2 and 2x4): l21, l22,
+ * l42, l44.  The reference prints the real parts of the even orders. */
+void oracle_wilson_loops(oracle_ctx *c, double *out) {
+  int N = c->N, n = SER(N);
+  cx *scr = (cx *)malloc(sizeof(cx) * n * 24);
+  cx *w22 = scr, *w21 = scr + n, *w42 = scr + 2 * n, *w44 = scr + 3 * n;
+  cx *bl = scr + 4 * n, *ml = scr + 5 * n, *cd = scr + 6 * n, *ld = scr + 7 * n;
+  cx *br = scr + 8 * n, *mr = scr + 9 * n, *tr = scr + 10 * n, *tl = scr + 11 * n;
+  cx *lu = scr + 12 * n, *cu = scr + 13 * n, *ru = scr + 14 * n, *rd = scr + 15 * n;
+  cx *t1 = scr + 16 * n, *t2 = scr + 17 * n, *t3 = scr + 18 * n, *t4 = scr + 19 * n;
+  cx *t5 = scr + 20 * n, *t6 = scr + 21 * n;
+  s_zero(w22, N);
+  s_zero(w21, N);
+  s_zero(w42, N);
+  s_zero(w44, N);
+#define LNK(site, d) link_ptr(c->U, c, site, d)
+  for (int mu = 0; mu < 3; mu++)
+    for (int nu = mu + 1; nu < 4; nu++)
+      for (long x = 0; x < c->V; x++) {
+        int X[4];
+        coords_of(c, x, X);
+        /* site at X + i mu + j nu (periodic) */
+#define AT(i, j)                                                               \
+  ({                                                                           \
+    int y_[4];                                                                 \
+    memcpy(y_, X, sizeof(y_));                                                 \
+    y_[mu] = (y_[mu] + (i)) % c->L[mu];                                        \
+    y_[nu] = (y_[nu] + (j)) % c->L[nu];                                        \
+    site_of(c, y_);                                                            \
+  })
+        long a = AT(1, 0), b = AT(2, 0), cc = AT(2, 1), e = AT(0, 1), d = AT(1, 1);
+        long f = AT(2, 2), g = AT(1, 2), h = AT(0, 2);
+        s_mul(bl, LNK(x, mu), LNK(a, mu), N);
+        s_mul(ml, LNK(h, mu), LNK(g, mu), N);
+        s_mul(cd, LNK(b, nu), LNK(cc, nu), N);
+        s_mul(ld, LNK(x, nu), LNK(e, nu), N);
+        /* w22 += bl*cd*dag(ld*ml) */
+        s_mul(t1, bl, cd, N);
+        s_mul(t2, ld, ml, N);
+        s_dag(t3, t2, N);
+        s_mul(t4, t1, t3, N);
+        s_acc(w22, t4, N);
+        /* w21 += bl*U_nu(b)*dag(U_nu(x)*U_mu(e)*U_mu(d))
+         *      + U_mu(x)*U_nu(a)*U_nu(d)*dag(ld*U_mu(h)) */
+        s_mul(t1, bl, LNK(b, nu), N);
+        s_mul(t2, LNK(x, nu), LNK(e, mu), N);
+        s_mul(t3, t2, LNK(d, mu), N);
+        s_dag(t2, t3, N);
+        s_mul(t5, t1, t2, N);
+        s_mul(t1, LNK(x, mu), LNK(a, nu), N);
+        s_mul(t2, t1, LNK(d, nu), N);
+        s_mul(t3, ld, LNK(h, mu), N);
+        s_dag(t1, t3, N);
+        s_mul(t6, t2, t1, N);
+        s_acc(t5, t6, N);
+        s_acc(w21, t5, N);
+        long i = AT(0, 3), j = AT(2, 3), k = AT(2, 4), nn = AT(0, 4), l = AT(1, 4);
+        long m = AT(3, 0), o = AT(4, 0), p = AT(4, 1), q = AT(4, 2), r = AT(3, 2);
+        long ss = AT(4, 3), t = AT(3, 4);
+        s_mul(br, LNK(b, mu), LNK(m, mu), N);
+        s_mul(mr, LNK(f, mu), LNK(r, mu), N);
+        s_mul(tr, LNK(k, mu), LNK(t, mu), N);
+        s_mul(tl, LNK(nn, mu), LNK(l, mu), N);
+        s_mul(lu, LNK(h, nu), LNK(i, nu), N);
+        s_mul(cu, LNK(f, nu), LNK(j, nu), N);
+        s_mul(ru, LNK(q, nu), LNK(ss, nu), N);
+        s_mul(rd, LNK(o, nu), LNK(p, nu), N);
+        /* w42 += bl*(br*rd*dag(ml*mr) + cd*cu*dag(lu*tl))*dag(ld) */
+        s_mul(t1, br, rd, N);
+        s_mul(t2, ml, mr, N);
+        s_dag(t3, t2, N);
+        s_mul(t5, t1, t3, N);
+        s_mul(t1, cd, cu, N);
+        s_mul(t2, lu, tl, N);
+        s_dag(t3, t2, N);
+        s_mul(t6, t1, t3, N);
+        s_acc(t5, t6, N);
+        s_mul(t1, bl, t5, N);
+        s_dag(t2, ld, N);
+        s_mul(t3, t1, t2, N);
+        s_acc(w42, t3, N);
+        /* w44 += bl*br*rd*ru*dag(ld*lu*tl*tr) */
+        s_mul(t1, bl, br, N);
+        s_mul(t2, t1, rd, N);
+        s_mul(t1, t2, ru, N);
+        s_mul(t2, ld, lu, N);
+        s_mul(t3, t2, tl, N);
+        s_mul(t2, t3, tr, N);
+        s_dag(t3, t2, N);
+        s_mul(t2, t1, t3, N);
+        s_acc(w44, t2, N);
+#undef AT
+      }
+#undef LNK
+  const double norm = 1. / (3 * 2 * 3 * (double)c->V);
+  const double fac[4] = {.5 * norm, norm, .5 * norm, norm};
+  cx *ws[4] = {w21, w22, w42, w44};
+  for (int q = 0; q < 4; q++) {
+    double *o = out + (size_t)q * 2 * (N + 1);
+    o[0] = 3. * ws[q][0].re * fac[q];
+    o[1] = 3. * ws[q][0].im * fac[q];
+    for (int k = 1; k <= N; k++) {
+      cx tt = m_tr(ws[q] + 1 + 9 * (k - 1));
+      o[2 * k] = tt.re * fac[q];
+      o[2 * k + 1] = tt.im * fac[q];
+    }
+  }
+  free(scr);
+}
+
 /* plaquette_measure, nspt.cc:1316-1406 (OpenMP variant) */
 void oracle_plaquette(oracle_ctx *c, double *plaq) {
   int N = c->N, n = SER(N);

@@ -53,6 +53,9 @@ void oracle_local_gauge_fix(oracle_ctx *c, double alpha);
 /* the same as the reference built with OpenMP thread grid
  * grid = {ntt, ntx, nty, ntz} runs it; -1 for a grid the reference rejects */
 int oracle_local_gauge_fix_grid(oracle_ctx *c, double alpha, const int *grid);
+/* ComputeLoops (nspt.cc:1148-1312, periodic): traces of the summed 1x2,
+ * 2x2, 2x4 and 4x4 loops, out[4][(N+1)*2], normalised as printed */
+void oracle_wilson_loops(oracle_ctx *c, double *out);
 /* plaquette_measure, nspt.cc:1316-1406 (OpenMP variant, /72V) */
 void oracle_plaquette(oracle_ctx *c, double *plaq);
 

@@ -51,6 +51,7 @@ def lib():
         L.oracle_local_gauge_fix.argtypes = [P, ctypes.c_double]
         L.oracle_local_gauge_fix_grid.argtypes = [P, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
         L.oracle_local_gauge_fix_grid.restype = ctypes.c_int
+        L.oracle_wilson_loops.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
         L.oracle_plaquette.argtypes = [P, D]
         for f in ("oracle_ser_mul",):
             getattr(L, f).argtypes = [ctypes.c_int, D, D, D]
@@ -152,6 +153,13 @@ class Oracle:
 
     def fa_gauge_fix(self, alpha: float):
         lib().oracle_fa_gauge_fix(self._h, float(alpha))
+
+    def wilson_loops(self) -> np.ndarray:
+        """ComputeLoops (nspt.cc:1148-1312): [4, N+1, 2] traces of the 1x2,
+        2x2, 2x4, 4x4 loops, normalised as the reference prints them."""
+        out = np.zeros((4, self.N + 1, 2))
+        lib().oracle_wilson_loops(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out
 
     def local_gauge_fix(self, alpha: float, grid=(1, 1, 1, 1)):
         """stochastic_gauge_fixing as the reference built with the OpenMP

@@ -75,7 +75,7 @@ static void usage() {
   fprintf(stderr,
           "ref_harness --L l0 l1 l2 l3 --steps S --dt DT --alpha A --seed S "
           "--start cold|FILE --out PREFIX [--noise FILE] [--twist-init] "
-          "[--project] [--time]\n");
+          "[--project] [--time] [--loops FILE]\n");
   exit(2);
 }
 
@@ -84,7 +84,7 @@ int main(int argc, char **argv) {
   int steps = 1;
   double dt = 0.01, alpha = 0.0;
   long seed = 12345;
-  std::string start = "cold", out = "ref", noise_path;
+  std::string start = "cold", out = "ref", noise_path, loops_path;
   bool twist_init = false, project = false, timing = false;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
@@ -110,6 +110,8 @@ int main(int argc, char **argv) {
       project = true;
     } else if (a == "--time") {
       timing = true;
+    } else if (a == "--loops" && i + 1 < argc) {
+      loops_path = argv[++i];
     } else {
       usage();
     }
@@ -163,7 +165,15 @@ int main(int argc, char **argv) {
   normfile << std::scientific;
   trufile << std::scientific;
 #ifdef __MANY_LOOP__
-  loop_nxm.open("/dev/null");
+  /* ComputeLoops' stream (nspt.cc:1283-1306): the loops of the final field */
+  loop_nxm.open(loops_path.empty() ? "/dev/null" : loops_path.c_str());
+  loop_nxm.precision(17);
+  loop_nxm << std::scientific;
+#else
+  if (!loops_path.empty()) {
+    fprintf(stderr, "ref_harness: --loops needs a periodic build\n");
+    return 2;
+  }
 #endif
 
   latt LL(act_pars.sz);
@@ -257,6 +267,9 @@ int main(int argc, char **argv) {
   if (fnoise) fclose(fnoise);
 
   plaquette_measure(Umu, act_pars);
+#ifdef __MANY_LOOP__
+  if (!loops_path.empty()) ComputeLoops(Umu);
+#endif
   std::string conf = out + ".dat";
   std::vector<char> name(conf.begin(), conf.end());
   name.push_back('\0');

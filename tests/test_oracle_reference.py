@@ -85,3 +85,32 @@ def test_oracle_local_gauge_fixing_matches_reference_thread_grid(oracle_mod, cas
             o.zero_modes()
         o.local_gauge_fix(alpha, grid=(1,) + tuple(grid))
     assert per_order_rel(o.links, r["links"], N).max() <= 1e-12
+
+
+@pytest.mark.parametrize("L,N,start", [((4, 4, 4, 4), 6, 5), ((6, 4, 4, 4), 4, 7)])
+def test_oracle_wilson_loops_match_reference(oracle_mod, L, N, start):
+    """ComputeLoops (nspt.cc:1148-1312) on a random configuration: the
+    reference prints the real parts of the even orders of the 1x2, 2x2, 2x4
+    and 4x4 loops (periodic builds)."""
+    O = oracle_mod
+    b = O.ref_binary(N, "pbc", "local")
+    if not os.path.exists(b) or os.path.getmtime(b) < os.path.getmtime(
+            os.path.join(os.path.dirname(O.__file__), "ref_harness.cc")):
+        if not os.path.exists(os.path.join(REF, "nspt.cc")):
+            pytest.skip("reference sources not available")
+        b = O.build_reference(N, "pbc", "local")
+    o = O.Oracle(L, N)
+    o.random_start(start, 0.5)
+    with tempfile.TemporaryDirectory() as d:
+        O.write_config(os.path.join(d, "s.dat"), o.links, o.plaquette())
+        loops = os.path.join(d, "loops.txt")
+        import subprocess
+        subprocess.run([b, "--L", *[str(x) for x in L], "--steps", "0", "--start",
+                        os.path.join(d, "s.dat"), "--out", os.path.join(d, "r"), "--loops", loops],
+                       check=True, capture_output=True)
+        ref = np.loadtxt(loops).reshape(4, -1)
+    got = o.wilson_loops()[:, ::2, 0]
+    assert ref.shape == got.shape
+    for q in range(4):
+        ok, w = obs_close(got[q], ref[q], 1e-12)
+        assert ok, (q, w)
