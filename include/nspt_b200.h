@@ -122,6 +122,14 @@ int nspt_observables(nspt_ctx *ctx, double *plaq, double *norm, double *trU);
  * field, plaq[(N+1)*2]. */
 int nspt_plaquette_measure(nspt_ctx *ctx, double *plaq);
 
+/* ComputeLoops (nspt.cc:1148-1312), periodic boundaries: traces per order
+ * 0..N of the 1x2 (both orientations), 2x2, 2x4 (both) and 4x4 Wilson loops
+ * summed over all planes and sites, loops[4][(N+1)*2] in that order,
+ * normalised as the reference prints them (1/(18V), halved for 1x2 and
+ * 2x4; it prints the real parts of the even orders).  NSPT_ERR_STATE with
+ * twisted boundaries. */
+int nspt_wilson_loops(nspt_ctx *ctx, double *loops);
+
 /* Configuration files in the reference's binary format
  * (QCDenvNODEpt_test.h:359-374: field, then (allocORD+1) complex plaquette).
  * save writes plaquette_measure of the current field as the trailer. */

@@ -267,6 +267,13 @@ class NsptEngine:
                     "nspt_plaquette_measure")
         return out
 
+    def ComputeLoops(self) -> np.ndarray:
+        """Wilson loops of nspt.cc:1148-1312: [4, N+1, 2] traces of the 1x2,
+        2x2, 2x4 and 4x4 loops, normalised as the reference prints them."""
+        out = np.zeros((4, self.N + 1, 2))
+        self._check(load_library().nspt_wilson_loops(self._h, _dp(out)), "nspt_wilson_loops")
+        return out
+
     def observables(self) -> SweepObservables:
         N = self.N
         plaq = np.zeros((N + 1, 2))

@@ -56,6 +56,7 @@ SIGNATURES = {
     "nspt_set_gf_grid": (_I, [_P, ctypes.POINTER(ctypes.c_int)]),
     "nspt_observables": (_I, [_P, _D, _D, _D]),
     "nspt_plaquette_measure": (_I, [_P, _D]),
+    "nspt_wilson_loops": (_I, [_P, _D]),
     "nspt_save_config": (_I, [_P, ctypes.c_char_p, _I]),
     "nspt_load_config": (_I, [_P, ctypes.c_char_p, _I, _D]),
     "nspt_last_step_ms": (ctypes.c_double, [_P]),

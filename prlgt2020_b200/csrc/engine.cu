@@ -18,6 +18,7 @@
 
 #include "../../include/nspt_b200.h"
 #include "kernels.cuh"
+#include "loops.cuh"
 
 using namespace nspt;
 
@@ -55,6 +56,8 @@ struct nspt_ctx {
   int gf_grid[4]; // local gauge fixing: the reference's thread grid (ntt, ntx, nty, ntz)
   unsigned long long *dcounter;  // Philox step counter on the device (advanced by k_inc)
   int sweep_warps;               // warps per CTA of the sweep, 0 = as many as fit
+  double2 *loop_part;            // Wilson loops: per-CTA rows and the summed row
+  size_t loop_part_n;
   double *noise;  // injected noise
   bool noise_pending;
   bool have_obs;
@@ -363,6 +366,7 @@ static int upload_constants(nspt_ctx *ctx) {
 
 static void free_all(nspt_ctx *ctx) {
   void *ptrs[] = {ctx->U, ctx->Uf, ctx->F, ctx->Ff, ctx->Lg, ctx->Wg, ctx->Gx, ctx->p2, ctx->dcounter,
+                  ctx->loop_part,
                   ctx->obs_tr, ctx->obs_tru, ctx->obs_norm, ctx->red2, ctx->red1, ctx->noise};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -399,6 +403,8 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->p2 = nullptr;
   ctx->dcounter = nullptr;
   ctx->sweep_warps = 0;
+  ctx->loop_part = nullptr;
+  ctx->loop_part_n = 0;
   // finest thread grid the reference accepts: blocks of 2 sites where L is even
   for (int d = 0; d < 4; d++) ctx->gf_grid[d] = (L[d] % 2 == 0) ? L[d] / 2 : 1;
   ctx->obs_tr = ctx->obs_tru = ctx->red2 = nullptr;
@@ -624,6 +630,50 @@ extern "C" int nspt_fa_gauge_fixing(nspt_ctx *ctx, double alpha) {
   int rc = timed_begin(ctx);
   if (rc || (rc = do_fa(ctx, alpha))) return rc;
   return timed_end(ctx);
+}
+
+extern "C" int nspt_wilson_loops(nspt_ctx *ctx, double *loops) {
+  if (!ctx || !loops) return NSPT_ERR_ARG;
+  if (ctx->geo.twist) return NSPT_ERR_STATE;  // the reference has them with periodic bc only
+  const int N = ctx->N, row = 4 * (N + 1);
+  const size_t gb = ((size_t)LOOP_SLOTS * ctx->SS + RING + row) * sizeof(double2);
+  const int warps = (int)std::min<size_t>(8, ctx->smem_optin / (LPW * gb));
+  if (warps < 1) return NSPT_ERR_ORDER;
+  const long units = 6L * ctx->V;
+  const long per_cta = (long)warps * LPW;
+  const int grid = (int)std::min<long>((units + per_cta - 1) / per_cta, 8L * ctx->nsm);
+  const size_t need = (size_t)(grid + 1) * row;
+  if (need > ctx->loop_part_n) {
+    if (ctx->loop_part) cudaFree(ctx->loop_part);
+    ctx->loop_part = nullptr;
+    ctx->loop_part_n = 0;
+    if (cudaMalloc(&ctx->loop_part, need * sizeof(double2)) != cudaSuccess) {
+      cudaGetLastError();
+      return NSPT_ERR_NOMEM;
+    }
+    ctx->loop_part_n = need;
+  }
+  double2 *part = ctx->loop_part, *res = ctx->loop_part + (size_t)grid * row;
+  const size_t smem = (size_t)warps * LPW * gb;
+  int rc = timed_begin(ctx);
+  if (rc) return rc;
+  CK(cudaFuncSetAttribute(k_loops, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_loops<<<grid, 32 * warps, smem, ctx->st>>>(ctx->U, ctx->Uf, N, ctx->SS, ctx->geo, part);
+  CK(cudaGetLastError());
+  k_rows_sum<<<(row + 127) / 128, 128, 0, ctx->st>>>(part, grid, row, res);
+  CK(cudaGetLastError());
+  std::vector<double2> h(row);
+  CK(cudaMemcpyAsync(h.data(), res, row * sizeof(double2), cudaMemcpyDeviceToHost, ctx->st));
+  if ((rc = timed_end(ctx))) return rc;
+  // loopNorm = 1/(3*2*3*V), halved for 1x2 and 2x4 (nspt.cc:1280-1306)
+  const double norm = 1. / (3 * 2 * 3 * (double)ctx->V);
+  const double fac[4] = {.5 * norm, norm, .5 * norm, norm};
+  for (int q = 0; q < 4; q++)
+    for (int k = 0; k <= N; k++) {
+      loops[2 * (q * (N + 1) + k)] = h[q * (N + 1) + k].x * fac[q];
+      loops[2 * (q * (N + 1) + k) + 1] = h[q * (N + 1) + k].y * fac[q];
+    }
+  return NSPT_OK;
 }
 
 extern "C" int nspt_local_gauge_fixing(nspt_ctx *ctx, double alpha) {

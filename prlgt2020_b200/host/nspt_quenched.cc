@@ -23,7 +23,10 @@
 // -Z 0|1 zero-mode subtraction (default: on with periodic boundaries, as
 // REMOVE_GLUON_ZEROMOM), -P device Philox noise instead of the reference's
 // rand55 stream.  The update is the Jacobi one (UPDATE_ONTHEFLY off).
-// Not reproduced: the Wilson-loop files of __MANY_LOOP__ / __WILLOOP_2x2__.
+// With periodic boundaries the Wilson loops of ComputeLoops (__MANY_LOOP__,
+// the reference's periodic default) go to <plaq_out>_nxm_SU3_wil_..._o<N>.txt
+// after every BEAT steps and at the end (nspt.cc:1283-1306).  Not
+// reproduced: the 2x2-only file of __WILLOOP_2x2__.
 #include <getopt.h>
 #include <unistd.h>
 
@@ -224,6 +227,12 @@ int main(int argc, char **argv) {
   const std::string norm_name = stem(p, type) + ".nor";
   const std::string tru_name = stem(p, type) + ".trU";
   FILE *plaqf = fopen(plaq_name.c_str(), "a");
+  const std::string loops_name = p.plaqn + "_nxm_" + stem(p, type) + ".txt";
+  FILE *loopf = periodic ? fopen(loops_name.c_str(), "a") : nullptr;
+  if (periodic && !loopf) {
+    fprintf(stderr, "nspt_quenched: cannot open %s\n", loops_name.c_str());
+    return 1;
+  }
   FILE *normf = fopen(norm_name.c_str(), "w");
   FILE *truf = fopen(tru_name.c_str(), "w");
   FILE *logf = fopen(log_name.c_str(), "w");
@@ -247,6 +256,18 @@ int main(int argc, char **argv) {
   if (p.grid[0] && (rc = nspt_set_gf_grid(ctx, p.grid))) return fail(ctx, rc, "thread grid");
   const int N = p.N;
   std::vector<double> plaq(2 * (N + 1)), w(2 * (N + 1)), norm(N), tru(8 * N);
+  std::vector<double> loops(8 * (N + 1));
+  // ComputeLoops' line: per loop (1x2, 2x2, 2x4, 4x4) the even orders
+  auto write_loops = [&]() -> int {
+    if (!loopf) return NSPT_OK;
+    const int r = nspt_wilson_loops(ctx, loops.data());
+    if (r) return r;
+    for (int q = 0; q < 4; q++)
+      for (int k = 0; k <= N; k += 2) fprintf(loopf, "%.30e\t", loops[2 * (q * (N + 1) + k)]);
+    fprintf(loopf, "\n");
+    fflush(loopf);
+    return NSPT_OK;
+  };
   if (p.init) {  // hot start from the saved configuration (Quenched.cc:612-637)
     if ((rc = nspt_load_config(ctx, conf_name.c_str(), N, w.data())))
       return fail(ctx, rc, "Errore nella lettura della configurazione");
@@ -295,6 +316,7 @@ int main(int argc, char **argv) {
     fflush(normf);
     fflush(truf);
     // AggiornaParametri (Quenched.cc:662-713)
+    if ((rc = write_loops())) return fail(ctx, rc, "ComputeLoops");
     fprintf(logf, "______________________________________\n\n");
     stamp(logf, "Damocle Update");
     fprintf(logf, "# Iterazioni\t\t%d\n", done);
@@ -319,6 +341,8 @@ int main(int argc, char **argv) {
   if ((rc = nspt_plaquette_measure(ctx, plaq.data()))) return fail(ctx, rc, "plaquette");
   printf("Misura della placchetta:\n");
   for (int k = 0; k <= N; k++) printf("%e\t%e\n", plaq[2 * k], plaq[2 * k + 1]);
+  if ((rc = write_loops())) return fail(ctx, rc, "ComputeLoops");
+  if (loopf) fclose(loopf);
   if ((rc = nspt_save_config(ctx, conf_name.c_str(), N))) return fail(ctx, rc, "save");
   fclose(plaqf);
   fclose(normf);

@@ -106,3 +106,18 @@ def test_driver_replays_reference_fixture(driver, oracle_mod, tmp_path, path):
     assert np.all(rel <= bound), rel
     ok, w = obs_close(trailer, g["plaq_final"][: N + 1], 1e-11)
     assert ok, ("saved plaquette", w)
+    loops_file = tmp_path / ("plaq_nxm_" + name + ".txt")
+    if twisted:
+        assert not loops_file.exists()
+    else:
+        # ComputeLoops after the BEAT and at the end: the last line is the
+        # saved field's loops, even orders, 1x2 2x2 2x4 4x4
+        lines = np.atleast_2d(np.loadtxt(loops_file))
+        assert lines.shape[0] == 2
+        o = O.Oracle(L, N)
+        o.set_links(links)
+        want = o.wilson_loops()[:, ::2, 0]
+        got = lines[-1].reshape(4, -1)
+        for q in range(4):
+            ok, w = obs_close(got[q], want[q], 1e-11)
+            assert ok, ("loops", q, w)

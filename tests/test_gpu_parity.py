@@ -295,3 +295,13 @@ def test_gf_grid_rejects_what_the_reference_rejects(engine_mod):
         e.set_gf_grid((2, 3, 2, 2))
     with pytest.raises(P.NsptError):
         P.NsptEngine((4, 4, 4, 4), 3, fa=True, local_gf=True)
+
+
+@pytest.mark.parametrize("L,N", [((4, 4, 4, 4), 6), ((6, 4, 4, 4), 4), ((4, 4, 4, 4), 12)])
+def test_wilson_loops_match_oracle(engine_mod, oracle_mod, L, N):
+    """ComputeLoops (nspt.cc:1148-1312): all orders of the four loop traces."""
+    e, o = make_pair(engine_mod, oracle_mod, L, N, start=31 + N)
+    got, want = e.ComputeLoops(), o.wilson_loops()
+    for q in range(4):
+        ok, w = obs_close(got[q], want[q], 1e-12)
+        assert ok, (q, w)
