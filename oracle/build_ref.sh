@@ -3,13 +3,15 @@
 # oracle binary, from the sources where they lie (nothing is copied into the
 # repository; every output goes under oracle/_ref/, which git ignores).
 #
-#   oracle/build_ref.sh N BC GF NTX NTY NTZ
+#   oracle/build_ref.sh N BC GF NTX NTY NTZ [ACTION]
 #     N    perturbative order: allocORD = PTORD = N  (choices.h:30)
 #     BC   pbc | tw          periodic, or twisted in y and z (choices.h:42-49)
 #     GF   local | fa        local stochastic gauge fixing (nspt.cc:660-862)
 #                            or Fourier accelerated (nspt.cc:866-948)
 #     NTX NTY NTZ            OpenMP block grid (choices.h:124-128); 1 1 1 for
 #                            parity runs, larger only for CPU timing
+#     ACTION                 wil (default) | tlsym | iwa | dbw2: GAUGE_ACTION
+#                            (choices.h:110, periodic builds only)
 #
 # The build uses the reference's flags (Makefile:2: -DUSE_RAND55
 # -D__PARALLEL_OMP__ -O3 -fopenmp -std=c++0x) plus
@@ -26,8 +28,9 @@
 set -euo pipefail
 REF=${REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
-N=${1:?N}; BC=${2:?BC}; GF=${3:?GF}; NTX=${4:-1}; NTY=${5:-1}; NTZ=${6:-1}
+N=${1:?N}; BC=${2:?BC}; GF=${3:?GF}; NTX=${4:-1}; NTY=${5:-1}; NTZ=${6:-1}; ACT=${7:-wil}
 NAME=ref_N${N}_${BC}_${GF}_t${NTX}${NTY}${NTZ}
+if [ "$ACT" != wil ]; then NAME=${NAME}_${ACT}; fi
 OUT=$HERE/_ref/$NAME
 if [ ! -f "$REF/nspt.cc" ]; then
   echo "build_ref: reference sources not found at $REF" >&2
@@ -47,6 +50,13 @@ else
   DEFS+=(-DPBC)
 fi
 if [ "$GF" = fa ]; then DEFS+=(-D__FA_GAUGE_FIXING__); fi
+case "$ACT" in
+  wil) ;;
+  tlsym|iwa|dbw2)
+    UP=$(echo "$ACT" | tr a-z A-Z)
+    SED+=(-e "s/^#define GAUGE_ACTION WIL \/\/Alternatives/#define GAUGE_ACTION $UP \/\/Alternatives/") ;;
+  *) echo "build_ref: unknown action $ACT" >&2; exit 2 ;;
+esac
 sed "${SED[@]}" "$REF/choices.h" > "$OUT/cfg/choices.h.new"
 if ! cmp -s "$OUT/cfg/choices.h.new" "$OUT/cfg/choices.h" 2>/dev/null; then
   mv "$OUT/cfg/choices.h.new" "$OUT/cfg/choices.h"

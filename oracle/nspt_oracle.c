@@ -49,6 +49,8 @@ struct oracle_ctx {
   cx *U, *F, *MM;
   cx omega[4][9], omegadag[4][9];
   double *p2hat[4];
+  double c1;          /* improved action: 0 = Wilson (Quenched.cc:311-322) */
+  double last_w2[2 * (64 + 1)];  /* rectangle traces of the last sweep, /72V */
 };
 
 /* ---------------- complex and 3x3 primitives (MyMath.h) ---------------- */
@@ -528,6 +530,73 @@ static void staple(const oracle_ctx *c, const cx *field, const int *x, int mu,
   S[0] = cadd(s1[0], s2[0]);
 }
 
+/* ptSU3::staple2x1 (QCDenvNODEpt_test.h:579-611), periodic: the six 2x1
+ * rectangles through link (x, mu) in the plane (mu, nu), summed as the
+ * reference sums them.  Scratch: 6 series. */
+static void staple2x1(const oracle_ctx *c, const cx *field, const int *x, int mu, int nu,
+                      cx *out, cx *scr) {
+  int N = c->N, n = SER(N);
+  cx *A = scr, *B = scr + n, *C = scr + 2 * n, *D = scr + 3 * n, *E = scr + 4 * n,
+     *G = scr + 5 * n;
+#define AT(i, j)                                                               \
+  ({                                                                           \
+    int y_[4];                                                                 \
+    memcpy(y_, x, sizeof(y_));                                                 \
+    y_[mu] = ((y_[mu] + (i)) % c->L[mu] + c->L[mu]) % c->L[mu];                \
+    y_[nu] = ((y_[nu] + (j)) % c->L[nu] + c->L[nu]) % c->L[nu];                \
+    site_of(c, y_);                                                            \
+  })
+#define LK(site, d) link_ptr((cx *)field, c, site, d)
+  long x0 = site_of(c, x);
+  long a = AT(1, 0), b = AT(1, 1), cc = AT(0, 1), d = AT(0, 2), e = AT(2, 0), f = AT(-1, 0),
+       g = AT(-1, 1);
+  /* U_nu(a) U_nu(b) dag(U_nu(x) U_nu(c) U_mu(d)) */
+  s_mul(A, LK(a, nu), LK(b, nu), N);
+  s_mul(B, LK(x0, nu), LK(cc, nu), N);
+  s_mul(C, B, LK(d, mu), N);
+  s_dag(D, C, N);
+  s_mul(out, A, D, N);
+  /* + U_mu(a) U_nu(e) dag(U_nu(x) U_mu(c) U_mu(b)) */
+  s_mul(A, LK(a, mu), LK(e, nu), N);
+  s_mul(B, LK(x0, nu), LK(cc, mu), N);
+  s_mul(C, B, LK(b, mu), N);
+  s_dag(D, C, N);
+  s_mul(E, A, D, N);
+  s_acc(out, E, N);
+  /* + U_nu(a) dag(U_nu(f) U_mu(g) U_mu(c)) U_mu(f) */
+  s_mul(B, LK(f, nu), LK(g, mu), N);
+  s_mul(C, B, LK(cc, mu), N);
+  s_dag(D, C, N);
+  s_mul(A, LK(a, nu), D, N);
+  s_mul(E, A, LK(f, mu), N);
+  s_acc(out, E, N);
+  long b2 = AT(1, -1), c2 = AT(0, -1), d2 = AT(0, -2), e2 = AT(1, -2), f2 = AT(2, -1),
+       g2 = AT(-1, -1), h2 = AT(-1, 0);
+  /* dag(U_mu(d) U_nu(e) U_nu(b)) U_nu(d) U_nu(c) */
+  s_mul(B, LK(d2, mu), LK(e2, nu), N);
+  s_mul(C, B, LK(b2, nu), N);
+  s_dag(D, C, N);
+  s_mul(A, D, LK(d2, nu), N);
+  s_mul(G, A, LK(c2, nu), N);
+  /* + U_mu(a) dag(U_mu(c) U_mu(b) U_nu(f)) U_nu(c) */
+  s_mul(B, LK(c2, mu), LK(b2, mu), N);
+  s_mul(C, B, LK(f2, nu), N);
+  s_dag(D, C, N);
+  s_mul(A, LK(a, mu), D, N);
+  s_mul(E, A, LK(c2, nu), N);
+  s_acc(G, E, N);
+  /* + dag(U_mu(g) U_mu(c) U_nu(b)) U_nu(g) U_mu(h) */
+  s_mul(B, LK(g2, mu), LK(c2, mu), N);
+  s_mul(C, B, LK(b2, nu), N);
+  s_dag(D, C, N);
+  s_mul(A, D, LK(g2, nu), N);
+  s_mul(E, A, LK(h2, mu), N);
+  s_acc(G, E, N);
+  s_acc(out, G, N);
+#undef AT
+#undef LK
+}
+
 /* ---------------- Langevin sweep (nspt.cc:258-600, Jacobi) ---------------- */
 
 void oracle_sweep(oracle_ctx *c, double dt, const double *noise, double *plaq,
@@ -542,9 +611,12 @@ void oracle_sweep(oracle_ctx *c, double dt, const double *noise, double *plaq,
   double *nrm = (double *)calloc((size_t)nl * N, sizeof(double));
   cx *tu = (cx *)calloc((size_t)nl * N, sizeof(cx));
   cx *lg = zero_modes ? (cx *)calloc((size_t)nl * n, sizeof(cx)) : NULL;
+  const int imp = c->c1 != 0.0;
+  cx *tr2 = imp ? (cx *)calloc((size_t)nl * (N + 1), sizeof(cx)) : NULL;
 #pragma omp parallel
   {
-    cx *scr = (cx *)malloc(sizeof(cx) * n * 14);
+    cx *scr = (cx *)malloc(sizeof(cx) * n * 24);
+    cx *W2 = scr + 14 * n, *S2 = scr + 15 * n, *P2 = scr + 16 * n, *rs = scr + 17 * n;
     cx *W = scr + 7 * n, *S = scr + 8 * n, *P = scr + 9 * n, *E = scr + 10 * n,
        *B = scr + 11 * n, *Bn = scr + 12 * n;
     cx t[9], d[9];
@@ -555,10 +627,15 @@ void oracle_sweep(oracle_ctx *c, double dt, const double *noise, double *plaq,
       coords_of(c, s, x);
       const cx *u = link_ptr(c->U, c, s, mu);
       s_zero(W, N);
+      if (imp) s_zero(W2, N);
       for (int nu = 0; nu < 4; nu++) {
         if (nu == mu) continue;
         staple(c, c->U, x, mu, nu, S, scr);
         s_acc(W, S, N);
+        if (imp) {
+          staple2x1(c, c->U, x, mu, nu, S2, rs);
+          s_acc(W2, S2, N);
+        }
       }
       s_mul(P, u, W, N);
       /* ptSU3::Tr QCDpt.cc:115-122 */
@@ -571,6 +648,18 @@ void oracle_sweep(oracle_ctx *c, double dt, const double *noise, double *plaq,
         m_mul(t, u + 1 + 9 * k, d);
         nrm[(size_t)l * N + k] = m_tr(t).re;
         tu[(size_t)l * N + k] = m_tr(u + 1 + 9 * k);
+      }
+      if (imp) { /* nspt.cc:294-303: W1 = c0 W1 + c1 (U W2) */
+        s_mul(P2, u, W2, N);
+        cx *t2l = tr2 + (size_t)l * (N + 1);
+        t2l[0].re = 3. * P2[0].re;
+        t2l[0].im = 3. * P2[0].im;
+        for (int k = 0; k < N; k++) t2l[k + 1] = m_tr(P2 + 1 + 9 * k);
+        const double c0 = 1. - 8. * c->c1;
+        for (int k = 0; k < n; k++) {
+          cx a0 = {c0 * P[k].re, c0 * P[k].im}, b0 = {c->c1 * P2[k].re, c->c1 * P2[k].im};
+          P[k] = cadd(a0, b0);
+        }
       }
       s_reH(P, N);
       s_scale(P, tau_g, N);
@@ -603,6 +692,17 @@ void oracle_sweep(oracle_ctx *c, double dt, const double *noise, double *plaq,
     if (zero_modes) s_acc(c->MM + (size_t)mu * n, lg + (size_t)l * n, N);
   }
   double V = (double)c->V;
+  if (imp) {
+    cx *w2 = (cx *)calloc(N + 1, sizeof(cx));
+    for (long l = 0; l < nl; l++)
+      for (int k = 0; k <= N; k++) w2[k] = cadd(w2[k], tr2[(size_t)l * (N + 1) + k]);
+    for (int k = 0; k <= N; k++) {
+      c->last_w2[2 * k] = w2[k].re / (double)(72 * c->V);
+      c->last_w2[2 * k + 1] = w2[k].im / (double)(72 * c->V);
+    }
+    free(w2);
+    free(tr2);
+  }
   if (plaq)
     for (int k = 0; k <= N; k++) {
       plaq[2 * k] = w1[k].re / (double)(72 * c->V);
@@ -1033,4 +1133,18 @@ void oracle_ser_log(int N, const double *a, double *out) {
 void oracle_ser_reH(int N, double *a) { s_reH((cx *)a, N); }
 void oracle_ser_dag(int N, const double *a, double *out) {
   s_dag((cx *)out, (const cx *)a, N);
+}
+
+/* Improved gauge action (Quenched.cc:311-322): c1 = -1/12 (TLSYM), -0.331
+ * (IWA), -1.4088 (DBW2), 0 (Wilson); c0 = 1 - 8 c1.  Periodic only. */
+int oracle_set_action(oracle_ctx *c, double c1) {
+  if (c1 != 0.0 && c->tw) return -1;
+  if (c1 != 0.0 && c->N > 64) return -1;
+  c->c1 = c1;
+  return 0;
+}
+
+/* rectangle traces of the last sweep (w2 of nspt.cc:294-303), /72V */
+void oracle_last_w2(oracle_ctx *c, double *out) {
+  memcpy(out, c->last_w2, sizeof(double) * 2 * (c->N + 1));
 }

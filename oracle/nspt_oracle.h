@@ -53,6 +53,10 @@ void oracle_local_gauge_fix(oracle_ctx *c, double alpha);
 /* the same as the reference built with OpenMP thread grid
  * grid = {ntt, ntx, nty, ntz} runs it; -1 for a grid the reference rejects */
 int oracle_local_gauge_fix_grid(oracle_ctx *c, double alpha, const int *grid);
+/* improved gauge action c1 (c0 = 1 - 8 c1), periodic only; -1 otherwise */
+int oracle_set_action(oracle_ctx *c, double c1);
+/* rectangle traces w2 of the last sweep, (N+1)*2, /72V */
+void oracle_last_w2(oracle_ctx *c, double *out);
 /* ComputeLoops (nspt.cc:1148-1312, periodic): traces of the summed 1x2,
  * 2x2, 2x4 and 4x4 loops, out[4][(N+1)*2], normalised as printed */
 void oracle_wilson_loops(oracle_ctx *c, double *out);

@@ -52,6 +52,9 @@ def lib():
         L.oracle_local_gauge_fix_grid.argtypes = [P, ctypes.c_double, ctypes.POINTER(ctypes.c_int)]
         L.oracle_local_gauge_fix_grid.restype = ctypes.c_int
         L.oracle_wilson_loops.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
+        L.oracle_set_action.argtypes = [P, ctypes.c_double]
+        L.oracle_set_action.restype = ctypes.c_int
+        L.oracle_last_w2.argtypes = [P, ctypes.POINTER(ctypes.c_double)]
         L.oracle_plaquette.argtypes = [P, D]
         for f in ("oracle_ser_mul",):
             getattr(L, f).argtypes = [ctypes.c_int, D, D, D]
@@ -154,6 +157,16 @@ class Oracle:
     def fa_gauge_fix(self, alpha: float):
         lib().oracle_fa_gauge_fix(self._h, float(alpha))
 
+    def set_action(self, c1: float):
+        """Improved gauge action c1 (Quenched.cc:311-322), periodic only."""
+        if lib().oracle_set_action(self._h, float(c1)) != 0:
+            raise ValueError("improved actions need periodic boundaries")
+
+    def last_w2(self) -> np.ndarray:
+        out = np.zeros((self.N + 1, 2))
+        lib().oracle_last_w2(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        return out
+
     def wilson_loops(self) -> np.ndarray:
         """ComputeLoops (nspt.cc:1148-1312): [4, N+1, 2] traces of the 1x2,
         2x2, 2x4, 4x4 loops, normalised as the reference prints them."""
@@ -185,15 +198,19 @@ def ser_op(name: str, N: int, *args: np.ndarray) -> np.ndarray:
 # The reference's own code (oracle/_ref, built by build_ref.sh)
 # ---------------------------------------------------------------------------
 
-def ref_binary(N: int, bc: str = "pbc", gf: str = "local", grid=(1, 1, 1)) -> str:
-    return os.path.join(HERE, "_ref", "ref_N%d_%s_%s_t%d%d%d" % ((N, bc, gf) + tuple(grid)),
-                        "ref_harness")
+def ref_binary(N: int, bc: str = "pbc", gf: str = "local", grid=(1, 1, 1),
+               action: str = "wil") -> str:
+    name = "ref_N%d_%s_%s_t%d%d%d" % ((N, bc, gf) + tuple(grid))
+    if action != "wil":
+        name += "_" + action
+    return os.path.join(HERE, "_ref", name, "ref_harness")
 
 
-def build_reference(N: int, bc: str = "pbc", gf: str = "local", grid=(1, 1, 1)) -> str:
+def build_reference(N: int, bc: str = "pbc", gf: str = "local", grid=(1, 1, 1),
+                    action: str = "wil") -> str:
     subprocess.run([os.path.join(HERE, "build_ref.sh"), str(N), bc, gf] +
-                   [str(g) for g in grid], check=True, stdout=subprocess.DEVNULL)
-    return ref_binary(N, bc, gf, grid)
+                   [str(g) for g in grid] + [action], check=True, stdout=subprocess.DEVNULL)
+    return ref_binary(N, bc, gf, grid, action)
 
 
 def read_config(path: str, V: int, N: int):
@@ -229,7 +246,11 @@ def run_reference(binary: str, L, steps: int, dt: float, alpha: float, seed: int
     V = int(np.prod(L))
     res = {"stdout": p.stdout}
     N = None
-    plaq = np.loadtxt(out + ".plaq").reshape(steps, -1, 2)
+    raw = np.loadtxt(out + ".plaq")
+    if raw.ndim == 2 and raw.shape[1] == 4:  # improved action: w1 and w2 (nspt.cc:586-597)
+        res["w2"] = raw[:, 2:].reshape(steps, -1, 2)
+        raw = raw[:, :2]
+    plaq = raw.reshape(steps, -1, 2)
     N = plaq.shape[1] - 1
     res["plaq"] = plaq
     res["norm"] = np.loadtxt(out + ".nor").reshape(steps, N)

@@ -132,7 +132,16 @@ int main(int argc, char **argv) {
   act_pars.rVol = 1.0 / (double)act_pars.iVol;
   act_pars.tau_g = dt;
   act_pars.alpha = alpha;
+  /* improved action parameters, Quenched.cc:311-322 */
+#if GAUGE_ACTION == WIL
   act_pars.c1 = 0.0;
+#elif GAUGE_ACTION == TLSYM
+  act_pars.c1 = -1.0 / 12.0;
+#elif GAUGE_ACTION == IWA
+  act_pars.c1 = -0.331;
+#elif GAUGE_ACTION == DBW2
+  act_pars.c1 = -1.4088;
+#endif
   act_pars.c0 = 1. - 8. * act_pars.c1;
   act_pars.stau = sqrt(act_pars.tau_g);
   act_pars.tau_g /= -(2 * NC);

@@ -114,3 +114,40 @@ def test_oracle_wilson_loops_match_reference(oracle_mod, L, N, start):
     for q in range(4):
         ok, w = obs_close(got[q], ref[q], 1e-12)
         assert ok, (q, w)
+
+
+@pytest.mark.parametrize("action,c1", [("tlsym", -1.0 / 12.0), ("dbw2", -1.4088)])
+def test_oracle_improved_action_matches_reference(oracle_mod, action, c1):
+    """gauge_wilson with an improved action (nspt.cc:272-308, staple2x1
+    QCDenvNODEpt_test.h:579-611): plaquette and rectangle traces per step and
+    the links after the sweeps, from a random start with the reference's
+    noise."""
+    O = oracle_mod
+    L, N, steps, dt = (4, 4, 4, 4), 4, 2, 0.01
+    b = O.ref_binary(N, "pbc", "local", (1, 1, 1), action)
+    if not os.path.exists(b):
+        if not os.path.exists(os.path.join(REF, "nspt.cc")):
+            pytest.skip("reference sources not available")
+        b = O.build_reference(N, "pbc", "local", (1, 1, 1), action)
+    o = O.Oracle(L, N)
+    o.random_start(23, 0.5)
+    o.set_action(c1)
+    with tempfile.TemporaryDirectory() as d:
+        O.write_config(os.path.join(d, "s.dat"), o.links, o.plaquette())
+        r = O.run_reference(b, L, steps, dt, 0.0, 5, d, start=os.path.join(d, "s.dat"))
+    rng = O.Rand55(5)
+    cum = np.zeros(2)
+    for s in range(steps):
+        nz = rng.gauss(o.V * 32)
+        assert np.array_equal(nz, r["noise"][s])
+        ob = o.sweep(dt, nz, zero_modes=True)
+        assert obs_close(ob.plaq, r["plaq"][s], 1e-12)[0], s
+        w2 = o.last_w2()
+        assert obs_close(w2[:N], r["w2"][s][:N], 1e-12)[0], s
+        # the reference never resets w2[PTORD] between steps (NsptEvolve,
+        # nspt.cc:972-985 zeroes w2[0..PTORD-1] and w1[PTORD] only): its
+        # printed top order is the running sum
+        cum += w2[N]
+        assert np.allclose(r["w2"][s][N], cum, rtol=1e-12, atol=1e-30), s
+        o.zero_modes()
+    assert per_order_rel(o.links, r["links"], N).max() <= 1e-12
