@@ -49,6 +49,11 @@ extern "C" {
 #define NSPT_GF_FA (1u << 5)     /* Fourier-accelerated gauge fixing */
 #define NSPT_GF_LOCAL (1u << 6)  /* local stochastic gauge fixing (the reference's
                                     default without __FA_GAUGE_FIXING__) */
+/* improved gauge actions (GAUGE_ACTION, choices.h:110; c1 of Quenched.cc:
+ * 311-322), periodic boundaries only; at most one */
+#define NSPT_ACTION_TLSYM (1u << 7)  /* tree-level Symanzik, c1 = -1/12 */
+#define NSPT_ACTION_IWA (1u << 8)    /* Iwasaki, c1 = -0.331 */
+#define NSPT_ACTION_DBW2 (1u << 9)   /* DBW2, c1 = -1.4088 */
 
 typedef struct nspt_ctx nspt_ctx;
 
@@ -117,6 +122,13 @@ int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]);
  * plaq[(N+1)*2] (/72V), norm[N] (/12V), trU[4*N*2] (/3V, mu major).
  * Any pointer may be NULL. */
 int nspt_observables(nspt_ctx *ctx, double *plaq, double *norm, double *trU);
+
+/* Improved actions: the rectangle traces w2 of the last sweep, per order
+ * 0..N, /72V as nspt.cc:586-597 prints them (NSPT_ERR_STATE for the Wilson
+ * action).  The reference never resets w2[PTORD] between steps
+ * (nspt.cc:972-985), so its printed top order is a running sum; this one is
+ * the sweep's own value. */
+int nspt_rect_observables(nspt_ctx *ctx, double *w2);
 
 /* plaquette_measure (nspt.cc:1316-1406): static plaquette of the current
  * field, plaq[(N+1)*2]. */

@@ -123,7 +123,7 @@ class NsptEngine:
     """
 
     def __init__(self, L, N: int, twist: str = "", zero_modes: bool = False, fa: bool = False,
-                 alpha: float = 0.0, local_gf: bool = False):
+                 alpha: float = 0.0, local_gf: bool = False, action: str = "wil"):
         lib = load_library()
         self.L = tuple(int(x) for x in L)
         if len(self.L) != 4:
@@ -139,6 +139,8 @@ class NsptEngine:
             flags |= NSPT_GF_FA
         if local_gf:
             flags |= NSPT_GF_LOCAL
+        flags |= {"wil": 0, "tlsym": _lib.NSPT_ACTION_TLSYM, "iwa": _lib.NSPT_ACTION_IWA,
+                  "dbw2": _lib.NSPT_ACTION_DBW2}[action]
         self.flags = flags
         self.alpha = float(alpha)
         arr = (ctypes.c_int * 4)(*self.L)
@@ -265,6 +267,13 @@ class NsptEngine:
         out = np.zeros((self.N + 1, 2))
         self._check(load_library().nspt_plaquette_measure(self._h, _dp(out)),
                     "nspt_plaquette_measure")
+        return out
+
+    def rect_observables(self) -> np.ndarray:
+        """Improved actions: rectangle traces w2 of the last sweep (/72V)."""
+        out = np.zeros((self.N + 1, 2))
+        self._check(load_library().nspt_rect_observables(self._h, _dp(out)),
+                    "nspt_rect_observables")
         return out
 
     def ComputeLoops(self) -> np.ndarray:

@@ -31,6 +31,9 @@ NSPT_TWIST_T = 1 << 3
 NSPT_ZEROMODE = 1 << 4
 NSPT_GF_FA = 1 << 5
 NSPT_GF_LOCAL = 1 << 6
+NSPT_ACTION_TLSYM = 1 << 7
+NSPT_ACTION_IWA = 1 << 8
+NSPT_ACTION_DBW2 = 1 << 9
 
 # every entry point the header declares: name -> (restype, argtypes)
 _P = ctypes.c_void_p
@@ -56,6 +59,7 @@ SIGNATURES = {
     "nspt_set_gf_grid": (_I, [_P, ctypes.POINTER(ctypes.c_int)]),
     "nspt_observables": (_I, [_P, _D, _D, _D]),
     "nspt_plaquette_measure": (_I, [_P, _D]),
+    "nspt_rect_observables": (_I, [_P, _D]),
     "nspt_wilson_loops": (_I, [_P, _D]),
     "nspt_save_config": (_I, [_P, ctypes.c_char_p, _I]),
     "nspt_load_config": (_I, [_P, ctypes.c_char_p, _I, _D]),

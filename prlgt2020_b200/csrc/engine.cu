@@ -56,6 +56,8 @@ struct nspt_ctx {
   int gf_grid[4]; // local gauge fixing: the reference's thread grid (ntt, ntx, nty, ntz)
   unsigned long long *dcounter;  // Philox step counter on the device (advanced by k_inc)
   int sweep_warps;               // warps per CTA of the sweep, 0 = as many as fit
+  double c1;                     // improved action weight (0: Wilson), c0 = 1 - 8 c1
+  double2 *obs_tr2;              // [(N+1)][4V] rectangle traces (improved actions)
   double2 *loop_part;            // Wilson loops: per-CTA rows and the summed row
   size_t loop_part_n;
   double *noise;  // injected noise
@@ -133,6 +135,18 @@ static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
   return NSPT_OK;
 }
 
+static int launch_sweep_imp(nspt_ctx *ctx, const SweepArgs &a) {
+  const long nl = 4 * ctx->V;
+  KernelShape k = choose_shape(ctx, IMP_SLOTS, nl, RING);
+  const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, IMP_SLOTS, RING);
+  const long per_cta = (long)k.warps * LPW;
+  const unsigned grid = (unsigned)((nl + per_cta - 1) / per_cta);
+  cudaFuncSetAttribute(k_sweep_imp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_sweep_imp<<<grid, 32 * k.warps, smem, ctx->st>>>(a);
+  CK(cudaGetLastError());
+  return NSPT_OK;
+}
+
 // Launch a per-link (or per-site) group kernel with `slots` series per group.
 template <class Fn>
 static int launch_groups(nspt_ctx *ctx, const void *fn, int slots, long units, Fn launch,
@@ -153,9 +167,15 @@ static int launch_groups(nspt_ctx *ctx, const void *fn, int slots, long units, F
 
 // ---------------- reductions ----------------
 
+// rectangle traces of the improved actions sit after the MM area of red2
+static size_t w2_offset(int N) { return (size_t)(N + 1) + 4 * N + 36 * N; }
+
 static int reduce_sweep_obs(nspt_ctx *ctx) {
   const int N = ctx->N;
   const long nl = 4 * ctx->V;
+  if (ctx->c1 != 0.0)
+    k_rowsum<double2><<<N + 1, 256, 0, ctx->st>>>(ctx->obs_tr2, (size_t)nl, nl,
+                                                   ctx->red2 + w2_offset(N));
   k_rowsum<double2><<<N + 1, 256, 0, ctx->st>>>(ctx->obs_tr, (size_t)nl, nl, ctx->red2);
   k_rowsum<double2><<<4 * N, 256, 0, ctx->st>>>(ctx->obs_tru, (size_t)ctx->V, ctx->V,
                                                    ctx->red2 + (N + 1));
@@ -178,6 +198,9 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   a.seed = ctx->seed;
   a.step = ctx->counter;
   a.stepp = ctx->dcounter;
+  a.obs_tr2 = ctx->obs_tr2;
+  a.c1 = ctx->c1;
+  a.c0 = 1. - 8. * ctx->c1;
   // QuenchedAllocate: stau = sqrt(tau_g); tau_g /= -(2 NC)  (Quenched.cc:584-589)
   a.stau = sqrt(dt);
   double tg = dt;
@@ -188,7 +211,7 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   a.g = ctx->geo;
   const bool timed = ctx->kcount < nspt_ctx::KEV;
   if (timed) CK(cudaEventRecord(ctx->kev[2 * ctx->kcount], ctx->st));
-  int rc = launch_sweep(ctx, a, false);
+  int rc = ctx->c1 != 0.0 ? launch_sweep_imp(ctx, a) : launch_sweep(ctx, a, false);
   if (rc) return rc;
   if (timed) {
     CK(cudaEventRecord(ctx->kev[2 * ctx->kcount + 1], ctx->st));
@@ -366,7 +389,7 @@ static int upload_constants(nspt_ctx *ctx) {
 
 static void free_all(nspt_ctx *ctx) {
   void *ptrs[] = {ctx->U, ctx->Uf, ctx->F, ctx->Ff, ctx->Lg, ctx->Wg, ctx->Gx, ctx->p2, ctx->dcounter,
-                  ctx->loop_part,
+                  ctx->loop_part, ctx->obs_tr2,
                   ctx->obs_tr, ctx->obs_tru, ctx->obs_norm, ctx->red2, ctx->red1, ctx->noise};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -377,9 +400,14 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   if (!out || !L) return NSPT_ERR_ARG;
   *out = nullptr;
   if (N < 1 || N > NSPT_MAX_ORDER) return NSPT_ERR_ORDER;
-  const unsigned known =
-      NSPT_TWIST_Y | NSPT_TWIST_Z | NSPT_TWIST_T | NSPT_ZEROMODE | NSPT_GF_FA | NSPT_GF_LOCAL;
+  const unsigned actions = NSPT_ACTION_TLSYM | NSPT_ACTION_IWA | NSPT_ACTION_DBW2;
+  const unsigned known = NSPT_TWIST_Y | NSPT_TWIST_Z | NSPT_TWIST_T | NSPT_ZEROMODE | NSPT_GF_FA |
+                         NSPT_GF_LOCAL | actions;
   if (flags & ~known) return NSPT_ERR_ARG;
+  if (__builtin_popcount(flags & actions) > 1) return NSPT_ERR_ARG;
+  // the reference has improved actions with periodic boundaries only (choices.h:110)
+  if ((flags & actions) && (flags & (NSPT_TWIST_Y | NSPT_TWIST_Z | NSPT_TWIST_T)))
+    return NSPT_ERR_ARG;
   if ((flags & NSPT_GF_FA) && (flags & NSPT_GF_LOCAL)) return NSPT_ERR_ARG;
   long V = 1;
   for (int d = 0; d < 4; d++) {
@@ -405,6 +433,12 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->sweep_warps = 0;
   ctx->loop_part = nullptr;
   ctx->loop_part_n = 0;
+  ctx->obs_tr2 = nullptr;
+  // improved action parameters, Quenched.cc:311-322
+  ctx->c1 = (flags & NSPT_ACTION_TLSYM) ? -1.0 / 12.0
+          : (flags & NSPT_ACTION_IWA)   ? -0.331
+          : (flags & NSPT_ACTION_DBW2)  ? -1.4088
+                                        : 0.0;
   // finest thread grid the reference accepts: blocks of 2 sites where L is even
   for (int d = 0; d < 4; d++) ctx->gf_grid[d] = (L[d] % 2 == 0) ? L[d] / 2 : 1;
   ctx->obs_tr = ctx->obs_tru = ctx->red2 = nullptr;
@@ -440,6 +474,8 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   while (ctx->SS % 8 != 1) ctx->SS++;
   // one warp (3 link groups of 3 slots) must fit in a CTA
   if ((size_t)LPW * group_bytes(ctx, SWEEP_SLOTS, RING) > ctx->smem_optin) return fail(NSPT_ERR_ORDER);
+  if (ctx->c1 != 0.0 && (size_t)LPW * group_bytes(ctx, IMP_SLOTS, RING) > ctx->smem_optin)
+    return fail(NSPT_ERR_ORDER);
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return fail(NSPT_ERR_CUDA);
   cudaEventCreate(&ctx->ev0);
   cudaEventCreate(&ctx->ev1);
@@ -459,11 +495,12 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
             alloc((void **)&ctx->obs_tr, (N + 1) * nl * sizeof(double2)) &&
             alloc((void **)&ctx->obs_tru, N * nl * sizeof(double2)) &&
             alloc((void **)&ctx->obs_norm, N * nl * sizeof(double)) &&
-            alloc((void **)&ctx->red2, ((N + 1) + 4 * N + 36 * N) * sizeof(double2)) &&
+            alloc((void **)&ctx->red2, (2 * (N + 1) + 4 * N + 36 * N) * sizeof(double2)) &&
             alloc((void **)&ctx->red1, N * sizeof(double)) &&
             alloc((void **)&ctx->p2, 4 * 128 * sizeof(double)) &&
             alloc((void **)&ctx->dcounter, sizeof(unsigned long long));
   if (ok && (flags & (NSPT_ZEROMODE | NSPT_GF_FA))) ok = alloc((void **)&ctx->Lg, field);
+  if (ok && ctx->c1 != 0.0) ok = alloc((void **)&ctx->obs_tr2, (N + 1) * nl * sizeof(double2));
   if (ok && (flags & NSPT_GF_FA))
     ok = alloc((void **)&ctx->Wg, field / 4) && alloc((void **)&ctx->Gx, field / 4);
   if (!ok) {
@@ -738,6 +775,21 @@ extern "C" int nspt_observables(nspt_ctx *ctx, double *plaq, double *norm, doubl
         trU[2 * (mu * N + k)] = t.x / (double)(3 * ctx->V);
         trU[2 * (mu * N + k) + 1] = t.y / (double)(3 * ctx->V);
       }
+  return NSPT_OK;
+}
+
+extern "C" int nspt_rect_observables(nspt_ctx *ctx, double *w2) {
+  if (!ctx || !w2) return NSPT_ERR_ARG;
+  if (ctx->c1 == 0.0 || !ctx->have_obs) return NSPT_ERR_STATE;
+  const int N = ctx->N;
+  std::vector<double2> r(N + 1);
+  CK(cudaMemcpyAsync(r.data(), ctx->red2 + w2_offset(N), r.size() * sizeof(double2),
+                     cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  for (int k = 0; k <= N; k++) {  // nspt.cc:586-597
+    w2[2 * k] = r[k].x / (double)(72 * ctx->V);
+    w2[2 * k + 1] = r[k].y / (double)(72 * ctx->V);
+  }
   return NSPT_OK;
 }
 

@@ -200,6 +200,8 @@ struct SweepArgs {
   const double *noise; // [V][4][8] injected, or null (Philox)
   uint64_t seed, step;
   const unsigned long long *stepp;  // device step counter (Philox), or null: use step
+  double2 *obs_tr2;    // [(N+1)][4V] Tr(U * rectangle staples), improved actions
+  double c0, c1;       // improved action weights (Quenched.cc:311-322)
   double tau_g, stau;  // -dt/6, sqrt(dt)  (Quenched.cc:584-589)
   int N, SS;
   Geo g;
@@ -223,6 +225,65 @@ __device__ __forceinline__ long group_unit(int g, long nunits, bool &valid) {
   long u = ((long)blockIdx.x * nw + warp) * LPW + g;
   valid = u < nunits;
   return valid ? u : nunits - 1;
+}
+
+// The rest of a link update once the force (nspt.cc:392-416) is in slot T and
+// U_mu(x) in slot Y, observables written: W1 = reH(W1) tau_g - stau eta,
+// F = exp(W1) U_mu(x), and the per-link log for the zero modes.  W is a
+// free slot.  Shared by the Wilson and the improved-action sweeps.
+__device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, double2 *Y, double2 *W,
+                                            long link, int mu, int site, const Nb &self,
+                                            const Lane &L) {
+  const int N = a.N, c = L.c;
+  const size_t V = (size_t)a.g.V;
+  const size_t plane_mu = (size_t)9 * N * V;
+  // ---- W1 = reH(W1) * tau_g; W1.ptU[0] -= stau * SU3rand  (nspt.cc:416-423)
+  ser_reH(T, N, L);
+  {
+    double gz[8];
+    if (L.j == 0) {
+      if (a.noise) {
+#pragma unroll
+        for (int q = 0; q < 8; q++) gz[q] = __ldg(a.noise + ((size_t)site * 4 + mu) * 8 + q);
+      } else {
+        philox_gauss8(a.seed, a.stepp ? *a.stepp : a.step, (uint32_t)link, gz);
+      }
+    }
+    for (int k = 1 + L.j; k <= N; k += GROUP) {
+      double2 *p = T + 1 + 9 * (k - 1);
+#pragma unroll
+      for (int e = 0; e < 9; e++) p[e] = cscale(p[e], a.tau_g);
+      if (k == 1) {
+        double2 eta[9];
+        su3rand(gz, eta);
+#pragma unroll
+        for (int r = 0; r < 3; r++)
+#pragma unroll
+          for (int q = 0; q < 3; q++) p[3 * q + r] = csub(p[3 * q + r], cscale(eta[3 * r + q], a.stau));
+      }
+    }
+    if (L.j == 0) T[0] = cscale(cz(), a.tau_g);
+    __syncwarp(L.mask);
+  }
+  // ---- F = exp(W1) * U  (nspt.cc:429): exp into Y (W holds the square of
+  // W1), U_mu(x) restaged into W
+  ser_exp<MO>(T, W, Y, N, L);
+  stage(W, a.U, a.Uf, mu, self, a.g, N, L);
+  const bool zm = a.Lg != nullptr;
+  double2 *Fc = a.F + (size_t)mu * plane_mu + site;
+  product<MO, false>(LeftS{Y}, make_double2(1.0, 0.0), W, W[0], N, L,
+                     [&](int k, int r, double2 v) {
+                       Fc[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
+                       if (zm) W[sidx(k, r, c)] = v;
+                     });
+  if (L.j == 0) a.Ff[(size_t)mu * V + site] = W[0];
+  if (!zm) return;
+  __syncwarp(L.mask);
+  // ---- MM[mu] += log(F[link])  (nspt.cc:432-439): logs stored per link
+  double2 *Lo = a.Lg + (size_t)mu * plane_mu + site;
+  ser_log<MO>(W, T, Y, N, L, [&](int k, int r, double2 v) {
+    Lo[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
+  });
 }
 
 // Jacobi Langevin sweep, one link per group: gauge_wilson, nspt.cc:362-439.
@@ -349,53 +410,269 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
   }
   if constexpr (MEASURE) return;
   __syncwarp(L.mask);
-  // ---- W1 = reH(W1) * tau_g; W1.ptU[0] -= stau * SU3rand  (nspt.cc:416-423)
-  ser_reH(T, N, L);
+  update_link(a, T, Y, W, link, mu, site, self, L);
+}
+
+// ---------------- improved gauge actions ----------------
+
+// Jacobi sweep with an improved gauge action (TLSYM, IWA, DBW2; periodic
+// boundaries): gauge_wilson, nspt.cc:272-308.  Besides the Wilson staples W,
+// the six 2x1 rectangles of staple2x1 (QCDenvNODEpt_test.h:579-611) per
+// plane go to W2; the force is c0 U W + c1 U W2, and Tr(U W2) is the w2
+// observable.  Each rectangle is four products: a two-link path A, the
+// dagger of A times a third link (written transposed and conjugated), and
+// two more factors.  Six slots per group: T, Y (paths), E (third path),
+// STG (staged links), W, W2.
+constexpr int IMP_SLOTS = 6;
+
+struct ImpCtx {
+  const double2 *U, *Uf;
+  double2 *STG, *ring;
+  size_t V, plane;
+  int N;
+  Geo g;
+};
+
+__device__ __forceinline__ void imp_stage(const ImpCtx &q, double2 *slot, int d, int st,
+                                          const Lane &L) {
+  Nb n;
+  n.site = st;
+  n.fwd = n.bwd = 0;
+  stage(slot, q.U, q.Uf, d, n, q.g, q.N, L);
+}
+
+// out = U_d1(s1) U_d2(s2)
+__device__ __noinline__ void imp_two(const ImpCtx &q, double2 *out, int d1, int s1, int d2, int s2,
+                                     const Lane &L) {
+  imp_stage(q, q.STG, d2, s2, L);
+  const double2 a0 = __ldg(q.Uf + (size_t)d1 * q.V + s1), b0 = q.STG[0];
+  const int c = L.c;
+  product<MO, false>(LeftG{q.U + d1 * q.plane + s1, q.V, q.ring}, a0, q.STG, b0, q.N, L,
+                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
+  if (L.j == 0) out[0] = flag_mul(a0, b0);
+  __syncwarp(L.mask);
+}
+
+// out = dag(A U_d(s)), written transposed and conjugated
+__device__ __noinline__ void imp_dag_path(const ImpCtx &q, double2 *out, const double2 *A, int d,
+                                          int s, const Lane &L) {
+  imp_stage(q, q.STG, d, s, L);
+  const double2 a0 = A[0], b0 = q.STG[0];
+  const int c = L.c;
+  product<MO, false>(LeftS{A}, a0, q.STG, b0, q.N, L,
+                     [&](int k, int r, double2 v) { out[sidx(k, c, r)] = cconj(v); });
+  if (L.j == 0) out[0] = cconj(flag_mul(a0, b0));
+  __syncwarp(L.mask);
+}
+
+// out = U_d(s) B (left link streamed)
+__device__ __noinline__ void imp_link_times(const ImpCtx &q, double2 *out, int d, int s,
+                                            const double2 *B, const Lane &L) {
+  const double2 a0 = __ldg(q.Uf + (size_t)d * q.V + s), b0 = B[0];
+  const int c = L.c;
+  product<MO, false>(LeftG{q.U + d * q.plane + s, q.V, q.ring}, a0, B, b0, q.N, L,
+                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
+  if (L.j == 0) out[0] = flag_mul(a0, b0);
+  __syncwarp(L.mask);
+}
+
+// out = A B (slots)
+__device__ __noinline__ void imp_mul(double2 *out, const double2 *A, const double2 *B, int N,
+                                     const Lane &L) {
+  const double2 a0 = A[0], b0 = B[0];
+  const int c = L.c;
+  product<MO, false>(LeftS{A}, a0, B, b0, N, L,
+                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
+  if (L.j == 0) out[0] = flag_mul(a0, b0);
+  __syncwarp(L.mask);
+}
+
+// W (+)= A B; first: W = A B.  Returns the product's flag.
+__device__ __noinline__ double2 imp_acc(double2 *Wacc, const double2 *A, const double2 *B, bool first,
+                                        int N, const Lane &L) {
+  const double2 a0 = A[0], b0 = B[0];
+  const int c = L.c;
+  product<MO, false>(LeftS{A}, a0, B, b0, N, L, [&](int k, int r, double2 v) {
+    double2 &w = Wacc[sidx(k, r, c)];
+    w = first ? v : cadd(w, v);
+  });
+  __syncwarp(L.mask);
+  return flag_mul(a0, b0);
+}
+
+__global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5;
+  const int N = a.N, SS = a.SS, c = L.c;
+  const size_t V = (size_t)a.g.V;
+  double2 *T = sm + (size_t)(warp * LPW + g) * (IMP_SLOTS * SS + RING), *Y = T + SS;
+  double2 *E = Y + SS, *STG = E + SS, *W = STG + SS, *W2 = W + SS, *ring = W2 + SS;
+  bool valid;
+  const long link = group_unit(g, 4L * a.g.V, valid);
+  if (!valid) return;
+  const int mu = (int)(link / a.g.V);
+  const int site = (int)(link - (long)mu * a.g.V);
+  int x[4];
+  coords(a.g, site, x);
+  ImpCtx q;
+  q.U = a.U;
+  q.Uf = a.Uf;
+  q.STG = STG;
+  q.ring = ring;
+  q.V = V;
+  q.plane = (size_t)9 * N * V;
+  q.N = N;
+  q.g = a.g;
+
+  // site x + i mu + j nu (periodic)
+  int nu = 0;
+  auto at = [&](int i, int j) {
+    int y[4] = {x[0], x[1], x[2], x[3]};
+    y[mu] = ((y[mu] + i) % a.g.L[mu] + a.g.L[mu]) % a.g.L[mu];
+    y[nu] = ((y[nu] + j) % a.g.L[nu] + a.g.L[nu]) % a.g.L[nu];
+    return y[0] * a.g.s0 + y[1] * a.g.s1 + y[2] * a.g.s2 + y[3];
+  };
+  double2 w2flag = cz();
+  bool first2 = true;
+  auto acc2 = [&](const double2 *A, const double2 *B) {
+    const double2 f = imp_acc(W2, A, B, first2, N, L);
+    w2flag = first2 ? f : cadd(w2flag, f);
+    first2 = false;
+  };
+
+  double2 wflag = cz();
+  bool first = true;
+  for (nu = 0; nu < 4; nu++) {
+    if (nu == mu) continue;
+    // ---- Wilson staples, as in k_sweep (QCDenvNODEpt_test.h:554-557)
+    {
+      imp_stage(q, Y, mu, at(0, 1), L);
+      const double2 a0 = __ldg(a.Uf + (size_t)nu * V + site);
+      product<MO, false>(LeftG{a.U + nu * q.plane + site, V, ring}, a0, Y, Y[0], N, L,
+                         [&](int k, int r, double2 v) { T[sidx(k, c, r)] = cconj(v); });
+      if (L.j == 0) T[0] = cconj(flag_mul(a0, Y[0]));
+      __syncwarp(L.mask);
+      imp_stage(q, Y, nu, at(1, 0), L);
+      const double2 y0 = Y[0], t0 = T[0];
+      const bool f0 = first;
+      product<MO, false>(LeftS{Y}, y0, T, t0, N, L, [&](int k, int r, double2 v) {
+        double2 &w = W[sidx(k, r, c)];
+        w = f0 ? v : cadd(w, v);
+      });
+      wflag = first ? flag_mul(y0, t0) : cadd(wflag, flag_mul(y0, t0));
+      first = false;
+      __syncwarp(L.mask);
+    }
+    {
+      imp_stage(q, Y, nu, at(1, -1), L);
+      imp_stage(q, T, mu, at(0, -1), L);
+      const double2 a0 = T[0], y0 = Y[0];
+      product<MO, false>(LeftS{T}, a0, Y, y0, N, L,
+                         [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+      if (L.j == 0) T[0] = flag_mul(a0, y0);
+      __syncwarp(L.mask);
+      imp_stage(q, Y, nu, at(0, -1), L);
+      const double2 ta = cconj(T[0]);
+      product<MO, true>(LeftS{T}, ta, Y, Y[0], N, L, [&](int k, int r, double2 v) {
+        double2 &w = W[sidx(k, r, c)];
+        w = cadd(w, v);
+      });
+      wflag = cadd(wflag, flag_mul(ta, Y[0]));
+      __syncwarp(L.mask);
+    }
+    // ---- the six rectangles of staple2x1
+    // U_nu(a) U_nu(b) dag(U_nu(x) U_nu(c) U_mu(d)),  a=x+mu b=x+mu+nu c=x+nu d=x+2nu
+    imp_two(q, T, nu, site, nu, at(0, 1), L);
+    imp_dag_path(q, Y, T, mu, at(0, 2), L);
+    imp_two(q, E, nu, at(1, 0), nu, at(1, 1), L);
+    acc2(E, Y);
+    // U_mu(a) U_nu(e) dag(U_nu(x) U_mu(c) U_mu(b)),  e=x+2mu
+    imp_two(q, T, nu, site, mu, at(0, 1), L);
+    imp_dag_path(q, Y, T, mu, at(1, 1), L);
+    imp_two(q, E, mu, at(1, 0), nu, at(2, 0), L);
+    acc2(E, Y);
+    // U_nu(a) dag(U_nu(f) U_mu(g) U_mu(c)) U_mu(f),  f=x-mu g=x-mu+nu
+    imp_two(q, T, nu, at(-1, 0), mu, at(-1, 1), L);
+    imp_dag_path(q, Y, T, mu, at(0, 1), L);
+    imp_link_times(q, E, nu, at(1, 0), Y, L);
+    imp_stage(q, Y, mu, at(-1, 0), L);
+    acc2(E, Y);
+    // dag(U_mu(d) U_nu(e) U_nu(b)) U_nu(d) U_nu(c),  b=x+mu-nu c=x-nu d=x-2nu e=x+mu-2nu
+    imp_two(q, T, mu, at(0, -2), nu, at(1, -2), L);
+    imp_dag_path(q, Y, T, nu, at(1, -1), L);
+    imp_stage(q, STG, nu, at(0, -2), L);
+    imp_mul(E, Y, STG, N, L);
+    imp_stage(q, Y, nu, at(0, -1), L);
+    acc2(E, Y);
+    // U_mu(a) dag(U_mu(c) U_mu(b) U_nu(f)) U_nu(c),  f=x+2mu-nu
+    imp_two(q, T, mu, at(0, -1), mu, at(1, -1), L);
+    imp_dag_path(q, Y, T, nu, at(2, -1), L);
+    imp_link_times(q, E, mu, at(1, 0), Y, L);
+    imp_stage(q, Y, nu, at(0, -1), L);
+    acc2(E, Y);
+    // dag(U_mu(g) U_mu(c) U_nu(b)) U_nu(g) U_mu(h),  g=x-mu-nu h=x-mu
+    imp_two(q, T, mu, at(-1, -1), mu, at(0, -1), L);
+    imp_dag_path(q, Y, T, nu, at(1, -1), L);
+    imp_stage(q, STG, nu, at(-1, -1), L);
+    imp_mul(E, Y, STG, N, L);
+    imp_stage(q, Y, mu, at(-1, 0), L);
+    acc2(E, Y);
+  }
+  if (L.j == 0) {
+    W[0] = wflag;
+    W2[0] = w2flag;
+  }
+  // ---- U W and U W2 (nspt.cc:286-303), traces, force c0 U W + c1 U W2
+  Nb self;
+  self.site = site;
+  self.fwd = self.bwd = 0;
+  stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
+  const double2 pflag = flag_mul(Y[0], wflag), p2flag = flag_mul(Y[0], w2flag);
+  product<MO, false>(LeftS{Y}, Y[0], W, wflag, N, L,
+                     [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+  product<MO, false>(LeftS{Y}, Y[0], W2, w2flag, N, L,
+                     [&](int k, int r, double2 v) { E[sidx(k, r, c)] = v; });
+  if (L.j == 0) {
+    T[0] = pflag;
+    E[0] = p2flag;
+  }
+  __syncwarp(L.mask);
   {
-    double gz[8];
+    const size_t nl4 = 4 * V;
     if (L.j == 0) {
-      if (a.noise) {
-#pragma unroll
-        for (int q = 0; q < 8; q++) gz[q] = __ldg(a.noise + ((size_t)site * 4 + mu) * 8 + q);
-      } else {
-        philox_gauss8(a.seed, a.stepp ? *a.stepp : a.step, (uint32_t)link, gz);
-      }
+      a.obs_tr[link] = make_double2(3. * pflag.x, 3. * pflag.y);
+      a.obs_tr2[link] = make_double2(3. * p2flag.x, 3. * p2flag.y);
     }
     for (int k = 1 + L.j; k <= N; k += GROUP) {
-      double2 *p = T + 1 + 9 * (k - 1);
+      a.obs_tr[(size_t)k * nl4 + link] =
+          cadd(cadd(T[sidx(k, 0, 0)], T[sidx(k, 1, 1)]), T[sidx(k, 2, 2)]);
+      a.obs_tr2[(size_t)k * nl4 + link] =
+          cadd(cadd(E[sidx(k, 0, 0)], E[sidx(k, 1, 1)]), E[sidx(k, 2, 2)]);
+      double nrm = 0.0;
 #pragma unroll
-      for (int e = 0; e < 9; e++) p[e] = cscale(p[e], a.tau_g);
-      if (k == 1) {
-        double2 eta[9];
-        su3rand(gz, eta);
+      for (int i = 0; i < 3; i++) {
+        double d = 0.0;
 #pragma unroll
-        for (int r = 0; r < 3; r++)
-#pragma unroll
-          for (int q = 0; q < 3; q++) p[3 * q + r] = csub(p[3 * q + r], cscale(eta[3 * r + q], a.stau));
+        for (int l = 0; l < 3; l++) {
+          const double2 u = Y[sidx(k, i, l)];
+          d += u.x * u.x + u.y * u.y;
+        }
+        nrm += d;
       }
+      a.obs_norm[(size_t)(k - 1) * nl4 + link] = nrm;
+      a.obs_tru[(size_t)(k - 1) * nl4 + link] =
+          cadd(cadd(Y[sidx(k, 0, 0)], Y[sidx(k, 1, 1)]), Y[sidx(k, 2, 2)]);
     }
-    if (L.j == 0) T[0] = cscale(cz(), a.tau_g);
-    __syncwarp(L.mask);
   }
-  // ---- F = exp(W1) * U  (nspt.cc:429): exp into Y (W holds the square of
-  // W1), U_mu(x) restaged into W
-  ser_exp<MO>(T, W, Y, N, L);
-  stage(W, a.U, a.Uf, mu, self, a.g, N, L);
-  const bool zm = a.Lg != nullptr;
-  double2 *Fc = a.F + (size_t)mu * plane_mu + site;
-  product<MO, false>(LeftS{Y}, make_double2(1.0, 0.0), W, W[0], N, L,
-                     [&](int k, int r, double2 v) {
-                       Fc[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
-                       if (zm) W[sidx(k, r, c)] = v;
-                     });
-  if (L.j == 0) a.Ff[(size_t)mu * V + site] = W[0];
-  if (!zm) return;
   __syncwarp(L.mask);
-  // ---- MM[mu] += log(F[link])  (nspt.cc:432-439): logs stored per link
-  double2 *Lo = a.Lg + (size_t)mu * plane_mu + site;
-  ser_log<MO>(W, T, Y, N, L, [&](int k, int r, double2 v) {
-    Lo[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
-  });
+  // W1 = c0 W1 + c1 W2 (ptSU3 operator*(double) and +, flags included)
+  for (int e = L.j; e < 1 + 9 * N; e += GROUP)
+    T[e] = cadd(cscale(T[e], a.c0), cscale(E[e], a.c1));
+  __syncwarp(L.mask);
+  update_link(a, T, Y, W, link, mu, site, self, L);
 }
 
 // Advance a device step counter by one (a kernel, so that it replays

@@ -21,8 +21,10 @@
 // -G ntt,ntx,nty,ntz the thread grid whose order the local gauge fixing
 // reproduces (choices.h:124-128; default: the finest the reference accepts),
 // -Z 0|1 zero-mode subtraction (default: on with periodic boundaries, as
-// REMOVE_GLUON_ZEROMOM), -P device Philox noise instead of the reference's
-// rand55 stream.  The update is the Jacobi one (UPDATE_ONTHEFLY off).
+// REMOVE_GLUON_ZEROMOM), -A tlsym|iwa|dbw2 an improved gauge action
+// (GAUGE_ACTION; file names and the plaquette file's extra two columns of
+// rectangle traces follow Quenched.cc:327-348 and nspt.cc:586-597), -P
+// device Philox noise instead of the reference's rand55 stream.  The update is the Jacobi one (UPDATE_ONTHEFLY off).
 // With periodic boundaries the Wilson loops of ComputeLoops (__MANY_LOOP__,
 // the reference's periodic default) go to <plaq_out>_nxm_SU3_wil_..._o<N>.txt
 // after every BEAT steps and at the end (nspt.cc:1283-1306).  Not
@@ -53,6 +55,7 @@ struct Params {
   bool fa = false, philox = false;
   int zm = -1;  // -1: as the boundary conditions imply
   int grid[4] = {0, 0, 0, 0};
+  unsigned action = 0;  // NSPT_ACTION_* or 0 (Wilson)
 };
 
 // get_val (Quenched.cc:97-114): the next word must be `key`, then a value.
@@ -120,6 +123,7 @@ void usage() {
          "-F\t\tFourier-accelerated gauge fixing (periodic boundaries)\n"
          "-G a,b,c,d\tthread grid (ntt,ntx,nty,ntz) of the local gauge fixing\n"
          "-Z 0|1\t\tzero-mode subtraction off/on\n"
+         "-A action\timproved gauge action: tlsym, iwa or dbw2\n"
          "-P\t\tdevice Philox noise instead of the reference's generator\n\n");
 }
 
@@ -167,7 +171,7 @@ int main(int argc, char **argv) {
     }
   if (!read_cfg(p)) return 1;
   int opt;
-  while ((opt = getopt(argc, argv, "l:s:b:d:r:g:a:t:p:c:n:hT:FG:Z:P")) != -1) {
+  while ((opt = getopt(argc, argv, "l:s:b:d:r:g:a:t:p:c:n:hT:FG:Z:PA:")) != -1) {
     switch (opt) {
       case 'l': p.L[0] = p.L[1] = p.L[2] = p.L[3] = atoi(optarg); break;
       case 's': p.sweep = atoi(optarg); break;
@@ -200,6 +204,15 @@ int main(int argc, char **argv) {
         break;
       case 'Z': p.zm = atoi(optarg); break;
       case 'P': p.philox = true; break;
+      case 'A':
+        if (!strcmp(optarg, "tlsym")) p.action = NSPT_ACTION_TLSYM;
+        else if (!strcmp(optarg, "iwa")) p.action = NSPT_ACTION_IWA;
+        else if (!strcmp(optarg, "dbw2")) p.action = NSPT_ACTION_DBW2;
+        else {
+          fprintf(stderr, "nspt_quenched: -A takes tlsym, iwa or dbw2\n");
+          return 1;
+        }
+        break;
       default: usage(); return 1;
     }
   }
@@ -217,10 +230,14 @@ int main(int argc, char **argv) {
   }
   const bool periodic = p.twist == 0;
   const bool zm = p.zm < 0 ? periodic : p.zm != 0;
-  unsigned flags = p.twist | (zm ? NSPT_ZEROMODE : 0u) | (p.fa ? NSPT_GF_FA : NSPT_GF_LOCAL);
+  unsigned flags = p.twist | (zm ? NSPT_ZEROMODE : 0u) | (p.fa ? NSPT_GF_FA : NSPT_GF_LOCAL) |
+                   p.action;
 
   // file names (Quenched.cc:376-407)
-  const char *type = "SU3_wil";
+  const char *type = p.action == NSPT_ACTION_TLSYM  ? "SU3_tls"
+                     : p.action == NSPT_ACTION_IWA  ? "SU3_iwa"
+                     : p.action == NSPT_ACTION_DBW2 ? "SU3_dbw"
+                                                    : "SU3_wil";
   const std::string plaq_name = p.plaqn + "_" + stem(p, type) + ".txt";
   const std::string conf_name = p.confn + stem(p, type);
   const std::string log_name = stem(p, type) + ".log";
@@ -256,7 +273,7 @@ int main(int argc, char **argv) {
   if (p.grid[0] && (rc = nspt_set_gf_grid(ctx, p.grid))) return fail(ctx, rc, "thread grid");
   const int N = p.N;
   std::vector<double> plaq(2 * (N + 1)), w(2 * (N + 1)), norm(N), tru(8 * N);
-  std::vector<double> loops(8 * (N + 1));
+  std::vector<double> loops(8 * (N + 1)), w2(2 * (N + 1));
   // ComputeLoops' line: per loop (1x2, 2x2, 2x4, 4x4) the even orders
   auto write_loops = [&]() -> int {
     if (!loopf) return NSPT_OK;
@@ -296,14 +313,23 @@ int main(int argc, char **argv) {
       if ((rc = nspt_gauge_wilson(ctx, p.tau_g))) return fail(ctx, rc, "gauge_wilson");
       if ((rc = nspt_observables(ctx, plaq.data(), norm.data(), tru.data())))
         return fail(ctx, rc, "observables");
-      for (int k = 0; k < N; k++) {  // nspt.cc:576-591
-        fprintf(plaqf, "%.30e\t%.30e\n", plaq[2 * k], plaq[2 * k + 1]);
+      if (p.action && (rc = nspt_rect_observables(ctx, w2.data())))
+        return fail(ctx, rc, "observables");
+      auto plaq_line = [&](int k) {  // nspt.cc:576-597
+        if (p.action)
+          fprintf(plaqf, "%.30e\t%.30e\t%.30e\t%.30e\n", plaq[2 * k], plaq[2 * k + 1], w2[2 * k],
+                  w2[2 * k + 1]);
+        else
+          fprintf(plaqf, "%.30e\t%.30e\n", plaq[2 * k], plaq[2 * k + 1]);
+      };
+      for (int k = 0; k < N; k++) {
+        plaq_line(k);
         fprintf(normf, "%g\n", norm[k]);
         for (int mu = 0; mu < 4; mu++)
           fprintf(truf, "%g\t%g\t", tru[2 * (mu * N + k)], tru[2 * (mu * N + k) + 1]);
         fprintf(truf, "\n");
       }
-      fprintf(plaqf, "%.30e\t%.30e\n", plaq[2 * N], plaq[2 * N + 1]);
+      plaq_line(N);
       if (zm && (rc = nspt_zero_modes_subtraction(ctx))) return fail(ctx, rc, "zero modes");
       if (p.fa)
         rc = nspt_fa_gauge_fixing(ctx, p.alpha);

@@ -39,13 +39,17 @@ CASES = [
          alpha=-0.1, seed=5, start=11, zm=True),
     dict(name="rand_pbc_localgf_n4", L=(4, 4, 4, 4), N=4, bc="pbc", gf="local", steps=2,
          dt=0.01, alpha=-0.05, seed=8, start=3, zm=True),
+    dict(name="rand_pbc_tlsym_n4", L=(4, 4, 4, 4), N=4, bc="pbc", gf="local", steps=2,
+         dt=0.01, alpha=0.0, seed=19, start=13, zm=True, action="tlsym"),
 ]
+C1 = {"wil": 0.0, "tlsym": -1.0 / 12.0, "iwa": -0.331, "dbw2": -1.4088}
 
 LINK_SITES = 6  # sites of the final field kept in the fixture
 
 
 def make_case(c: dict) -> dict:
-    binary = O.build_reference(c["N"], c["bc"], c["gf"])
+    action = c.get("action", "wil")
+    binary = O.build_reference(c["N"], c["bc"], c["gf"], (1, 1, 1), action)
     with tempfile.TemporaryDirectory() as d:
         start = "cold"
         twist_mask = 6 if c["bc"] == "tw" else 0
@@ -56,11 +60,17 @@ def make_case(c: dict) -> dict:
             start = os.path.join(d, "start.dat")
         r = O.run_reference(binary, c["L"], c["steps"], c["dt"], c["alpha"], c["seed"], d,
                             start=start, noise=True, twist_init=(c["bc"] == "tw"))
-    return dict(
+    out = dict(
         plaq=r["plaq"], norm=r["norm"], tru=r["tru"], plaq0=r["plaq0"],
         plaq_final=r["plaq_final"], links=r["links"][:LINK_SITES],
         noise0=r["noise"][0][:64],
     )
+    if action != "wil":
+        # rectangle traces; the reference's top order is a running sum over
+        # the steps (w2[PTORD] is never reset), the others are per step
+        out["w2"] = r["w2"]
+        out["c1"] = C1[action]
+    return out
 
 
 def main():

@@ -76,7 +76,9 @@ def test_driver_replays_reference_fixture(driver, oracle_mod, tmp_path, path):
     alpha, seed, start = float(g["alpha"]), int(g["seed"]), int(g["start"])
     twisted, fa, zm = bool(g["twisted"]), bool(g["fa"]), bool(g["zm"])
     V = int(np.prod(L))
-    name = stem(L, alpha, dt, N)
+    action = {-1.0 / 12.0: "tlsym", -0.331: "iwa", -1.4088: "dbw2"}.get(
+        float(g["c1"]) if "c1" in g else 0.0, "wil")
+    name = stem(L, alpha, dt, N).replace("SU3_wil", "SU3_" + action[:3])
     write_cfg(tmp_path, L, steps, steps, dt, alpha, 1 if start >= 0 else 0, N, seed)
     write_damocle(tmp_path, dt, alpha)
     if start >= 0:
@@ -90,9 +92,18 @@ def test_driver_replays_reference_fixture(driver, oracle_mod, tmp_path, path):
         args += ["-F"]
     if not zm:
         args += ["-Z", "0"]
+    if action != "wil":
+        args += ["-A", action]
     r = subprocess.run(args, cwd=tmp_path, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
-    plaq = np.loadtxt(tmp_path / ("plaq_" + name + ".txt")).reshape(steps, N + 1, 2)
+    raw = np.loadtxt(tmp_path / ("plaq_" + name + ".txt"))
+    if action != "wil":  # w1 and w2 columns (nspt.cc:586-597)
+        w2 = raw[:, 2:].reshape(steps, N + 1, 2)
+        raw = raw[:, :2]
+        for s in range(steps):
+            ok, w = obs_close(w2[s][:N], g["w2"][s][:N], 1e-11)
+            assert ok, ("w2", s, w)
+    plaq = raw.reshape(steps, N + 1, 2)
     norm = np.loadtxt(tmp_path / (name + ".nor")).reshape(steps, N)
     for s in range(steps):
         ok, w = obs_close(plaq[s], g["plaq"][s], 1e-11)

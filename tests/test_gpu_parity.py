@@ -141,8 +141,13 @@ def test_reference_golden_fixture(engine_mod, oracle_mod, path):
     N = int(g["N"])
     twist = "yz" if bool(g["twisted"]) else ""
     fa, zm, alpha = bool(g["fa"]), bool(g["zm"]), float(g["alpha"])
-    e, o = make_pair(engine_mod, oracle_mod, L, N, twist=twist, zm=zm, fa=fa, alpha=alpha,
-                     start=int(g["start"]) if int(g["start"]) >= 0 else None)
+    action = {-1.0 / 12.0: "tlsym", -0.331: "iwa", -1.4088: "dbw2"}.get(
+        float(g["c1"]) if "c1" in g else 0.0, "wil")
+    o = oracle_mod.Oracle(L, N, twist_mask=6 if twist else 0)
+    if int(g["start"]) >= 0:
+        o.random_start(int(g["start"]), 0.5)
+    e = engine_mod.NsptEngine(L, N, twist=twist, zero_modes=zm, fa=fa, alpha=alpha, action=action)
+    e.upload(o.links)
     ok, w = obs_close(e.plaquette_measure(), g["plaq0"], 1e-12)
     assert ok, ("start plaquette", w)
     if local_gf:
@@ -155,6 +160,9 @@ def test_reference_golden_fixture(engine_mod, oracle_mod, path):
         for name, a, b in (("plaq", ob.plaq, g["plaq"][s]), ("norm", ob.norm, g["norm"][s])):
             ok, w = obs_close(a, b, 1e-11)
             assert ok, (name, s, w)
+        if action != "wil":  # orders below N (the reference's top order is cumulative)
+            ok, w = obs_close(e.rect_observables()[:N], g["w2"][s][:N], 1e-11)
+            assert ok, ("w2", s, w)
         if zm:
             e.zero_modes_subtraction()
         if fa:
@@ -305,3 +313,29 @@ def test_wilson_loops_match_oracle(engine_mod, oracle_mod, L, N):
     for q in range(4):
         ok, w = obs_close(got[q], want[q], 1e-12)
         assert ok, (q, w)
+
+
+@pytest.mark.parametrize("action,c1,L,N", [("tlsym", -1.0 / 12.0, (4, 4, 4, 4), 6),
+                                           ("iwa", -0.331, (6, 4, 4, 4), 4),
+                                           ("dbw2", -1.4088, (4, 4, 4, 4), 8)])
+def test_improved_action_sweeps_match_oracle(engine_mod, oracle_mod, action, c1, L, N):
+    """gauge_wilson with an improved action (nspt.cc:272-308): links, the
+    plaquette and the rectangle traces w2, two sweeps with zero modes."""
+    P, O = engine_mod, oracle_mod
+    o = O.Oracle(L, N)
+    o.random_start(88, 0.5)
+    o.set_action(c1)
+    e = P.NsptEngine(L, N, zero_modes=True, action=action)
+    e.upload(o.links)
+    rng = O.Rand55(9)
+    for s in range(2):
+        nz = rng.gauss(o.V * 32)
+        e.set_noise(nz)
+        eo = e.gauge_wilson(0.01)
+        oo = o.sweep(0.01, nz, zero_modes=True)
+        check_obs(eo, oo, 1e-12 if s == 0 else 1e-11)
+        ok, w = obs_close(e.rect_observables(), o.last_w2(), 1e-12 if s == 0 else 1e-11)
+        assert ok, ("w2", s, w)
+        e.zero_modes_subtraction()
+        o.zero_modes()
+    assert per_order_rel(e.download(), o.links, N).max() <= 1e-11

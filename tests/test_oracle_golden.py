@@ -20,6 +20,8 @@ def replay(O, g):
     o = O.Oracle(L, N, twist_mask=6 if bool(g["twisted"]) else 0)
     if int(g["start"]) >= 0:
         o.random_start(int(g["start"]), 0.5)
+    if "c1" in g:
+        o.set_action(float(g["c1"]))
     p0 = o.plaquette()
     rng = O.Rand55(int(g["seed"]))
     obs = []
@@ -29,6 +31,8 @@ def replay(O, g):
         if s == 0:
             noise0 = nz[:64].copy()
         ob = o.sweep(float(g["dt"]), nz, zero_modes=bool(g["zm"]))
+        if "c1" in g:
+            ob.w2 = o.last_w2()
         obs.append(ob)
         if bool(g["zm"]):
             o.zero_modes()
@@ -52,6 +56,9 @@ def test_oracle_matches_reference_golden(oracle_mod, path):
                            ("tru", ob.tru.transpose(1, 0, 2), g["tru"][s].transpose(1, 0, 2))):
             ok, w = obs_close(a, b, TOL)
             assert ok, (name, s, w)
+        if "c1" in g:  # orders below N; the reference's top order is cumulative
+            ok, w = obs_close(ob.w2[:N], g["w2"][s][:N], TOL)
+            assert ok, ("w2", s, w)
     rel = per_order_rel(o.links[: g["links"].shape[0]], g["links"], N)
     assert rel.max() <= TOL, rel
     ok, w = obs_close(o.plaquette(), g["plaq_final"][: N + 1], TOL)
