@@ -356,7 +356,9 @@ def run_c2(args, world, rank, local):
     import prlgt2020_b200 as P
     from prlgt2020_b200.replicas import max_over_ranks, replica_seed, whole_job_rate
     torch.cuda.set_device(local)
-    L, N, alpha, dt = (16, 16, 16, 16), 20, -0.05, 0.01
+    # FA with alpha > 0: its step multiplies by -alpha/p^2 (nspt.cc:888-892); the
+    # negative alpha of the reference's Quench.cfg makes FA grow exponentially
+    L, N, alpha, dt = (16, 16, 16, 16), 20, 0.05, 0.01
     V = int(np.prod(L))
     peak = P.fp64_peak_tflops()
     eng = P.NsptEngine(L, N, zero_modes=True, fa=True, alpha=alpha)
@@ -421,7 +423,7 @@ def run_c4(args, world, rank, local):
     import prlgt2020_b200 as P
     from prlgt2020_b200.replicas import max_over_ranks, replica_seed, whole_job_rate
     torch.cuda.set_device(local)
-    nrep, N, alpha = 64, 12, -0.05
+    nrep, N, alpha = 64, 12, 0.05  # FA damps for alpha > 0 (nspt.cc:888-892)
     Ls = [(v,) * 4 for v in (6, 8, 10) for _ in range(1)]
     L = [Ls[r % 3] for r in range(nrep)]
     dts = [(0.005, 0.01, 0.02)[(r // 3) % 3] for r in range(nrep)]
@@ -484,6 +486,116 @@ def run_c4(args, world, rank, local):
         print(json.dumps(line), flush=True)
 
 
+def run_c5(args, world, rank, local):
+    """Float-float Cauchy products against the plain FP64 path, periodic,
+    zero modes + FA gauge fixing every step, same seed on both.  FA runs
+    with alpha = +0.05: the reference's FA step multiplies by -alpha/p^2
+    (nspt.cc:888-892), and with the negative alpha of its Quench.cfg (meant for
+    the local gauge fixing) the reference's own FA path grows exponentially
+    in Langevin time at every order.
+    Speed at 24^4 x 40 orders: the sweep kernel and the whole step, each
+    engine alone.  Accuracy at 8^4 x 40 (so that 1000 steps take about a
+    minute): from a common field (20 FP64 steps from a cold start) the
+    float-float and the FP64 engine run on with the same noise, and the
+    per-order relative difference max|ff - fp64| / max|fp64| over each
+    order's coefficients is taken after 1, 100 and 1000 steps.  Beside it,
+    the same figure for a second FP64 run whose dt is larger by one part in
+    2^52: the growth of a rounding-level difference that FP64 itself
+    cannot avoid, i.e. the accuracy an FP64 run has at that order."""
+    import numpy as np
+    import torch
+
+    import prlgt2020_b200 as P
+    from prlgt2020_b200.replicas import max_over_ranks, replica_seed
+    torch.cuda.set_device(local)
+    N, alpha, dt = 40, 0.05, 0.01
+    kw = dict(zero_modes=True, fa=True, alpha=alpha)
+    seed = replica_seed(5000, rank)
+    K = args.steps
+    Pn = N * (N - 1) // 2
+    E = (N - 1) * N * (N + 1) // 6
+    speed = {}
+    L = (24, 24, 24, 24)
+    V = int(np.prod(L))
+    for prec in ("fp64", "ff"):
+        eng = P.NsptEngine(L, N, precision=prec, **kw)
+        eng.seed(seed, 0)
+        eng.NsptEvolve(dt, args.warmup, 1)
+        kern = 0.0
+        for _ in range(K):
+            eng.gauge_wilson(dt)
+            kern += eng.last_kernel_ms()
+            eng.zero_modes_subtraction()
+            eng.FAstochastic_gauge_fixing(alpha)
+        eng.NsptEvolve(dt, K, 1)
+        step_ms = max_over_ranks(eng.last_step_ms()) / K
+        kern = max_over_ranks(kern) / K
+        f = (14 * Pn + 2 * E) * 216.0 * 4 * V
+        speed[prec] = {"step_ms": step_ms, "sweep_kernel_ms": kern,
+                       "sweep_canonical_tflops": f / (kern * 1e-3) / 1e12}
+        if prec == "ff":
+            speed[prec]["scale_exponent"] = eng.ff_scale()
+        eng.close()
+    # accuracy: float-float vs FP64 from a common field, same noise
+    La, warm = (8, 8, 8, 8), 20
+    base = P.NsptEngine(La, N, **kw)
+    base.seed(seed, 0)
+    base.NsptEvolve(dt, warm, 1)
+    start = base.download()
+    base.close()
+    ff = P.NsptEngine(La, N, precision="ff", **kw)
+    ref = P.NsptEngine(La, N, **kw)
+    pert = P.NsptEngine(La, N, **kw)
+    for e in (ff, ref, pert):
+        e.upload(start)
+        e.seed(seed, warm)
+    dt_pert = dt * (1.0 + 2.0 ** -52)
+
+    def rel_per_order(a, b):
+        a = a.reshape(-1, 2 + 18 * N)
+        b = b.reshape(-1, 2 + 18 * N)
+        out = []
+        for k in range(1, N + 1):
+            sl = slice(2 + 18 * (k - 1), 2 + 18 * k)
+            den = np.abs(b[:, sl]).max()
+            out.append(float(np.abs(a[:, sl] - b[:, sl]).max() / den))
+        return out
+
+    err, done = {}, 0
+    for m in (1, 100, 1000):
+        ff.NsptEvolve(dt, m - done, 1)
+        ref.NsptEvolve(dt, m - done, 1)
+        pert.NsptEvolve(dt_pert, m - done, 1)
+        done = m
+        r = ref.download()
+        e_ff = rel_per_order(ff.download(), r)
+        e_64 = rel_per_order(pert.download(), r)
+        err[str(m)] = {"ff_vs_fp64": e_ff, "fp64_ulp_dt_vs_fp64": e_64,
+                       "ff_max": max(e_ff), "fp64_ulp_dt_max": max(e_64),
+                       "finite": bool(np.isfinite(r).all())}
+    for e in (ff, ref, pert):
+        e.close()
+    if rank == 0:
+        line = {
+            "metric": "Langevin steps/s at 24^4 x 40 orders, float-float Cauchy products "
+                      "(ZM + FA every step)",
+            "value": 1e3 / speed["ff"]["step_ms"] * world, "unit": "steps/s",
+            "n_gpus": world, "steps": K, "warmup": args.warmup,
+            "ms_per_step": speed["ff"]["step_ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32x2 products, f64 elsewhere",
+            "data": "synthetic (cold start + warm-up, device Philox noise, same seed both paths)",
+            "config": {"workload": "c5_24^4_N40_ff_vs_fp64", "L": list(L), "N": N, "dt": dt,
+                       "alpha": alpha, "accuracy_lattice": list(La),
+                       "accuracy_start": "%d FP64 steps from a cold start" % warm},
+            "fp64": speed["fp64"], "ff": speed["ff"],
+            "ff_over_fp64_speed": speed["fp64"]["step_ms"] / speed["ff"]["step_ms"],
+            "ff_over_fp64_sweep_kernel": speed["fp64"]["sweep_kernel_ms"]
+                                         / speed["ff"]["sweep_kernel_ms"],
+            "per_order_rel_error_after_steps": err,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -496,10 +608,12 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-gf", action="store_true", help="skip the gauge-fixing figure")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "c2", "c4"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "c2", "c4", "c5"],
                     help="sweep: 32^4 x 24 twisted (the headline); c2: 16^4 x 20 periodic "
                          "with zero modes and FA gauge fixing every step, per pass; c4: 64 "
-                         "replicas of 6^4..10^4 x 12, batched in one CUDA graph vs plain")
+                         "replicas of 6^4..10^4 x 12, batched in one CUDA graph vs plain; "
+                         "c5: 24^4 x 40 float-float products vs FP64, speed and per-order "
+                         "error after 1/100/1000 steps")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -510,6 +624,9 @@ def main():
         return
     if args.workload == "c4":
         run_c4(args, world, rank, local)
+        return
+    if args.workload == "c5":
+        run_c5(args, world, rank, local)
         return
     run_ours(args, world, rank, local)
 

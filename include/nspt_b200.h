@@ -54,6 +54,12 @@ extern "C" {
 #define NSPT_ACTION_TLSYM (1u << 7)  /* tree-level Symanzik, c1 = -1/12 */
 #define NSPT_ACTION_IWA (1u << 8)    /* Iwasaki, c1 = -0.331 */
 #define NSPT_ACTION_DBW2 (1u << 9)   /* DBW2, c1 = -1.4088 */
+/* Float-float Cauchy products in the Wilson sweep: the staple and
+ * U*staples products run in compensated FP32 pairs (48 significant bits)
+ * with a per-order scale 2^(e k); exp, log, exp*U, the force, the
+ * accumulations and everything else stay FP64.  No reference counterpart
+ * (the reference multiplies in double, QCDpt.h operator*); Wilson action. */
+#define NSPT_PRECISION_FF (1u << 10)
 
 typedef struct nspt_ctx nspt_ctx;
 
@@ -141,6 +147,20 @@ int nspt_plaquette_measure(nspt_ctx *ctx, double *plaq);
  * 2x4; it prints the real parts of the even orders).  NSPT_ERR_STATE with
  * twisted boundaries. */
 int nspt_wilson_loops(nspt_ctx *ctx, double *loops);
+
+/* WL2x2 (nspt.cc:1064-1140, __WILLOOP_2x2__, periodic boundaries): trace of
+ * the 2x2 Wilson loop summed over all planes and sites, per order 0..N,
+ * loop[(N+1)*2], normalised by 1/(18V); the reference prints the real parts
+ * of orders 2, 4, ... (its ptU[1], ptU[3], ...).  NSPT_ERR_STATE with
+ * twisted boundaries. */
+int nspt_wl2x2(nspt_ctx *ctx, double *loop);
+
+/* Per-order scale of the float-float products (NSPT_PRECISION_FF): with
+ * automatic != 0 (the default) each sweep fits e to the field, so that
+ * 2^(e k) max|U_k| is about the same for every order k; otherwise e is
+ * fixed (|e| N <= 1000).  nspt_get_ff_scale gives the e of the last sweep. */
+int nspt_set_ff_scale(nspt_ctx *ctx, int automatic, int e);
+int nspt_get_ff_scale(nspt_ctx *ctx, int *e);
 
 /* Configuration files in the reference's binary format
  * (QCDenvNODEpt_test.h:359-374: field, then (allocORD+1) complex plaquette).

@@ -17,7 +17,9 @@
 # -D__PARALLEL_OMP__ -O3 -fopenmp -std=c++0x) plus
 #   * a choices.h generated from the reference's copy with sed: allocORD = N,
 #     UPDATE_ONTHEFLY off (the reference's Jacobi option, nspt.cc:428-430 and
-#     nspt.cc:992), the boundary conditions and the thread grid;
+#     nspt.cc:992), the boundary conditions and the thread grid, and
+#     __WILLOOP_2x2__ on (choices.h:77, periodic builds; WL2x2 only adds a
+#     measurement that the harness runs on request);
 #   * -DPBC for periodic builds, which the FA path needs for p2hat[0]
 #     (lattice.h:1144-1149) and the zero-momentum cut (nspt.cc:881-883);
 #   * -D__FA_GAUGE_FIXING__ for GF=fa (nspt.cc:1019-1023);
@@ -41,7 +43,8 @@ SED=(-e "s/^#define allocORD 6\$/#define allocORD $N/"
      -e "s/^#define UPDATE_ONTHEFLY\$/\/* UPDATE_ONTHEFLY off: Jacobi update *\//"
      -e "s/^#define ntx  1\$/#define ntx  $NTX/"
      -e "s/^#define nty  1\$/#define nty  $NTY/"
-     -e "s/^#define ntz  1\$/#define ntz  $NTZ/")
+     -e "s/^#define ntz  1\$/#define ntz  $NTZ/"
+     -e "s/^\/\/#define __WILLOOP_2x2__\$/#define __WILLOOP_2x2__/")
 DEFS=(-DDSFMT_MEXP=19937 -DUSE_RAND55 -D__PARALLEL_OMP__)
 if [ "$BC" = tw ]; then
   SED+=(-e "s/^#define PERIODIC_BC\$/\/* PERIODIC_BC off *\//"
@@ -64,6 +67,7 @@ else
   rm -f "$OUT/cfg/choices.h.new"
 fi
 grep -q "^#define allocORD $N\$" "$OUT/cfg/choices.h"
+grep -q "^#define __WILLOOP_2x2__" "$OUT/cfg/choices.h"  # inside #ifdef PERIODIC_BC
 CXX=${ORACLE_CXX:-/usr/bin/g++}
 FLAGS=(-O3 -fopenmp -std=c++11 -w "${DEFS[@]}" -I"$OUT/cfg" -I- -I"$REF"
        -I"$REF/ranlxd" -I"$HERE/fftw_shim")

@@ -229,7 +229,8 @@ def write_config(path: str, links: np.ndarray, plaq: np.ndarray):
 
 def run_reference(binary: str, L, steps: int, dt: float, alpha: float, seed: int,
                   workdir: str, start: str = "cold", noise: bool = True,
-                  twist_init: bool = False, project: bool = False, timing: bool = False):
+                  twist_init: bool = False, project: bool = False, timing: bool = False,
+                  wl2x2: bool = False):
     """Run the reference harness; returns dict of parsed outputs."""
     out = os.path.join(workdir, "ref")
     cmd = [binary, "--L", *[str(x) for x in L], "--steps", str(steps), "--dt", repr(dt),
@@ -242,6 +243,8 @@ def run_reference(binary: str, L, steps: int, dt: float, alpha: float, seed: int
         cmd.append("--project")
     if timing:
         cmd.append("--time")
+    if wl2x2:
+        cmd += ["--wl2x2", out + ".wl2x2"]
     p = subprocess.run(cmd, check=True, capture_output=True, text=True)
     V = int(np.prod(L))
     res = {"stdout": p.stdout}
@@ -259,4 +262,6 @@ def run_reference(binary: str, L, steps: int, dt: float, alpha: float, seed: int
     res["links"], res["plaq_final"] = read_config(out + ".dat", V, N)
     if noise:
         res["noise"] = np.fromfile(out + ".noise", dtype=np.float64).reshape(steps, V * 4 * 8)
+    if wl2x2:  # WL2x2 (nspt.cc:1118-1124): Re Tr /(18V) of ptU[1], ptU[3], ...
+        res["wl2x2"] = np.atleast_1d(np.loadtxt(out + ".wl2x2"))
     return res

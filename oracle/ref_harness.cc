@@ -75,7 +75,7 @@ static void usage() {
   fprintf(stderr,
           "ref_harness --L l0 l1 l2 l3 --steps S --dt DT --alpha A --seed S "
           "--start cold|FILE --out PREFIX [--noise FILE] [--twist-init] "
-          "[--project] [--time] [--loops FILE]\n");
+          "[--project] [--time] [--loops FILE] [--wl2x2 FILE]\n");
   exit(2);
 }
 
@@ -84,7 +84,7 @@ int main(int argc, char **argv) {
   int steps = 1;
   double dt = 0.01, alpha = 0.0;
   long seed = 12345;
-  std::string start = "cold", out = "ref", noise_path, loops_path;
+  std::string start = "cold", out = "ref", noise_path, loops_path, wl2x2_path;
   bool twist_init = false, project = false, timing = false;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
@@ -112,6 +112,8 @@ int main(int argc, char **argv) {
       timing = true;
     } else if (a == "--loops" && i + 1 < argc) {
       loops_path = argv[++i];
+    } else if (a == "--wl2x2" && i + 1 < argc) {
+      wl2x2_path = argv[++i];
     } else {
       usage();
     }
@@ -181,6 +183,18 @@ int main(int argc, char **argv) {
 #else
   if (!loops_path.empty()) {
     fprintf(stderr, "ref_harness: --loops needs a periodic build\n");
+    return 2;
+  }
+#endif
+
+#ifdef __WILLOOP_2x2__
+  /* WL2x2's stream (nspt.cc:1064-1140): the 2x2 loops of the final field */
+  loop2x2.open(wl2x2_path.empty() ? "/dev/null" : wl2x2_path.c_str());
+  loop2x2.precision(17);
+  loop2x2 << std::scientific;
+#else
+  if (!wl2x2_path.empty()) {
+    fprintf(stderr, "ref_harness: --wl2x2 needs a periodic build\n");
     return 2;
   }
 #endif
@@ -278,6 +292,10 @@ int main(int argc, char **argv) {
   plaquette_measure(Umu, act_pars);
 #ifdef __MANY_LOOP__
   if (!loops_path.empty()) ComputeLoops(Umu);
+#endif
+#ifdef __WILLOOP_2x2__
+  if (!wl2x2_path.empty()) WL2x2(Umu);
+  loop2x2.close();
 #endif
   std::string conf = out + ".dat";
   std::vector<char> name(conf.begin(), conf.end());

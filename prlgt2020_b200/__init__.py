@@ -120,10 +120,16 @@ class NsptEngine:
     fa          Fourier-accelerated Landau gauge fixing (nspt.cc:866-948)
     alpha       act_pars.alpha as in Quench.cfg (negative in the reference
                 config; FA multiplies by -alpha/p^2)
+    local_gf    local stochastic gauge fixing (nspt.cc:660-862)
+    action      "wil", or an improved action "tlsym", "iwa", "dbw2"
+                (Quenched.cc:311-322)
+    precision   "fp64", or "ff": the sweep's Cauchy products in compensated
+                float-float with a per-order scale (Wilson action)
     """
 
     def __init__(self, L, N: int, twist: str = "", zero_modes: bool = False, fa: bool = False,
-                 alpha: float = 0.0, local_gf: bool = False, action: str = "wil"):
+                 alpha: float = 0.0, local_gf: bool = False, action: str = "wil",
+                 precision: str = "fp64"):
         lib = load_library()
         self.L = tuple(int(x) for x in L)
         if len(self.L) != 4:
@@ -141,6 +147,7 @@ class NsptEngine:
             flags |= NSPT_GF_LOCAL
         flags |= {"wil": 0, "tlsym": _lib.NSPT_ACTION_TLSYM, "iwa": _lib.NSPT_ACTION_IWA,
                   "dbw2": _lib.NSPT_ACTION_DBW2}[action]
+        flags |= {"fp64": 0, "ff": _lib.NSPT_PRECISION_FF}[precision]
         self.flags = flags
         self.alpha = float(alpha)
         arr = (ctypes.c_int * 4)(*self.L)
@@ -274,6 +281,30 @@ class NsptEngine:
         out = np.zeros((self.N + 1, 2))
         self._check(load_library().nspt_rect_observables(self._h, _dp(out)),
                     "nspt_rect_observables")
+        return out
+
+    def set_ff_scale(self, e=None):
+        """Float-float products: fixed per-order scale exponent e (order k
+        multiplied by 2^(e k) before the split), or None to fit it to the
+        field every sweep (the default)."""
+        lib = load_library()
+        if e is None:
+            self._check(lib.nspt_set_ff_scale(self._h, 1, 0), "nspt_set_ff_scale")
+        else:
+            self._check(lib.nspt_set_ff_scale(self._h, 0, int(e)), "nspt_set_ff_scale")
+
+    def ff_scale(self) -> int:
+        """Scale exponent the last float-float sweep used."""
+        e = ctypes.c_int(0)
+        self._check(load_library().nspt_get_ff_scale(self._h, ctypes.byref(e)),
+                    "nspt_get_ff_scale")
+        return e.value
+
+    def WL2x2(self) -> np.ndarray:
+        """WL2x2 of nspt.cc:1064-1140: [N+1, 2] trace of the 2x2 loop per
+        order, /(18V); the reference prints the real parts of orders 2, 4, ..."""
+        out = np.zeros((self.N + 1, 2))
+        self._check(load_library().nspt_wl2x2(self._h, _dp(out)), "nspt_wl2x2")
         return out
 
     def ComputeLoops(self) -> np.ndarray:

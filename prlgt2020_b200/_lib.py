@@ -34,6 +34,7 @@ NSPT_GF_LOCAL = 1 << 6
 NSPT_ACTION_TLSYM = 1 << 7
 NSPT_ACTION_IWA = 1 << 8
 NSPT_ACTION_DBW2 = 1 << 9
+NSPT_PRECISION_FF = 1 << 10
 
 # every entry point the header declares: name -> (restype, argtypes)
 _P = ctypes.c_void_p
@@ -61,6 +62,9 @@ SIGNATURES = {
     "nspt_plaquette_measure": (_I, [_P, _D]),
     "nspt_rect_observables": (_I, [_P, _D]),
     "nspt_wilson_loops": (_I, [_P, _D]),
+    "nspt_wl2x2": (_I, [_P, _D]),
+    "nspt_set_ff_scale": (_I, [_P, _I, _I]),
+    "nspt_get_ff_scale": (_I, [_P, ctypes.POINTER(_I)]),
     "nspt_save_config": (_I, [_P, ctypes.c_char_p, _I]),
     "nspt_load_config": (_I, [_P, ctypes.c_char_p, _I, _D]),
     "nspt_last_step_ms": (ctypes.c_double, [_P]),

@@ -58,6 +58,9 @@ struct nspt_ctx {
   int sweep_warps;               // warps per CTA of the sweep, 0 = as many as fit
   double c1;                     // improved action weight (0: Wilson), c0 = 1 - 8 c1
   double2 *obs_tr2;              // [(N+1)][4V] rectangle traces (improved actions)
+  int *ff_e;                     // float-float scale exponent used by the sweep (device)
+  unsigned long long *ff_mx;     // [N] per-order max |U_k| (bit patterns)
+  bool ff_auto;                  // fit the exponent each sweep
   double2 *loop_part;            // Wilson loops: per-CTA rows and the summed row
   size_t loop_part_n;
   double *noise;  // injected noise
@@ -115,6 +118,12 @@ static KernelShape choose_shape(const nspt_ctx *ctx, int slots, long units, int 
   return k;
 }
 
+template <bool MEASURE, bool FF>
+static void sweep_kernel(dim3 grid, dim3 blk, size_t smem, cudaStream_t st, const SweepArgs &a) {
+  cudaFuncSetAttribute(k_sweep<MEASURE, FF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_sweep<MEASURE, FF><<<grid, blk, smem, st>>>(a);
+}
+
 static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
   const long nl = 4 * ctx->V;
   KernelShape k = choose_shape(ctx, SWEEP_SLOTS, nl, RING,
@@ -124,13 +133,13 @@ static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
   const long per_cta = (long)k.warps * LPW;
   const unsigned grid = (unsigned)((nl + per_cta - 1) / per_cta);
   const dim3 blk(32 * k.warps);
-  if (measure) {
-    cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_sweep<true><<<grid, blk, smem, ctx->st>>>(a);
-  } else {
-    cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_sweep<false><<<grid, blk, smem, ctx->st>>>(a);
-  }
+  const bool ff = (ctx->flags & NSPT_PRECISION_FF) != 0;
+  if (measure)
+    sweep_kernel<true, false>(grid, blk, smem, ctx->st, a);
+  else if (ff)
+    sweep_kernel<false, true>(grid, blk, smem, ctx->st, a);
+  else
+    sweep_kernel<false, false>(grid, blk, smem, ctx->st, a);
   CK(cudaGetLastError());
   return NSPT_OK;
 }
@@ -201,6 +210,7 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   a.obs_tr2 = ctx->obs_tr2;
   a.c1 = ctx->c1;
   a.c0 = 1. - 8. * ctx->c1;
+  a.ff_scale = ctx->ff_e;
   // QuenchedAllocate: stau = sqrt(tau_g); tau_g /= -(2 NC)  (Quenched.cc:584-589)
   a.stau = sqrt(dt);
   double tg = dt;
@@ -209,6 +219,14 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   a.N = ctx->N;
   a.SS = ctx->SS;
   a.g = ctx->geo;
+  if ((ctx->flags & NSPT_PRECISION_FF) && ctx->ff_auto) {
+    // per-order scale of the float-float products, fitted to this field
+    CK(cudaMemsetAsync(ctx->ff_mx, 0, ctx->N * sizeof(unsigned long long), ctx->st));
+    k_order_absmax<<<dim3(2 * ctx->nsm, ctx->N), 256, 0, ctx->st>>>(ctx->U, ctx->N,
+                                                                    (size_t)ctx->V, ctx->ff_mx);
+    k_ff_fit<<<1, 1, 0, ctx->st>>>(ctx->ff_mx, ctx->N, ctx->ff_e);
+    CK(cudaGetLastError());
+  }
   const bool timed = ctx->kcount < nspt_ctx::KEV;
   if (timed) CK(cudaEventRecord(ctx->kev[2 * ctx->kcount], ctx->st));
   int rc = ctx->c1 != 0.0 ? launch_sweep_imp(ctx, a) : launch_sweep(ctx, a, false);
@@ -389,7 +407,7 @@ static int upload_constants(nspt_ctx *ctx) {
 
 static void free_all(nspt_ctx *ctx) {
   void *ptrs[] = {ctx->U, ctx->Uf, ctx->F, ctx->Ff, ctx->Lg, ctx->Wg, ctx->Gx, ctx->p2, ctx->dcounter,
-                  ctx->loop_part, ctx->obs_tr2,
+                  ctx->loop_part, ctx->obs_tr2, ctx->ff_e, ctx->ff_mx,
                   ctx->obs_tr, ctx->obs_tru, ctx->obs_norm, ctx->red2, ctx->red1, ctx->noise};
   for (void *p : ptrs)
     if (p) cudaFree(p);
@@ -402,8 +420,10 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   if (N < 1 || N > NSPT_MAX_ORDER) return NSPT_ERR_ORDER;
   const unsigned actions = NSPT_ACTION_TLSYM | NSPT_ACTION_IWA | NSPT_ACTION_DBW2;
   const unsigned known = NSPT_TWIST_Y | NSPT_TWIST_Z | NSPT_TWIST_T | NSPT_ZEROMODE | NSPT_GF_FA |
-                         NSPT_GF_LOCAL | actions;
+                         NSPT_GF_LOCAL | actions | NSPT_PRECISION_FF;
   if (flags & ~known) return NSPT_ERR_ARG;
+  // float-float products are built into the Wilson sweep only
+  if ((flags & NSPT_PRECISION_FF) && (flags & actions)) return NSPT_ERR_ARG;
   if (__builtin_popcount(flags & actions) > 1) return NSPT_ERR_ARG;
   // the reference has improved actions with periodic boundaries only (choices.h:110)
   if ((flags & actions) && (flags & (NSPT_TWIST_Y | NSPT_TWIST_Z | NSPT_TWIST_T)))
@@ -434,6 +454,9 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->loop_part = nullptr;
   ctx->loop_part_n = 0;
   ctx->obs_tr2 = nullptr;
+  ctx->ff_e = nullptr;
+  ctx->ff_mx = nullptr;
+  ctx->ff_auto = true;
   // improved action parameters, Quenched.cc:311-322
   ctx->c1 = (flags & NSPT_ACTION_TLSYM) ? -1.0 / 12.0
           : (flags & NSPT_ACTION_IWA)   ? -0.331
@@ -501,6 +524,9 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
             alloc((void **)&ctx->dcounter, sizeof(unsigned long long));
   if (ok && (flags & (NSPT_ZEROMODE | NSPT_GF_FA))) ok = alloc((void **)&ctx->Lg, field);
   if (ok && ctx->c1 != 0.0) ok = alloc((void **)&ctx->obs_tr2, (N + 1) * nl * sizeof(double2));
+  if (ok && (flags & NSPT_PRECISION_FF))
+    ok = alloc((void **)&ctx->ff_e, sizeof(int)) &&
+         alloc((void **)&ctx->ff_mx, N * sizeof(unsigned long long));
   if (ok && (flags & NSPT_GF_FA))
     ok = alloc((void **)&ctx->Wg, field / 4) && alloc((void **)&ctx->Gx, field / 4);
   if (!ok) {
@@ -509,7 +535,8 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
     return fail(NSPT_ERR_NOMEM);
   }
   if (upload_constants(ctx) != NSPT_OK) return fail(NSPT_ERR_CUDA);
-  if (cudaMemsetAsync(ctx->dcounter, 0, sizeof(unsigned long long), ctx->st) != cudaSuccess) {
+  if (cudaMemsetAsync(ctx->dcounter, 0, sizeof(unsigned long long), ctx->st) != cudaSuccess ||
+      (ctx->ff_e && cudaMemsetAsync(ctx->ff_e, 0, sizeof(int), ctx->st) != cudaSuccess)) {
     cudaStreamDestroy(ctx->st);
     return fail(NSPT_ERR_CUDA);
   }
@@ -669,9 +696,9 @@ extern "C" int nspt_fa_gauge_fixing(nspt_ctx *ctx, double alpha) {
   return timed_end(ctx);
 }
 
-extern "C" int nspt_wilson_loops(nspt_ctx *ctx, double *loops) {
-  if (!ctx || !loops) return NSPT_ERR_ARG;
-  if (ctx->geo.twist) return NSPT_ERR_STATE;  // the reference has them with periodic bc only
+// Sums over planes and sites of the 1x2, 2x2, 2x4 and 4x4 loop traces,
+// h[q * (N+1) + k], un-normalised (k_loops, then its per-CTA rows summed)
+static int loop_sums(nspt_ctx *ctx, std::vector<double2> &h) {
   const int N = ctx->N, row = 4 * (N + 1);
   const size_t gb = ((size_t)LOOP_SLOTS * ctx->SS + RING + row) * sizeof(double2);
   const int warps = (int)std::min<size_t>(8, ctx->smem_optin / (LPW * gb));
@@ -699,9 +726,18 @@ extern "C" int nspt_wilson_loops(nspt_ctx *ctx, double *loops) {
   CK(cudaGetLastError());
   k_rows_sum<<<(row + 127) / 128, 128, 0, ctx->st>>>(part, grid, row, res);
   CK(cudaGetLastError());
-  std::vector<double2> h(row);
+  h.resize(row);
   CK(cudaMemcpyAsync(h.data(), res, row * sizeof(double2), cudaMemcpyDeviceToHost, ctx->st));
-  if ((rc = timed_end(ctx))) return rc;
+  return timed_end(ctx);
+}
+
+extern "C" int nspt_wilson_loops(nspt_ctx *ctx, double *loops) {
+  if (!ctx || !loops) return NSPT_ERR_ARG;
+  if (ctx->geo.twist) return NSPT_ERR_STATE;  // the reference has them with periodic bc only
+  const int N = ctx->N;
+  std::vector<double2> h;
+  int rc = loop_sums(ctx, h);
+  if (rc) return rc;
   // loopNorm = 1/(3*2*3*V), halved for 1x2 and 2x4 (nspt.cc:1280-1306)
   const double norm = 1. / (3 * 2 * 3 * (double)ctx->V);
   const double fac[4] = {.5 * norm, norm, .5 * norm, norm};
@@ -710,6 +746,24 @@ extern "C" int nspt_wilson_loops(nspt_ctx *ctx, double *loops) {
       loops[2 * (q * (N + 1) + k)] = h[q * (N + 1) + k].x * fac[q];
       loops[2 * (q * (N + 1) + k) + 1] = h[q * (N + 1) + k].y * fac[q];
     }
+  return NSPT_OK;
+}
+
+extern "C" int nspt_wl2x2(nspt_ctx *ctx, double *loop) {
+  if (!ctx || !loop) return NSPT_ERR_ARG;
+  if (ctx->geo.twist) return NSPT_ERR_STATE;  // __WILLOOP_2x2__ is periodic only (choices.h:75-78)
+  const int N = ctx->N;
+  std::vector<double2> h;
+  int rc = loop_sums(ctx, h);
+  if (rc) return rc;
+  // WL2x2 walks each plane's 2x2 loop the other way round from ComputeLoops'
+  // 2x2 (mu > nu, along mu first): its trace is the complex conjugate.
+  // Normalisation rVol * D18 (nspt.cc:1121).
+  const double norm = 1. / (18. * (double)ctx->V);
+  for (int k = 0; k <= N; k++) {
+    loop[2 * k] = h[(N + 1) + k].x * norm;
+    loop[2 * k + 1] = -h[(N + 1) + k].y * norm;
+  }
   return NSPT_OK;
 }
 
@@ -775,6 +829,37 @@ extern "C" int nspt_observables(nspt_ctx *ctx, double *plaq, double *norm, doubl
         trU[2 * (mu * N + k)] = t.x / (double)(3 * ctx->V);
         trU[2 * (mu * N + k) + 1] = t.y / (double)(3 * ctx->V);
       }
+  return NSPT_OK;
+}
+
+extern "C" int nspt_set_ff_scale(nspt_ctx *ctx, int automatic, int e) {
+  if (!ctx) return NSPT_ERR_ARG;
+  if (!(ctx->flags & NSPT_PRECISION_FF)) {
+    ctx->err = "float-float scale: context created without NSPT_PRECISION_FF";
+    return NSPT_ERR_STATE;
+  }
+  if (automatic) {
+    ctx->ff_auto = true;
+    return NSPT_OK;
+  }
+  if ((long)std::abs(e) * ctx->N > 1000) {
+    ctx->err = "float-float scale: |e| N above 1000";
+    return NSPT_ERR_ARG;
+  }
+  ctx->ff_auto = false;
+  CK(cudaMemcpyAsync(ctx->ff_e, &e, sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
+  return NSPT_OK;
+}
+
+extern "C" int nspt_get_ff_scale(nspt_ctx *ctx, int *e) {
+  if (!ctx || !e) return NSPT_ERR_ARG;
+  if (!(ctx->flags & NSPT_PRECISION_FF)) {
+    ctx->err = "float-float scale: context created without NSPT_PRECISION_FF";
+    return NSPT_ERR_STATE;
+  }
+  CK(cudaMemcpyAsync(e, ctx->ff_e, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+  CK(cudaStreamSynchronize(ctx->st));
   return NSPT_OK;
 }
 

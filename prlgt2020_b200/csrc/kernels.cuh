@@ -202,6 +202,7 @@ struct SweepArgs {
   const unsigned long long *stepp;  // device step counter (Philox), or null: use step
   double2 *obs_tr2;    // [(N+1)][4V] Tr(U * rectangle staples), improved actions
   double c0, c1;       // improved action weights (Quenched.cc:311-322)
+  const int *ff_scale;  // float-float products: per-order scale exponent (device)
   double tau_g, stau;  // -dt/6, sqrt(dt)  (Quenched.cc:584-589)
   int N, SS;
   Geo g;
@@ -298,8 +299,9 @@ __device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, doub
 constexpr int SWEEP_THREADS = NSPT_SWEEP_THREADS;
 constexpr int SWEEP_SLOTS = 3;
 
-template <bool MEASURE>
+template <bool MEASURE, bool FF = false>
 __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
+  const int ffe = FF ? *a.ff_scale : 0;
   extern __shared__ double2 sm[];
   Lane L;
   int g;
@@ -329,7 +331,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
       const double2 a0 = __ldg(a.Uf + (size_t)nu * V + site);
       const LeftG A{a.U + nu * plane_mu + site, V, ring};
       // T holds dag(U_nu(x) U_mu(x+nu))
-      product<MO, false>(A, a0, Y, Y[0], N, L,
+      cprod<FF, MO, false>(A, a0, Y, Y[0], N, L, ffe,
                          [&](int k, int r, double2 v) { T[sidx(k, c, r)] = cconj(v); });
       if (L.j == 0) T[0] = cconj(flag_mul(a0, Y[0]));
       __syncwarp(L.mask);
@@ -341,7 +343,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
       const double2 a0 = Y[0];
       const double2 b0 = T[0];
       const bool f0 = first;
-      product<MO, false>(LeftS{Y}, a0, T, b0, N, L, [&](int k, int r, double2 v) {
+      cprod<FF, MO, false>(LeftS{Y}, a0, T, b0, N, L, ffe, [&](int k, int r, double2 v) {
         double2 &w = W[sidx(k, r, c)];
         w = f0 ? v : cadd(w, v);
       });
@@ -359,13 +361,13 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
       // of a result cell reads only that cell's own column of the left operand
       stage(T, a.U, a.Uf, mu, d, a.g, N, L);
       const double2 a0 = T[0], y0 = Y[0];
-      product<MO, false>(LeftS{T}, a0, Y, y0, N, L,
+      cprod<FF, MO, false>(LeftS{T}, a0, Y, y0, N, L, ffe,
                          [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
       if (L.j == 0) T[0] = flag_mul(a0, y0);
       __syncwarp(L.mask);
       stage(Y, a.U, a.Uf, nu, d, a.g, N, L);
       const double2 ta = cconj(T[0]);
-      product<MO, true>(LeftS{T}, ta, Y, Y[0], N, L, [&](int k, int r, double2 v) {
+      cprod<FF, MO, true>(LeftS{T}, ta, Y, Y[0], N, L, ffe, [&](int k, int r, double2 v) {
         double2 &w = W[sidx(k, r, c)];
         w = cadd(w, v);
       });
@@ -379,7 +381,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
   self.fwd = self.bwd = 0;
   stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
   const double2 pflag = flag_mul(Y[0], wflag);
-  product<MO, false>(LeftS{Y}, Y[0], W, wflag, N, L,
+  cprod<FF, MO, false>(LeftS{Y}, Y[0], W, wflag, N, L, ffe,
                      [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
   if (L.j == 0) T[0] = pflag;
   __syncwarp(L.mask);
@@ -1094,6 +1096,54 @@ __global__ void k_rowsum(const T *__restrict__ in, size_t stride, long n, T *out
 }
 
 // MMs[mu][e] = MM[mu][e] * (1/V)  (MM[mu] *= rVol, nspt.cc:607-609)
+// ---------------- float-float scale exponent ----------------
+
+// mx[k-1] = max over the field's order-k entries of max(|re|, |im|), as the
+// bit pattern of a non-negative double (ordered like the value); one row of
+// blocks per order (blockIdx.y), mx zeroed by the caller
+__global__ void k_order_absmax(const double2 *__restrict__ U, int N, size_t V,
+                               unsigned long long *mx) {
+  const int k = blockIdx.y + 1;
+  const size_t per = 9 * V;  // entries of one order in one direction plane
+  double m = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < 4 * per;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const size_t mu = i / per, r = i - mu * per;
+    const double2 v = __ldg(U + (mu * 9 * N + 9 * (size_t)(k - 1)) * V + r);
+    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0 && m > 0.0)
+    atomicMax(mx + (k - 1), (unsigned long long)__double_as_longlong(m));
+}
+
+// Per-order scale exponent: order k is multiplied by 2^(e k) before its
+// float-float split.  e = -(slope of log2 max|U_k| over k), a least-squares
+// fit over the orders that are non-zero, so that the scaled orders keep one
+// common size whatever their geometric growth or decay; |e| N <= 1000.
+__global__ void k_ff_fit(const unsigned long long *mx, int N, int *e_out) {
+  double sk = 0, sl = 0, skk = 0, skl = 0;
+  int n = 0;
+  for (int k = 1; k <= N; k++) {
+    const double m = __longlong_as_double((long long)mx[k - 1]);
+    if (m > 0.0) {
+      const double l = (double)ilogb(m);
+      sk += k;
+      sl += l;
+      skk += (double)k * k;
+      skl += k * l;
+      n++;
+    }
+  }
+  int e = 0;
+  if (n >= 2) {
+    const double slope = (n * skl - sk * sl) / (n * skk - sk * sk);
+    e = (int)rint(-slope);
+  }
+  const int lim = 1000 / (N > 0 ? N : 1);
+  *e_out = max(-lim, min(lim, e));
+}
+
 __global__ void k_scale_mm(double2 *MM, int n, double rvol) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) MM[i] = cscale(MM[i], rvol);

@@ -245,6 +245,153 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
   }
 }
 
+// ---------------- compensated float-float Cauchy product ----------------
+//
+// The same truncated product as product(), with every 3x3 multiply-add of
+// the triangle in float-float arithmetic: a double x is split into
+// hi = fl32(x 2^e) and lo = fl32(x 2^e - hi) (48 significant bits together);
+// a product of two such numbers is formed with an exact FP32 product
+// (p = xh yh, err = fma(xh, yh, -p)) plus the cross terms, and added to the
+// accumulator by an error-free two-sum whose error is carried in the low
+// word.  Order i of the left operand and order j of the right one are
+// scaled by 2^(e i) and 2^(e j) before the split (exact), so that orders of
+// very different size keep inside the FP32 exponent range; the order-k
+// result is scaled back by 2^(-e k) when it is rejoined into FP64.  The flag
+// terms, the output and everything around the products stay FP64.
+struct ffc {
+  float rh, rl, ih, il;  // re = rh + rl, im = ih + il
+};
+
+// 2^n as a double, exact for -1022 <= n <= 1023
+__device__ __forceinline__ double pow2i(int n) { return __hiloint2double((1023 + n) << 20, 0); }
+
+__device__ __forceinline__ ffc ff_split(double2 v, double scale) {
+  const double x = v.x * scale, y = v.y * scale;
+  const float xh = __double2float_rn(x), yh = __double2float_rn(y);
+  return {xh, __double2float_rn(x - (double)xh), yh, __double2float_rn(y - (double)yh)};
+}
+
+// (ah, al) += (xh, xl) (yh, yl); rounding-explicit so nothing is contracted
+__device__ __forceinline__ void ff_mac(float &ah, float &al, float xh, float xl, float yh,
+                                       float yl) {
+  const float p = __fmul_rn(xh, yh);
+  float e = __fmaf_rn(xh, yh, -p);
+  e = __fmaf_rn(xh, yl, e);
+  e = __fmaf_rn(xl, yh, e);
+  const float s = __fadd_rn(ah, p);
+  const float b = __fsub_rn(s, ah);
+  const float err = __fadd_rn(__fsub_rn(ah, __fsub_rn(s, b)), __fsub_rn(p, b));
+  ah = s;
+  al = __fadd_rn(al, __fadd_rn(err, e));
+}
+
+__device__ __forceinline__ void ff_cmac(ffc &acc, const ffc &a, const ffc &b) {
+  ff_mac(acc.rh, acc.rl, a.rh, a.rl, b.rh, b.rl);
+  ff_mac(acc.rh, acc.rl, -a.ih, -a.il, b.ih, b.il);
+  ff_mac(acc.ih, acc.il, a.rh, a.rl, b.ih, b.il);
+  ff_mac(acc.ih, acc.il, a.ih, a.il, b.rh, b.rl);
+}
+
+// product() with the triangle in float-float; e: per-order scale exponent,
+// |e| * M <= 1022 (the caller clamps it).
+template <int MO, bool DA, class Left, class Emit>
+__device__ __forceinline__ void product_ff(const Left &A, double2 a0, const double2 *B, double2 b0,
+                                           int M, const Lane &L, int e, Emit emit) {
+  const int c = L.c;
+  constexpr int PASS = 3 * MO;
+  const int npass = (M + PASS - 1) / PASS;
+  for (int ps = npass - 1; ps >= 0; --ps) {
+    const int kb = ps * PASS;
+    const int kend = min(kb + PASS, M);
+    ffc acc[MO][3];
+#pragma unroll
+    for (int q = 0; q < MO; q++)
+#pragma unroll
+      for (int r = 0; r < 3; r++) acc[q][r] = {0.f, 0.f, 0.f, 0.f};
+    double2 a[9];
+    if constexpr (Left::kRing) {
+      if (1 < kend) A.issue(1, L.j);
+      cp_commit();
+      if (2 < kend) A.issue(2, L.j);
+      cp_commit();
+    }
+    for (int i = 1; i < kend; i++) {
+      if constexpr (Left::kRing) {
+        cp_wait1();
+        __syncwarp(L.mask);
+        if (i + 2 < kend) A.issue(i + 2, L.j);
+        cp_commit();
+        A.template from_ring<DA>(i, a);
+      } else {
+        A.template load<DA>(i, a);
+      }
+      ffc af[9];
+      const double sa = pow2i(e * i);
+#pragma unroll
+      for (int t = 0; t < 9; t++) af[t] = ff_split(a[t], sa);
+#pragma unroll
+      for (int q = 0; q < MO; q++) {
+        const int k = kb + L.s + 1 + 3 * q;
+        if (k <= kend && k > i) {
+          const double2 *bj = B + 1 + 9 * (k - i - 1) + 3 * c;
+          const double sb = pow2i(e * (k - i));
+          const ffc b0_ = ff_split(bj[0], sb), b1 = ff_split(bj[1], sb), b2 = ff_split(bj[2], sb);
+#pragma unroll
+          for (int r = 0; r < 3; r++) {
+            ff_cmac(acc[q][r], af[3 * r], b0_);
+            ff_cmac(acc[q][r], af[3 * r + 1], b1);
+            ff_cmac(acc[q][r], af[3 * r + 2], b2);
+          }
+        }
+      }
+    }
+    if constexpr (Left::kRing) cp_wait0();
+    __syncwarp(L.mask);
+    const bool fa = !cis0(a0), fb = !cis0(b0);
+#pragma unroll
+    for (int q = 0; q < MO; q++) {
+      const int k = kb + L.s + 1 + 3 * q;
+      if (k <= kend) {
+        double2 ak[3];
+        if (fb) A.template col<DA>(k, c, ak);
+        const double su = pow2i(-e * k);
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          const ffc &f = acc[q][r];
+          double2 v = make_double2(((double)f.rh + (double)f.rl) * su,
+                                   ((double)f.ih + (double)f.il) * su);
+          if (fa || fb) {
+            double2 u;
+            if (!fa)
+              u = cmul(b0, ak[r]);
+            else if (!fb)
+              u = cmul(a0, B[sidx(k, r, c)]);
+            else
+              u = cadd(cmul(b0, ak[r]), cmul(a0, B[sidx(k, r, c)]));
+            v = cadd(v, u);
+          }
+          emit(k, r, v);
+        }
+      }
+    }
+    __syncwarp(L.mask);
+  }
+}
+
+// Orders per lane and pass of the float-float product: its accumulators
+// take as many registers as the FP64 ones, its split operands twice as many.
+constexpr int MO_FF = 4;
+
+// product() or product_ff(), chosen at compile time
+template <bool FF, int MO, bool DA, class Left, class Emit>
+__device__ __forceinline__ void cprod(const Left &A, double2 a0, const double2 *B, double2 b0,
+                                      int M, const Lane &L, int e, Emit emit) {
+  if constexpr (FF)
+    product_ff<MO_FF, DA>(A, a0, B, b0, M, L, e, emit);
+  else
+    product<MO, DA>(A, a0, B, b0, M, L, emit);
+}
+
 // Polynomial p(X) = sum_{n<=N} coef(n) X^n of a series X with flag 0,
 // truncated at order N, by Paterson-Stockmeyer with block 2.  Y = X^2 is
 // formed once; then Horner in Y,

@@ -27,8 +27,10 @@
 // device Philox noise instead of the reference's rand55 stream.  The update is the Jacobi one (UPDATE_ONTHEFLY off).
 // With periodic boundaries the Wilson loops of ComputeLoops (__MANY_LOOP__,
 // the reference's periodic default) go to <plaq_out>_nxm_SU3_wil_..._o<N>.txt
-// after every BEAT steps and at the end (nspt.cc:1283-1306).  Not
-// reproduced: the 2x2-only file of __WILLOOP_2x2__.
+// after every BEAT steps and at the end (nspt.cc:1283-1306); with -W also
+// the 2x2 loops of WL2x2 (__WILLOOP_2x2__, periodic only) go to
+// <plaq_out>2x2_SU3_wil_..._o<N>.txt at the same points (Quenched.cc:389-393,
+// 658-660, 737-739; nspt.cc:1118-1124).
 #include <getopt.h>
 #include <unistd.h>
 
@@ -52,7 +54,7 @@ struct Params {
   long seed = 0;
   std::string plaqn, confn, damon = "damocle.dag";
   unsigned twist = 0;
-  bool fa = false, philox = false;
+  bool fa = false, philox = false, wl2x2 = false;
   int zm = -1;  // -1: as the boundary conditions imply
   int grid[4] = {0, 0, 0, 0};
   unsigned action = 0;  // NSPT_ACTION_* or 0 (Wilson)
@@ -124,7 +126,8 @@ void usage() {
          "-G a,b,c,d\tthread grid (ntt,ntx,nty,ntz) of the local gauge fixing\n"
          "-Z 0|1\t\tzero-mode subtraction off/on\n"
          "-A action\timproved gauge action: tlsym, iwa or dbw2\n"
-         "-P\t\tdevice Philox noise instead of the reference's generator\n\n");
+         "-P\t\tdevice Philox noise instead of the reference's generator\n"
+         "-W\t\t2x2 Wilson loops file (WL2x2, periodic boundaries)\n\n");
 }
 
 // AggiornaParametri's damocle.dag read (Quenched.cc:677-685)
@@ -171,7 +174,7 @@ int main(int argc, char **argv) {
     }
   if (!read_cfg(p)) return 1;
   int opt;
-  while ((opt = getopt(argc, argv, "l:s:b:d:r:g:a:t:p:c:n:hT:FG:Z:PA:")) != -1) {
+  while ((opt = getopt(argc, argv, "l:s:b:d:r:g:a:t:p:c:n:hT:FG:Z:PA:W")) != -1) {
     switch (opt) {
       case 'l': p.L[0] = p.L[1] = p.L[2] = p.L[3] = atoi(optarg); break;
       case 's': p.sweep = atoi(optarg); break;
@@ -204,6 +207,7 @@ int main(int argc, char **argv) {
         break;
       case 'Z': p.zm = atoi(optarg); break;
       case 'P': p.philox = true; break;
+      case 'W': p.wl2x2 = true; break;
       case 'A':
         if (!strcmp(optarg, "tlsym")) p.action = NSPT_ACTION_TLSYM;
         else if (!strcmp(optarg, "iwa")) p.action = NSPT_ACTION_IWA;
@@ -250,6 +254,16 @@ int main(int argc, char **argv) {
     fprintf(stderr, "nspt_quenched: cannot open %s\n", loops_name.c_str());
     return 1;
   }
+  const std::string wl_name = p.plaqn + "2x2_" + stem(p, type) + ".txt";
+  if (p.wl2x2 && !periodic) {
+    fprintf(stderr, "nspt_quenched: -W (WL2x2) needs periodic boundaries\n");
+    return 1;
+  }
+  FILE *wlf = p.wl2x2 ? fopen(wl_name.c_str(), "a") : nullptr;
+  if (p.wl2x2 && !wlf) {
+    fprintf(stderr, "nspt_quenched: cannot open %s\n", wl_name.c_str());
+    return 1;
+  }
   FILE *normf = fopen(norm_name.c_str(), "w");
   FILE *truf = fopen(tru_name.c_str(), "w");
   FILE *logf = fopen(log_name.c_str(), "w");
@@ -283,6 +297,17 @@ int main(int argc, char **argv) {
       for (int k = 0; k <= N; k += 2) fprintf(loopf, "%.30e\t", loops[2 * (q * (N + 1) + k)]);
     fprintf(loopf, "\n");
     fflush(loopf);
+    return NSPT_OK;
+  };
+  // WL2x2's line: Re Tr of orders 2, 4, ... <= N (its ptU[1], ptU[3], ...)
+  std::vector<double> wl(2 * (N + 1));
+  auto write_wl2x2 = [&]() -> int {
+    if (!wlf) return NSPT_OK;
+    const int r = nspt_wl2x2(ctx, wl.data());
+    if (r) return r;
+    for (int k = 2; k <= N; k += 2) fprintf(wlf, "%.30e\t", wl[2 * k]);
+    fprintf(wlf, "\n");
+    fflush(wlf);
     return NSPT_OK;
   };
   if (p.init) {  // hot start from the saved configuration (Quenched.cc:612-637)
@@ -341,7 +366,8 @@ int main(int argc, char **argv) {
     fflush(plaqf);
     fflush(normf);
     fflush(truf);
-    // AggiornaParametri (Quenched.cc:662-713)
+    // AggiornaParametri (Quenched.cc:656-713)
+    if ((rc = write_wl2x2())) return fail(ctx, rc, "WL2x2");
     if ((rc = write_loops())) return fail(ctx, rc, "ComputeLoops");
     fprintf(logf, "______________________________________\n\n");
     stamp(logf, "Damocle Update");
@@ -367,6 +393,8 @@ int main(int argc, char **argv) {
   if ((rc = nspt_plaquette_measure(ctx, plaq.data()))) return fail(ctx, rc, "plaquette");
   printf("Misura della placchetta:\n");
   for (int k = 0; k <= N; k++) printf("%e\t%e\n", plaq[2 * k], plaq[2 * k + 1]);
+  if ((rc = write_wl2x2())) return fail(ctx, rc, "WL2x2");
+  if (wlf) fclose(wlf);
   if ((rc = write_loops())) return fail(ctx, rc, "ComputeLoops");
   if (loopf) fclose(loopf);
   if ((rc = nspt_save_config(ctx, conf_name.c_str(), N))) return fail(ctx, rc, "save");

@@ -88,6 +88,8 @@ def test_driver_replays_reference_fixture(driver, oracle_mod, tmp_path, path):
     args = [driver, "-G", "1,1,1,1"]  # the fixtures' reference builds run one thread
     if twisted:
         args += ["-T", "yz"]
+    else:
+        args += ["-W"]
     if fa:
         args += ["-F"]
     if not zm:
@@ -132,3 +134,8 @@ def test_driver_replays_reference_fixture(driver, oracle_mod, tmp_path, path):
         for q in range(4):
             ok, w = obs_close(got[q], want[q], 1e-11)
             assert ok, ("loops", q, w)
+        # WL2x2's file: Re Tr of the 2x2 loop, orders 2, 4, ... <= N
+        wl = np.atleast_2d(np.loadtxt(tmp_path / ("plaq2x2_" + name + ".txt")))
+        assert wl.shape == (2, N // 2)
+        ok, w = obs_close(wl[-1], o.wilson_loops()[1, 2::2, 0], 1e-11)
+        assert ok, ("wl2x2", w)

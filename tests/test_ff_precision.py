@@ -1,0 +1,102 @@
+"""Float-float Cauchy products (NSPT_PRECISION_FF) against the FP64 oracle.
+
+The float-float sweep computes the staple and U*staples products in pairs of
+FP32 numbers (48 significant bits, error-free products and two-sums) with a
+per-order scale 2^(e k); exp, log, exp*U and the accumulations stay FP64.
+Its per-order error therefore sits a few bits above FP64 rounding: the bound
+here is 1e-11 per order after one sweep (FP64 path: 1e-12), in the same
+per-order metric as test_gpu_parity.py (max|gpu - oracle| / max|oracle| over
+the order-k coefficients of all links).  The same seed on the FP64 engine
+gives a different field (the products really ran in float-float), and with
+the scale fixed at e = 0 the high orders of a field that grows tenfold per
+order overflow FP32 -- the per-order rescaling is what keeps them.
+"""
+import numpy as np
+import pytest
+
+from helpers import flag_diff, obs_close, per_order_rel
+
+pytestmark = pytest.mark.gpu
+
+FF_TOL = 1e-11
+
+
+def _pair(P, O, L, N, start, precision):
+    o = O.Oracle(L, N)
+    if start is not None:
+        o.random_start(start, 0.5)
+    e = P.NsptEngine(L, N, precision=precision)
+    e.upload(o.links)
+    return e, o
+
+
+def _sweeps(O, e, o, steps, dt, seed):
+    rng = O.Rand55(seed)
+    for _ in range(steps):
+        nz = rng.gauss(o.V * 32)
+        e.set_noise(nz)
+        eo = e.gauge_wilson(dt)
+        oo = o.sweep(dt, nz)
+    return eo, oo
+
+
+@pytest.mark.parametrize("L,N", [((4, 4, 4, 4), 8), ((2, 4, 2, 4), 24)])
+def test_ff_one_sweep_random_start(engine_mod, oracle_mod, L, N):
+    e, o = _pair(engine_mod, oracle_mod, L, N, 77 + N, "ff")
+    d, _ = _pair(engine_mod, oracle_mod, L, N, 77 + N, "fp64")
+    start = o.links.copy()
+    eo, oo = _sweeps(oracle_mod, e, o, 1, 0.01, 5)
+    o2 = oracle_mod.Oracle(L, N)
+    o2.set_links(start)
+    _sweeps(oracle_mod, d, o2, 1, 0.01, 5)
+    rel = per_order_rel(e.download(), o.links, N)
+    assert rel.max() <= FF_TOL, rel
+    assert flag_diff(e.download(), o.links, N) == 0.0
+    for name, a, b in (("plaq", eo.plaq, oo.plaq), ("norm", eo.norm, oo.norm)):
+        ok, w = obs_close(a, b, FF_TOL)
+        assert ok, (name, w)
+    # the FP64 engine on the same input differs from the float-float one
+    assert np.abs(d.download() - e.download()).max() > 0.0
+    assert per_order_rel(d.download(), o.links, N).max() <= 1e-12
+
+
+def test_ff_high_orders_need_the_rescaling(engine_mod, oracle_mod):
+    """A random start whose order-k coefficients grow about tenfold per order
+    (2e44 at k = 40, above FP32's largest number from k ~ 34 on): with the
+    fitted scale every order stays within FF_TOL of the oracle after a
+    sweep; with the scale fixed at e = 0 the top orders overflow FP32."""
+    L, N = (2, 4, 2, 4), 40
+    o = oracle_mod.Oracle(L, N)
+    o.random_start(3, 4.0)
+    auto = engine_mod.NsptEngine(L, N, precision="ff")
+    fixed = engine_mod.NsptEngine(L, N, precision="ff")
+    auto.upload(o.links)
+    fixed.upload(o.links)
+    fixed.set_ff_scale(0)
+    nz = oracle_mod.Rand55(9).gauss(o.V * 32)
+    for e in (auto, fixed):
+        e.set_noise(nz)
+        e.gauge_wilson(0.01)
+    o.sweep(0.01, nz)
+    assert auto.ff_scale() < 0 and fixed.ff_scale() == 0
+    rel = per_order_rel(auto.download(), o.links, N)
+    assert rel.max() <= FF_TOL, rel
+    with np.errstate(invalid="ignore"):
+        lost = per_order_rel(fixed.download(), o.links, N)
+    assert not np.isfinite(lost[-1]) or lost[-1] > 1e-3, lost
+
+
+def test_ff_options_checked(engine_mod):
+    P = engine_mod
+    with pytest.raises(P.NsptError):
+        P.NsptEngine((4, 4, 4, 4), 4, action="tlsym", precision="ff")
+    e = P.NsptEngine((4, 4, 4, 4), 20, precision="ff")
+    with pytest.raises(P.NsptError):
+        e.set_ff_scale(51)  # |e| N > 1000
+    e.set_ff_scale(-50)
+    e.set_ff_scale(None)
+    d = P.NsptEngine((4, 4, 4, 4), 4)
+    with pytest.raises(P.NsptError):
+        d.set_ff_scale(1)
+    with pytest.raises(P.NsptError):
+        d.ff_scale()

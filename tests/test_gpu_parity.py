@@ -313,6 +313,18 @@ def test_wilson_loops_match_oracle(engine_mod, oracle_mod, L, N):
     for q in range(4):
         ok, w = obs_close(got[q], want[q], 1e-12)
         assert ok, (q, w)
+    # WL2x2 (nspt.cc:1064-1140): the 2x2 loop walked the other way round
+    want22 = want[1] * np.array([1.0, -1.0])
+    ok, w = obs_close(e.WL2x2(), want22, 1e-12)
+    assert ok, ("wl2x2", w)
+
+
+def test_wilson_loops_need_periodic_boundaries(engine_mod):
+    e = engine_mod.NsptEngine((4, 4, 4, 4), 4, twist="yz")
+    with pytest.raises(engine_mod.NsptError):
+        e.ComputeLoops()
+    with pytest.raises(engine_mod.NsptError):
+        e.WL2x2()
 
 
 @pytest.mark.parametrize("action,c1,L,N", [("tlsym", -1.0 / 12.0, (4, 4, 4, 4), 6),

@@ -91,7 +91,9 @@ def test_oracle_local_gauge_fixing_matches_reference_thread_grid(oracle_mod, cas
 def test_oracle_wilson_loops_match_reference(oracle_mod, L, N, start):
     """ComputeLoops (nspt.cc:1148-1312) on a random configuration: the
     reference prints the real parts of the even orders of the 1x2, 2x2, 2x4
-    and 4x4 loops (periodic builds)."""
+    and 4x4 loops (periodic builds).  WL2x2 (nspt.cc:1064-1140) prints the
+    2x2 loop traversed the other way round, Re Tr /(18V) of ptU[1], ptU[3],
+    ... (orders 2, 4, ...): the real part of the same 2x2 trace."""
     O = oracle_mod
     b = O.ref_binary(N, "pbc", "local")
     if not os.path.exists(b) or os.path.getmtime(b) < os.path.getmtime(
@@ -104,16 +106,21 @@ def test_oracle_wilson_loops_match_reference(oracle_mod, L, N, start):
     with tempfile.TemporaryDirectory() as d:
         O.write_config(os.path.join(d, "s.dat"), o.links, o.plaquette())
         loops = os.path.join(d, "loops.txt")
+        wl = os.path.join(d, "wl2x2.txt")
         import subprocess
         subprocess.run([b, "--L", *[str(x) for x in L], "--steps", "0", "--start",
-                        os.path.join(d, "s.dat"), "--out", os.path.join(d, "r"), "--loops", loops],
-                       check=True, capture_output=True)
+                        os.path.join(d, "s.dat"), "--out", os.path.join(d, "r"), "--loops", loops,
+                        "--wl2x2", wl], check=True, capture_output=True)
         ref = np.loadtxt(loops).reshape(4, -1)
+        ref22 = np.atleast_1d(np.loadtxt(wl))
     got = o.wilson_loops()[:, ::2, 0]
     assert ref.shape == got.shape
     for q in range(4):
         ok, w = obs_close(got[q], ref[q], 1e-12)
         assert ok, (q, w)
+    assert ref22.shape == (N // 2,)
+    ok, w = obs_close(o.wilson_loops()[1, 2::2, 0], ref22, 1e-12)
+    assert ok, ("wl2x2", w)
 
 
 @pytest.mark.parametrize("action,c1", [("tlsym", -1.0 / 12.0), ("dbw2", -1.4088)])
