@@ -38,6 +38,8 @@ extern "C" {
 #define NSPT_ERR_NODEVICE 5  /* no CUDA device */
 #define NSPT_ERR_STATE 6     /* call out of sequence (e.g. no noise set) */
 #define NSPT_ERR_IO 7        /* file I/O error */
+#define NSPT_ERR_TIMEOUT 8   /* device work still running at the time limit
+                                (nspt_set_timeout); the work is not cancelled */
 
 #define NSPT_MAX_ORDER 48
 
@@ -154,6 +156,14 @@ int nspt_wilson_loops(nspt_ctx *ctx, double *loops);
  * of orders 2, 4, ... (its ptU[1], ptU[3], ...).  NSPT_ERR_STATE with
  * twisted boundaries. */
 int nspt_wl2x2(nspt_ctx *ctx, double *loop);
+
+/* Host-side watchdog: the calls that wait for their device work (the step,
+ * sweep, gauge-fixing, zero-mode and loop calls) wait at most `seconds`
+ * (0, the default: without limit) and then return NSPT_ERR_TIMEOUT.  The
+ * device work is not interrupted and stays queued in order; the next such
+ * call waits for it first, so the context stays usable.  No kernel of the
+ * engine spins on a flag, so only slow work can reach the limit. */
+int nspt_set_timeout(nspt_ctx *ctx, double seconds);
 
 /* Per-order scale of the float-float products (NSPT_PRECISION_FF): with
  * automatic != 0 (the default) each sweep fits e to the field, so that

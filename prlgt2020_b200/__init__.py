@@ -283,6 +283,12 @@ class NsptEngine:
                     "nspt_rect_observables")
         return out
 
+    def set_timeout(self, seconds: float = 0.0):
+        """Wait at most `seconds` for a call's device work (0: no limit);
+        past it the call raises NsptError with code NSPT_ERR_TIMEOUT while
+        the work runs on, and the next call waits for it first."""
+        self._check(load_library().nspt_set_timeout(self._h, float(seconds)), "nspt_set_timeout")
+
     def set_ff_scale(self, e=None):
         """Float-float products: fixed per-order scale exponent e (order k
         multiplied by 2^(e k) before the split), or None to fit it to the

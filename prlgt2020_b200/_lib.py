@@ -23,6 +23,7 @@ NSPT_ERR_CUDA = 4
 NSPT_ERR_NODEVICE = 5
 NSPT_ERR_STATE = 6
 NSPT_ERR_IO = 7
+NSPT_ERR_TIMEOUT = 8
 NSPT_MAX_ORDER = 48
 
 NSPT_TWIST_Y = 1 << 1
@@ -63,6 +64,7 @@ SIGNATURES = {
     "nspt_rect_observables": (_I, [_P, _D]),
     "nspt_wilson_loops": (_I, [_P, _D]),
     "nspt_wl2x2": (_I, [_P, _D]),
+    "nspt_set_timeout": (_I, [_P, ctypes.c_double]),
     "nspt_set_ff_scale": (_I, [_P, _I, _I]),
     "nspt_get_ff_scale": (_I, [_P, ctypes.POINTER(_I)]),
     "nspt_save_config": (_I, [_P, ctypes.c_char_p, _I]),

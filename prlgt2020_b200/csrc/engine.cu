@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -61,6 +62,8 @@ struct nspt_ctx {
   int *ff_e;                     // float-float scale exponent used by the sweep (device)
   unsigned long long *ff_mx;     // [N] per-order max |U_k| (bit patterns)
   bool ff_auto;                  // fit the exponent each sweep
+  double timeout_s;              // host-side limit on waiting for a call's device work (0: none)
+  bool busy;                     // a call returned NSPT_ERR_TIMEOUT; its work may still run
   double2 *loop_part;            // Wilson loops: per-CTA rows and the summed row
   size_t loop_part_n;
   double *noise;  // injected noise
@@ -78,10 +81,11 @@ static const char *kErr[] = {"ok",
                              "CUDA runtime error",
                              "no CUDA device",
                              "call out of sequence",
-                             "file I/O error"};
+                             "file I/O error",
+                             "device work still running at the time limit"};
 
 extern "C" const char *nspt_error_string(int code) {
-  if (code < 0 || code > 7) return "unknown error";
+  if (code < 0 || code > 8) return "unknown error";
   return kErr[code];
 }
 
@@ -453,6 +457,8 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->sweep_warps = 0;
   ctx->loop_part = nullptr;
   ctx->loop_part_n = 0;
+  ctx->timeout_s = 0.0;
+  ctx->busy = false;
   ctx->obs_tr2 = nullptr;
   ctx->ff_e = nullptr;
   ctx->ff_mx = nullptr;
@@ -650,14 +656,47 @@ extern "C" int nspt_seed(nspt_ctx *ctx, uint64_t seed, uint64_t counter) {
 }
 
 // Device time of a call: events on the context's stream around its launches.
+// Wait for the context's stream, at most timeout_s seconds when a limit is
+// set: the device work itself is never interrupted; past the limit the call
+// returns NSPT_ERR_TIMEOUT and the next call waits for that work first.
+static int wait_stream(nspt_ctx *ctx, cudaEvent_t done) {
+  if (ctx->timeout_s <= 0.0) {
+    CK(cudaEventSynchronize(done));
+    ctx->busy = false;
+    return NSPT_OK;
+  }
+  const auto t0 = std::chrono::steady_clock::now();
+  for (;;) {
+    const cudaError_t e = cudaEventQuery(done);
+    if (e == cudaSuccess) break;
+    if (e != cudaErrorNotReady) CK(e);
+    const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (el > ctx->timeout_s) {
+      ctx->busy = true;
+      char msg[96];
+      snprintf(msg, sizeof(msg), "device work still running after %.3g s", el);
+      ctx->err = msg;
+      return NSPT_ERR_TIMEOUT;
+    }
+  }
+  ctx->busy = false;
+  return NSPT_OK;
+}
+
 static int timed_begin(nspt_ctx *ctx) {
+  if (ctx->busy) {  // the work a timed-out call left behind
+    CK(cudaEventRecord(ctx->ev1, ctx->st));
+    int rc = wait_stream(ctx, ctx->ev1);
+    if (rc) return rc;
+  }
   ctx->kcount = 0;
   CK(cudaEventRecord(ctx->ev0, ctx->st));
   return NSPT_OK;
 }
 static int timed_end(nspt_ctx *ctx) {
   CK(cudaEventRecord(ctx->ev1, ctx->st));
-  CK(cudaStreamSynchronize(ctx->st));
+  int rc = wait_stream(ctx, ctx->ev1);
+  if (rc) return rc;
   cudaEventElapsedTime(&ctx->last_ms, ctx->ev0, ctx->ev1);
   double sum = 0.0;
   for (int i = 0; i < ctx->kcount; i++) {
@@ -829,6 +868,12 @@ extern "C" int nspt_observables(nspt_ctx *ctx, double *plaq, double *norm, doubl
         trU[2 * (mu * N + k)] = t.x / (double)(3 * ctx->V);
         trU[2 * (mu * N + k) + 1] = t.y / (double)(3 * ctx->V);
       }
+  return NSPT_OK;
+}
+
+extern "C" int nspt_set_timeout(nspt_ctx *ctx, double seconds) {
+  if (!ctx || !(seconds >= 0.0)) return NSPT_ERR_ARG;
+  ctx->timeout_s = seconds;
   return NSPT_OK;
 }
 

@@ -40,8 +40,9 @@ def test_library_exports_every_declared_symbol(engine_mod):
 def test_error_strings(engine_mod):
     from prlgt2020_b200 import _lib
     lib = _lib.load()
-    for code in range(8):
-        assert lib.nspt_error_string(code)
+    for code in range(9):
+        assert lib.nspt_error_string(code) != b"unknown error"
+    assert b"time limit" in lib.nspt_error_string(_lib.NSPT_ERR_TIMEOUT)
     assert lib.nspt_error_string(99) == b"unknown error"
 
 

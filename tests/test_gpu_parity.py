@@ -351,3 +351,24 @@ def test_improved_action_sweeps_match_oracle(engine_mod, oracle_mod, action, c1,
         e.zero_modes_subtraction()
         o.zero_modes()
     assert per_order_rel(e.download(), o.links, N).max() <= 1e-11
+
+
+def test_watchdog_timeout_returns_and_the_context_stays_usable(engine_mod):
+    """nspt_set_timeout: a call whose device work outlasts the limit returns
+    NSPT_ERR_TIMEOUT while the work runs on; the next call waits for it, and
+    the field equals that of a context run without a limit."""
+    from prlgt2020_b200 import _lib
+    P = engine_mod
+    L, N = (16, 16, 16, 16), 12
+    a, b = P.NsptEngine(L, N, zero_modes=True), P.NsptEngine(L, N, zero_modes=True)
+    for e in (a, b):
+        e.seed(77, 0)
+    a.set_timeout(1e-6)
+    with pytest.raises(P.NsptError) as err:
+        a.NsptEvolve(0.01, 3, 1)
+    assert err.value.code == _lib.NSPT_ERR_TIMEOUT
+    a.set_timeout(0.0)
+    a.NsptEvolve(0.01, 1, 1)
+    b.NsptEvolve(0.01, 4, 1)
+    assert np.array_equal(a.download(), b.download())
+    assert np.array_equal(a.observables().plaq, b.observables().plaq)
