@@ -12,6 +12,9 @@
 #                            parity runs, larger only for CPU timing
 #     ACTION                 wil (default) | tlsym | iwa | dbw2: GAUGE_ACTION
 #                            (choices.h:110, periodic builds only)
+#     UPDATE                 jacobi (default): UPDATE_ONTHEFLY off, the parity
+#                            builds; otf: the reference's default on-the-fly
+#                            (Gauss-Seidel) update, for statistical comparisons
 #
 # The build uses the reference's flags (Makefile:2: -DUSE_RAND55
 # -D__PARALLEL_OMP__ -O3 -fopenmp -std=c++0x) plus
@@ -31,8 +34,12 @@ set -euo pipefail
 REF=${REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
 N=${1:?N}; BC=${2:?BC}; GF=${3:?GF}; NTX=${4:-1}; NTY=${5:-1}; NTZ=${6:-1}; ACT=${7:-wil}
+UPD=${8:-jacobi}
 NAME=ref_N${N}_${BC}_${GF}_t${NTX}${NTY}${NTZ}
 if [ "$ACT" != wil ]; then NAME=${NAME}_${ACT}; fi
+if [ "$UPD" = otf ]; then NAME=${NAME}_otf; elif [ "$UPD" != jacobi ]; then
+  echo "build_ref: unknown update $UPD" >&2; exit 2
+fi
 OUT=$HERE/_ref/$NAME
 if [ ! -f "$REF/nspt.cc" ]; then
   echo "build_ref: reference sources not found at $REF" >&2
@@ -40,11 +47,13 @@ if [ ! -f "$REF/nspt.cc" ]; then
 fi
 mkdir -p "$OUT/cfg" "$OUT/obj"
 SED=(-e "s/^#define allocORD 6\$/#define allocORD $N/"
-     -e "s/^#define UPDATE_ONTHEFLY\$/\/* UPDATE_ONTHEFLY off: Jacobi update *\//"
      -e "s/^#define ntx  1\$/#define ntx  $NTX/"
      -e "s/^#define nty  1\$/#define nty  $NTY/"
      -e "s/^#define ntz  1\$/#define ntz  $NTZ/"
      -e "s/^\/\/#define __WILLOOP_2x2__\$/#define __WILLOOP_2x2__/")
+if [ "$UPD" = jacobi ]; then
+  SED+=(-e "s/^#define UPDATE_ONTHEFLY\$/\/* UPDATE_ONTHEFLY off: Jacobi update *\//")
+fi
 DEFS=(-DDSFMT_MEXP=19937 -DUSE_RAND55 -D__PARALLEL_OMP__)
 if [ "$BC" = tw ]; then
   SED+=(-e "s/^#define PERIODIC_BC\$/\/* PERIODIC_BC off *\//"

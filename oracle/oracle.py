@@ -199,18 +199,23 @@ def ser_op(name: str, N: int, *args: np.ndarray) -> np.ndarray:
 # ---------------------------------------------------------------------------
 
 def ref_binary(N: int, bc: str = "pbc", gf: str = "local", grid=(1, 1, 1),
-               action: str = "wil") -> str:
+               action: str = "wil", update: str = "jacobi") -> str:
     name = "ref_N%d_%s_%s_t%d%d%d" % ((N, bc, gf) + tuple(grid))
     if action != "wil":
         name += "_" + action
+    if update != "jacobi":
+        name += "_" + update
     return os.path.join(HERE, "_ref", name, "ref_harness")
 
 
 def build_reference(N: int, bc: str = "pbc", gf: str = "local", grid=(1, 1, 1),
-                    action: str = "wil") -> str:
+                    action: str = "wil", update: str = "jacobi") -> str:
+    """update: "jacobi" (UPDATE_ONTHEFLY off, the parity builds) or "otf"
+    (the reference's default on-the-fly update, choices.h:61)."""
     subprocess.run([os.path.join(HERE, "build_ref.sh"), str(N), bc, gf] +
-                   [str(g) for g in grid] + [action], check=True, stdout=subprocess.DEVNULL)
-    return ref_binary(N, bc, gf, grid, action)
+                   [str(g) for g in grid] + [action, update], check=True,
+                   stdout=subprocess.DEVNULL)
+    return ref_binary(N, bc, gf, grid, action, update)
 
 
 def read_config(path: str, V: int, N: int):
