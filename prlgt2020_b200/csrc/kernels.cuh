@@ -93,10 +93,22 @@ __device__ __forceinline__ void stage(double2 *slot, const double2 *U, const dou
     // lane j copies colour component j (= 3r + c) of every order
     const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
     const int off = dag ? 3 * r + c : 3 * c + r;
+    // every order in flight at once, global -> shared without registers
+    // (cp.async.cg reads through L2, so it is coherent for RW as well); the
+    // dagger is the transposed position plus a sign flip of the imaginary
+    // parts this lane copied, once they have landed
     for (int k = 1; k <= N; k++) {
-      const double2 v = ld_link<RW>(src + (size_t)(9 * (k - 1) + L.j) * V);
-      slot[1 + 9 * (k - 1) + off] = dag ? cconj(v) : v;
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(slot + 1 + 9 * (k - 1) + off);
+      const double2 *gp = src + (size_t)(9 * (k - 1) + L.j) * V;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gp) : "memory");
     }
+    cp_commit();
+    cp_wait0();
+    if (dag)
+      for (int k = 1; k <= N; k++) {
+        double *im = &slot[1 + 9 * (k - 1) + off].y;
+        *im = -*im;
+      }
     if (L.j == 0) {
       const double2 f = ld_link<RW>(Uf + (size_t)mu * V + n.site);
       slot[0] = dag ? cconj(f) : f;
@@ -124,10 +136,19 @@ __device__ __forceinline__ void stage_site(double2 *slot, const double2 *__restr
                                            bool dag = false) {
   const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
   const int off = dag ? 3 * r + c : 3 * c + r;
+  // as stage(): all orders in flight, then the dagger's sign flip
   for (int k = 1; k <= N; k++) {
-    const double2 v = __ldg(src + (size_t)(9 * (k - 1) + L.j) * V + site);
-    slot[1 + 9 * (k - 1) + off] = dag ? cconj(v) : v;
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(slot + 1 + 9 * (k - 1) + off);
+    const double2 *gp = src + (size_t)(9 * (k - 1) + L.j) * V + site;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gp) : "memory");
   }
+  cp_commit();
+  cp_wait0();
+  if (dag)
+    for (int k = 1; k <= N; k++) {
+      double *im = &slot[1 + 9 * (k - 1) + off].y;
+      *im = -*im;
+    }
   if (L.j == 0) slot[0] = dag ? cconj(flag) : flag;
   __syncwarp(L.mask);
 }
@@ -701,11 +722,17 @@ __global__ void __launch_bounds__(256, 1)
   const double2 *src = Lg + (size_t)mu * 9 * N * V + site;
   const double2 *mm = MMs + (size_t)mu * 9 * N;
   {
+    // the logs arrive by cp.async (all orders in flight), then MM/V is
+    // subtracted in place from the entries this lane copied
     const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
     for (int k = 1; k <= N; k++) {
-      const int e = 9 * (k - 1) + L.j;
-      P[sidx(k, r, c)] = csub(__ldg(src + (size_t)e * V), mm[e]);
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(P + sidx(k, r, c));
+      const double2 *gp = src + (size_t)(9 * (k - 1) + L.j) * V;
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gp) : "memory");
     }
+    cp_commit();
+    cp_wait0();
+    for (int k = 1; k <= N; k++) P[sidx(k, r, c)] = csub(P[sidx(k, r, c)], mm[9 * (k - 1) + L.j]);
   }
   if (L.j == 0) P[0] = cz();
   __syncwarp(L.mask);
@@ -760,7 +787,14 @@ __global__ void __launch_bounds__(256, 1)
   const double dv = (double)geo.V;
   const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
   for (int k = 1; k <= N; k++) {
-    const double2 w = __ldg(Wg + (size_t)(9 * (k - 1) + L.j) * V + site);
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(P + sidx(k, r, c));
+    const double2 *gp = Wg + (size_t)(9 * (k - 1) + L.j) * V + site;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gp) : "memory");
+  }
+  cp_commit();
+  cp_wait0();
+  for (int k = 1; k <= N; k++) {
+    const double2 w = P[sidx(k, r, c)];
     P[sidx(k, r, c)] = make_double2(w.x / dv, w.y / dv);
   }
   if (L.j == 0) P[0] = cz();
