@@ -345,26 +345,31 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
   bool first = true;
   for (int nu = 0; nu < 4; nu++) {
     if (nu == mu) continue;
-    // ---- upper staple U_nu(x+mu) [U_nu(x) U_mu(x+nu)]^dag (QCDenvNODEpt_test.h:555)
+    // ---- upper staple U_nu(x+mu) [U_nu(x) U_mu(x+nu)]^dag (QCDenvNODEpt_test.h:555),
+    // formed as (U_nu(x+mu) U_mu(x+nu)^dag) U_nu(x)^dag: the same truncated
+    // series (the product is associative), with every operand staged
     {
+      // U_nu(x+mu) into T (twisted when it crosses a twisted face), then
+      // T <- T U_mu(x+nu)^dag in place
+      const Nb m = neighbour(a.g, x, mu, 1);
       const Nb b = neighbour(a.g, x, nu, 1);
-      stage(Y, a.U, a.Uf, mu, b, a.g, N, L);
-      const double2 a0 = __ldg(a.Uf + (size_t)nu * V + site);
-      const LeftG A{a.U + nu * plane_mu + site, V, ring};
-      // T holds dag(U_nu(x) U_mu(x+nu))
-      cprod<FF, MO, false>(A, a0, Y, Y[0], N, L, ffe,
-                         [&](int k, int r, double2 v) { T[sidx(k, c, r)] = cconj(v); });
-      if (L.j == 0) T[0] = cconj(flag_mul(a0, Y[0]));
+      stage(T, a.U, a.Uf, nu, m, a.g, N, L);
+      stage(Y, a.U, a.Uf, mu, b, a.g, N, L, true);
+      const double2 a0 = T[0], y0 = Y[0];
+      cprod<FF, MO, false>(LeftS{T}, a0, Y, y0, N, L, ffe,
+                           [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+      if (L.j == 0) T[0] = flag_mul(a0, y0);
       __syncwarp(L.mask);
     }
     {
-      // U_nu(x+mu) is staged (twisted when it crosses a twisted face)
-      const Nb m = neighbour(a.g, x, mu, 1);
-      stage(Y, a.U, a.Uf, nu, m, a.g, N, L);
-      const double2 a0 = Y[0];
-      const double2 b0 = T[0];
+      Nb self;
+      self.site = site;
+      self.fwd = self.bwd = 0;
+      stage(Y, a.U, a.Uf, nu, self, a.g, N, L, true);
+      const double2 a0 = T[0];
+      const double2 b0 = Y[0];
       const bool f0 = first;
-      cprod<FF, MO, false>(LeftS{Y}, a0, T, b0, N, L, ffe, [&](int k, int r, double2 v) {
+      cprod<FF, MO, false>(LeftS{T}, a0, Y, b0, N, L, ffe, [&](int k, int r, double2 v) {
         double2 &w = W[sidx(k, r, c)];
         w = f0 ? v : cadd(w, v);
       });
