@@ -94,6 +94,10 @@ int nspt_cold_start(nspt_ctx *ctx);
  * Injected noise is consumed by exactly one sweep. */
 int nspt_set_noise(nspt_ctx *ctx, const double *eta);
 int nspt_seed(nspt_ctx *ctx, uint64_t seed, uint64_t counter);
+/* The device generator's seed and its counter: the number of sweeps whose
+ * noise has been drawn since nspt_seed.  Saved beside a configuration, they
+ * let a resumed run continue the same noise stream (nspt_seed with both). */
+int nspt_get_seed(nspt_ctx *ctx, uint64_t *seed, uint64_t *counter);
 
 /* NsptEvolve (nspt.cc:953-1039) with Beat = nsteps and dt = tau_g of
  * Quench.cfg (before the /(-2 NC) of Quenched.cc:584-589): per step a

@@ -234,6 +234,15 @@ class NsptEngine:
     def seed(self, seed: int, counter: int = 0):
         self._check(load_library().nspt_seed(self._h, int(seed), int(counter)), "nspt_seed")
 
+    def rng_state(self):
+        """(seed, counter) of the device noise generator: with seed(seed,
+        counter) a context loaded from a saved configuration continues the
+        same noise stream."""
+        s, c = ctypes.c_uint64(0), ctypes.c_uint64(0)
+        self._check(load_library().nspt_get_seed(self._h, ctypes.byref(s), ctypes.byref(c)),
+                    "nspt_get_seed")
+        return int(s.value), int(c.value)
+
     # -- the reference's hot-path functions (nspt.h:55-94) -----------------
     def gauge_wilson(self, dt: float) -> SweepObservables:
         """One Jacobi Langevin sweep (nspt.cc:258-600); dt = tau_g of Quench.cfg."""

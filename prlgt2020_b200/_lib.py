@@ -53,6 +53,7 @@ SIGNATURES = {
     "nspt_cold_start": (_I, [_P]),
     "nspt_set_noise": (_I, [_P, _D]),
     "nspt_seed": (_I, [_P, ctypes.c_uint64, ctypes.c_uint64]),
+    "nspt_get_seed": (_I, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "nspt_step": (_I, [_P, ctypes.c_double, _I, _I]),
     "nspt_gauge_wilson": (_I, [_P, ctypes.c_double]),
     "nspt_zero_modes_subtraction": (_I, [_P]),

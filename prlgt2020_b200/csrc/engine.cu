@@ -655,6 +655,13 @@ extern "C" int nspt_seed(nspt_ctx *ctx, uint64_t seed, uint64_t counter) {
   return NSPT_OK;
 }
 
+extern "C" int nspt_get_seed(nspt_ctx *ctx, uint64_t *seed, uint64_t *counter) {
+  if (!ctx || !seed || !counter) return NSPT_ERR_ARG;
+  *seed = ctx->seed;
+  *counter = ctx->counter;
+  return NSPT_OK;
+}
+
 // Device time of a call: events on the context's stream around its launches.
 // Wait for the context's stream, at most timeout_s seconds when a limit is
 // set: the device work itself is never interrupted; past the limit the call

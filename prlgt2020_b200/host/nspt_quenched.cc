@@ -14,7 +14,10 @@
 //     (appended, 30 digits), .nor, .trU, .log, and the final configuration
 //     <last_conf>SU3_wil_nf0_..._o<N> in the reference's binary format
 //     (checkpoints add _<k>.dat), one line per order per step as
-//     gauge_wilson writes them (nspt.cc:570-597).
+//     gauge_wilson writes them (nspt.cc:570-597);
+//   * beside every saved configuration a noise-state sidecar <name>.rng (no
+//     reference counterpart), read back on a hot start when present, so a run
+//     resumed from a checkpoint continues the same noise stream.
 // The reference fixes some choices at compile time (choices.h); here they are
 // options: -T <dirs> twisted boundaries in y/z/t (TWISTED_BC, _TWIST_*),
 // -F Fourier-accelerated gauge fixing (__FA_GAUGE_FIXING__, periodic only),
@@ -128,6 +131,39 @@ void usage() {
          "-A action\timproved gauge action: tlsym, iwa or dbw2\n"
          "-P\t\tdevice Philox noise instead of the reference's generator\n"
          "-W\t\t2x2 Wilson loops file (WL2x2, periodic boundaries)\n\n");
+}
+
+// Noise-state sidecar <configuration>.rng, written beside every saved
+// configuration: the device generator's seed and counter and the host
+// rand55 state.  The reference keeps no noise state (a hot start reseeds,
+// Quenched.cc:612-637); with the sidecar a run split at a checkpoint draws
+// the same noise as one that ran through.  A hot start without a sidecar
+// reseeds from Quench.cfg, as the reference does.
+int write_rng_sidecar(const std::string &path, nspt_ctx *ctx, const Rand55 &rng) {
+  uint64_t seed = 0, counter = 0;
+  const int rc = nspt_get_seed(ctx, &seed, &counter);
+  if (rc) return rc;
+  FILE *f = fopen(path.c_str(), "w");
+  if (!f) return NSPT_ERR_IO;
+  fprintf(f, "nspt_rng 1\nphilox %llu %llu\n", (unsigned long long)seed,
+          (unsigned long long)counter);
+  rng.save(f);
+  return fclose(f) == 0 ? NSPT_OK : NSPT_ERR_IO;
+}
+
+int read_rng_sidecar(const std::string &path, nspt_ctx *ctx, Rand55 &rng) {
+  FILE *f = fopen(path.c_str(), "r");
+  if (!f) return NSPT_OK;  // none: fresh seed, as the reference
+  int version = 0;
+  unsigned long long seed = 0, counter = 0;
+  const bool ok = fscanf(f, " nspt_rng %d philox %llu %llu", &version, &seed, &counter) == 3 &&
+                  version == 1 && rng.load(f);
+  fclose(f);
+  if (!ok) {
+    fprintf(stderr, "nspt_quenched: unreadable noise state %s\n", path.c_str());
+    return NSPT_ERR_IO;
+  }
+  return nspt_seed(ctx, seed, counter);
 }
 
 // AggiornaParametri's damocle.dag read (Quenched.cc:677-685)
@@ -323,6 +359,8 @@ int main(int argc, char **argv) {
   }
   Rand55 rng(p.seed);
   if (p.philox && (rc = nspt_seed(ctx, (uint64_t)p.seed, 0))) return fail(ctx, rc, "seed");
+  if (p.init && (rc = read_rng_sidecar(conf_name + ".rng", ctx, rng)))
+    return fail(ctx, rc, "noise state");
   std::vector<double> eta;
   if (!p.philox) eta.resize((size_t)p.L[0] * p.L[1] * p.L[2] * p.L[3] * 32);
   stamp(logf, "Inizio run");
@@ -383,6 +421,7 @@ int main(int argc, char **argv) {
     if (save == 1) {
       const std::string name = conf_name + "_" + std::to_string(++config_counter) + ".dat";
       if ((rc = nspt_save_config(ctx, name.c_str(), N))) return fail(ctx, rc, "checkpoint");
+      if ((rc = write_rng_sidecar(name + ".rng", ctx, rng))) return fail(ctx, rc, "checkpoint");
     }
     if (kill == 1) p.sweep = 0;
   }
@@ -398,6 +437,7 @@ int main(int argc, char **argv) {
   if ((rc = write_loops())) return fail(ctx, rc, "ComputeLoops");
   if (loopf) fclose(loopf);
   if ((rc = nspt_save_config(ctx, conf_name.c_str(), N))) return fail(ctx, rc, "save");
+  if ((rc = write_rng_sidecar(conf_name + ".rng", ctx, rng))) return fail(ctx, rc, "save");
   fclose(plaqf);
   fclose(normf);
   fclose(truf);

@@ -9,6 +9,7 @@
 
 #include <cmath>
 #include <cstdint>
+#include <cstdio>
 
 class Rand55 {
  public:
@@ -52,6 +53,26 @@ class Rand55 {
 
   void fill(double *out, long n) {
     for (long k = 0; k < n; k++) out[k] = gauss();
+  }
+
+  // The whole generator state as text (ring, links, positions, the cached
+  // second normal of a Box-Muller pair), so that a resumed run draws the
+  // numbers an uninterrupted one would.  Doubles go as hex floats: exact.
+  void save(FILE *f) const {
+    fprintf(f, "rand55 %d %d %d %a %a\n", n1_, n2_, have_ ? 1 : 0, r_, t_);
+    for (int i = 0; i < 55; i++)
+      fprintf(f, "%llu %d\n", (unsigned long long)ring_[i], next_[i]);
+  }
+  bool load(FILE *f) {
+    int have = 0;
+    if (fscanf(f, " rand55 %d %d %d %la %la", &n1_, &n2_, &have, &r_, &t_) != 5) return false;
+    have_ = have != 0;
+    for (int i = 0; i < 55; i++) {
+      unsigned long long w = 0;
+      if (fscanf(f, "%llu %d", &w, &next_[i]) != 2) return false;
+      ring_[i] = (uint64_t)w;
+    }
+    return n1_ >= 0 && n1_ < 55 && n2_ >= 0 && n2_ < 55;
   }
 
  private:

@@ -139,3 +139,30 @@ def test_driver_replays_reference_fixture(driver, oracle_mod, tmp_path, path):
         assert wl.shape == (2, N // 2)
         ok, w = obs_close(wl[-1], o.wilson_loops()[1, 2::2, 0], 1e-11)
         assert ok, ("wl2x2", w)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("philox", [False, True], ids=["rand55", "philox"])
+def test_driver_resumes_a_run_from_its_noise_state_sidecar(driver, tmp_path, philox):
+    """A run of 6 sweeps and the same run split into 3 + 3 (hot start from
+    the saved configuration and its .rng sidecar) write the same plaquette
+    series and save the same configuration, bit for bit."""
+    L, N, dt, alpha, seed = (4, 4, 4, 4), 4, 0.01, -0.05, 4242
+    extra = ["-P"] if philox else []
+    name = stem(L, alpha, dt, N)
+    whole, split = tmp_path / "whole", tmp_path / "split"
+    for d in (whole, split):
+        d.mkdir()
+        write_damocle(d, dt, alpha)
+    write_cfg(whole, L, 6, 6, dt, alpha, 0, N, seed)
+    r = subprocess.run([driver] + extra, cwd=whole, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    write_cfg(split, L, 3, 3, dt, alpha, 0, N, seed)
+    r = subprocess.run([driver] + extra, cwd=split, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert (split / ("conf" + name + ".rng")).exists()
+    write_cfg(split, L, 3, 3, dt, alpha, 1, N, seed)
+    r = subprocess.run([driver] + extra, cwd=split, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    for f in ("plaq_" + name + ".txt", "conf" + name, "conf" + name + ".rng"):
+        assert (whole / f).read_bytes() == (split / f).read_bytes(), f

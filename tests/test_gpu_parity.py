@@ -372,3 +372,27 @@ def test_watchdog_timeout_returns_and_the_context_stays_usable(engine_mod):
     b.NsptEvolve(0.01, 4, 1)
     assert np.array_equal(a.download(), b.download())
     assert np.array_equal(a.observables().plaq, b.observables().plaq)
+
+
+def test_checkpoint_with_rng_state_resumes_the_same_stream(engine_mod, tmp_path):
+    """save + rng_state, then load + seed(seed, counter) in a new context:
+    the resumed run equals the uninterrupted one bit for bit."""
+    P = engine_mod
+    L, N = (4, 4, 4, 4), 6
+    kw = dict(zero_modes=True, local_gf=True, alpha=-0.05)
+    whole = P.NsptEngine(L, N, **kw)
+    whole.seed(31337, 0)
+    whole.NsptEvolve(0.01, 5, 1)
+    first = P.NsptEngine(L, N, **kw)
+    first.seed(31337, 0)
+    first.NsptEvolve(0.01, 2, 1)
+    path = str(tmp_path / "conf.dat")
+    first.save(path)
+    state = first.rng_state()
+    assert state == (31337, 2)
+    resumed = P.NsptEngine(L, N, **kw)
+    resumed.load(path)
+    resumed.seed(*state)
+    resumed.NsptEvolve(0.01, 3, 1)
+    assert np.array_equal(whole.download(), resumed.download())
+    assert resumed.rng_state() == whole.rng_state() == (31337, 5)
