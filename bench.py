@@ -131,6 +131,20 @@ def read_profile_traffic():
     return None
 
 
+def host_cpu() -> dict:
+    """The host's CPU model and logical core count (/proc/cpuinfo)."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"model": model, "nproc": os.cpu_count()}
+
+
 def cpu_reference_sample(N: int, L_sample, steps: int, threads_cap: int | None = None):
     """Time the reference's own code (oracle/_ref) on a bounded sample with the
     largest OpenMP grid the sample and the host allow; returns (seconds per
@@ -306,9 +320,14 @@ def run_ours(args, world, rank, local):
     cpu = None
     if rank == 0 and not args.no_cpu:
         spp, threads, kind, _b = cpu_reference_sample(N, (8, 8, 8, 8), 1)
+        spp1, _t1, kind1, _b1 = cpu_reference_sample(N, (4, 4, 4, 4), 1, threads_cap=1)
         cpu = {"value": 1.0 / (spp * V / 8 ** 4), "unit": "sweeps/s", "cores": threads,
                "kind": kind,
-               "sample": "1 sweep of 8^4 x %d orders (twisted y,z), scaled by V to 32^4" % N}
+               "sample": "1 sweep of 8^4 x %d orders (twisted y,z), scaled by V to 32^4" % N,
+               "single_thread": {"value": 1.0 / (spp1 * V / 4 ** 4), "unit": "sweeps/s",
+                                 "cores": 1, "kind": kind1,
+                                 "sample": "1 sweep of 4^4 x %d orders, scaled by V to 32^4" % N},
+               "host": host_cpu()}
 
     if rank == 0:
         line = {
