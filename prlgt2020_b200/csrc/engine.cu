@@ -130,10 +130,10 @@ static void sweep_kernel(dim3 grid, dim3 blk, size_t smem, cudaStream_t st, cons
 
 static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
   const long nl = 4 * ctx->V;
-  KernelShape k = choose_shape(ctx, SWEEP_SLOTS, nl, RING,
+  KernelShape k = choose_shape(ctx, SWEEP_SLOTS, nl, 0,
                                ctx->sweep_warps > 0 ? std::min(ctx->sweep_warps, SWEEP_THREADS / 32)
                                                     : SWEEP_THREADS / 32);
-  const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, SWEEP_SLOTS, RING);
+  const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, SWEEP_SLOTS, 0);
   const long per_cta = (long)k.warps * LPW;
   const unsigned grid = (unsigned)((nl + per_cta - 1) / per_cta);
   const dim3 blk(32 * k.warps);

@@ -311,9 +311,9 @@ __device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, doub
 // Jacobi Langevin sweep, one link per group: gauge_wilson, nspt.cc:362-439.
 // MEASURE: only the plaquette traces (plaquette_measure, nspt.cc:1362-1383).
 //
-// Three series slots per group (T, Y, W) plus the left-operand ring: W
-// holds the staple sum, then X^2 of the series exp; T and Y hold staged
-// operands, products, the force and the exp.
+// Three series slots per group (T, Y, W): W holds the staple sum, then X^2
+// of the series exp; T and Y hold staged operands, products, the force and
+// the exp.  Every operand is staged by cp.async, so no left-operand ring.
 #ifndef NSPT_SWEEP_THREADS
 #define NSPT_SWEEP_THREADS 256
 #endif
@@ -330,8 +330,8 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
   const int warp = threadIdx.x >> 5;
   const int N = a.N, SS = a.SS, c = L.c;
   const size_t V = (size_t)a.g.V;
-  double2 *T = sm + (size_t)(warp * LPW + g) * (SWEEP_SLOTS * SS + RING), *Y = T + SS;
-  double2 *W = Y + SS, *ring = W + SS;
+  double2 *T = sm + (size_t)(warp * LPW + g) * (SWEEP_SLOTS * SS), *Y = T + SS;
+  double2 *W = Y + SS;
   bool valid;
   const long link = group_unit(g, 4L * a.g.V, valid);
   if (!valid) return;  // groups are independent: a group past the end has no work
