@@ -351,7 +351,9 @@ def run_ours(args, world, rank, local):
             "clocks": clocks,
             "e2e": e2e,
             "with_gf": with_gf,
-            "gpu_launches": 4 * args.steps,
+            # per sweep: k_sweep, three k_rowsum reductions, k_inc (the
+            # Philox step counter) -- the launch list in profiles/
+            "gpu_launches": 5 * args.steps,
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
