@@ -21,11 +21,11 @@ pytestmark = pytest.mark.gpu
 FF_TOL = 1e-11
 
 
-def _pair(P, O, L, N, start, precision):
-    o = O.Oracle(L, N)
+def _pair(P, O, L, N, start, precision, twist=""):
+    o = O.Oracle(L, N, twist_mask=sum({"y": 2, "z": 4, "t": 8}[d] for d in twist))
     if start is not None:
         o.random_start(start, 0.5)
-    e = P.NsptEngine(L, N, precision=precision)
+    e = P.NsptEngine(L, N, precision=precision, twist=twist)
     e.upload(o.links)
     return e, o
 
@@ -58,6 +58,18 @@ def test_ff_one_sweep_random_start(engine_mod, oracle_mod, L, N):
     # the FP64 engine on the same input differs from the float-float one
     assert np.abs(d.download() - e.download()).max() > 0.0
     assert per_order_rel(d.download(), o.links, N).max() <= 1e-12
+
+
+def test_ff_twisted_boundaries(engine_mod, oracle_mod):
+    """The float-float sweep with twisted y,z boundaries (twists applied to
+    the staged neighbour links before the float-float products)."""
+    L, N = (4, 4, 4, 4), 10
+    e, o = _pair(engine_mod, oracle_mod, L, N, 515, "ff", twist="yz")
+    eo, oo = _sweeps(oracle_mod, e, o, 2, 0.005, 17)
+    rel = per_order_rel(e.download(), o.links, N)
+    assert rel.max() <= FF_TOL, rel
+    ok, w = obs_close(eo.plaq, oo.plaq, FF_TOL)
+    assert ok, w
 
 
 def test_ff_high_orders_need_the_rescaling(engine_mod, oracle_mod):
