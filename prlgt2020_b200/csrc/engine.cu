@@ -150,8 +150,8 @@ static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
 
 static int launch_sweep_imp(nspt_ctx *ctx, const SweepArgs &a) {
   const long nl = 4 * ctx->V;
-  KernelShape k = choose_shape(ctx, IMP_SLOTS, nl, RING);
-  const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, IMP_SLOTS, RING);
+  KernelShape k = choose_shape(ctx, IMP_SLOTS, nl, 0);
+  const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, IMP_SLOTS, 0);
   const long per_cta = (long)k.warps * LPW;
   const unsigned grid = (unsigned)((nl + per_cta - 1) / per_cta);
   cudaFuncSetAttribute(k_sweep_imp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -503,7 +503,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   while (ctx->SS % 8 != 1) ctx->SS++;
   // one warp (3 link groups of 3 slots) must fit in a CTA
   if ((size_t)LPW * group_bytes(ctx, SWEEP_SLOTS, RING) > ctx->smem_optin) return fail(NSPT_ERR_ORDER);
-  if (ctx->c1 != 0.0 && (size_t)LPW * group_bytes(ctx, IMP_SLOTS, RING) > ctx->smem_optin)
+  if (ctx->c1 != 0.0 && (size_t)LPW * group_bytes(ctx, IMP_SLOTS, 0) > ctx->smem_optin)
     return fail(NSPT_ERR_ORDER);
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return fail(NSPT_ERR_CUDA);
   cudaEventCreate(&ctx->ev0);

@@ -447,85 +447,64 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
 // boundaries): gauge_wilson, nspt.cc:272-308.  Besides the Wilson staples W,
 // the six 2x1 rectangles of staple2x1 (QCDenvNODEpt_test.h:579-611) per
 // plane go to W2; the force is c0 U W + c1 U W2, and Tr(U W2) is the w2
-// observable.  Each rectangle is four products: a two-link path A, the
-// dagger of A times a third link (written transposed and conjugated), and
-// two more factors.  Six slots per group: T, Y (paths), E (third path),
-// STG (staged links), W, W2.
-constexpr int IMP_SLOTS = 6;
+// observable.  Every staple is a chain of links (daggered where the
+// reference takes a dagger of a path: dag(A B C) = C^dag B^dag A^dag),
+// multiplied left to right in the work slot T while the next link is staged
+// into Y: four products per rectangle, as the reference's, associated the
+// other way (the truncated product is associative).  Four slots per group:
+// T, Y (work), W, W2 (sums).
+constexpr int IMP_SLOTS = 4;
 
-struct ImpCtx {
-  const double2 *U, *Uf;
-  double2 *STG, *ring;
-  size_t V, plane;
-  int N;
-  Geo g;
+// One link of a staple chain: direction, site and whether it is daggered.
+struct ImpLink {
+  int d, site;
+  bool dag;
 };
 
-__device__ __forceinline__ void imp_stage(const ImpCtx &q, double2 *slot, int d, int st,
+__device__ __forceinline__ void imp_stage(const SweepArgs &a, double2 *slot, const ImpLink &l,
                                           const Lane &L) {
   Nb n;
-  n.site = st;
+  n.site = l.site;
   n.fwd = n.bwd = 0;
-  stage(slot, q.U, q.Uf, d, n, q.g, q.N, L);
+  stage(slot, a.U, a.Uf, l.d, n, a.g, a.N, L, l.dag);
 }
 
-// out = U_d1(s1) U_d2(s2)
-__device__ __noinline__ void imp_two(const ImpCtx &q, double2 *out, int d1, int s1, int d2, int s2,
-                                     const Lane &L) {
-  imp_stage(q, q.STG, d2, s2, L);
-  const double2 a0 = __ldg(q.Uf + (size_t)d1 * q.V + s1), b0 = q.STG[0];
+// T <- T Y, in place
+__device__ __noinline__ void imp_mul(double2 *T, const double2 *Y, int N, const Lane &L) {
+  const double2 a0 = T[0], b0 = Y[0];
   const int c = L.c;
-  product<MO, false>(LeftG{q.U + d1 * q.plane + s1, q.V, q.ring}, a0, q.STG, b0, q.N, L,
-                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
-  if (L.j == 0) out[0] = flag_mul(a0, b0);
+  product<MO, false>(LeftS{T}, a0, Y, b0, N, L,
+                     [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+  if (L.j == 0) T[0] = flag_mul(a0, b0);
   __syncwarp(L.mask);
 }
 
-// out = dag(A U_d(s)), written transposed and conjugated
-__device__ __noinline__ void imp_dag_path(const ImpCtx &q, double2 *out, const double2 *A, int d,
-                                          int s, const Lane &L) {
-  imp_stage(q, q.STG, d, s, L);
-  const double2 a0 = A[0], b0 = q.STG[0];
+// Wacc (+)= T Y; first: Wacc = T Y.  Returns the product's flag.
+__device__ __noinline__ double2 imp_acc(double2 *Wacc, const double2 *T, const double2 *Y,
+                                        bool first, int N, const Lane &L) {
+  const double2 a0 = T[0], b0 = Y[0];
   const int c = L.c;
-  product<MO, false>(LeftS{A}, a0, q.STG, b0, q.N, L,
-                     [&](int k, int r, double2 v) { out[sidx(k, c, r)] = cconj(v); });
-  if (L.j == 0) out[0] = cconj(flag_mul(a0, b0));
-  __syncwarp(L.mask);
-}
-
-// out = U_d(s) B (left link streamed)
-__device__ __noinline__ void imp_link_times(const ImpCtx &q, double2 *out, int d, int s,
-                                            const double2 *B, const Lane &L) {
-  const double2 a0 = __ldg(q.Uf + (size_t)d * q.V + s), b0 = B[0];
-  const int c = L.c;
-  product<MO, false>(LeftG{q.U + d * q.plane + s, q.V, q.ring}, a0, B, b0, q.N, L,
-                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
-  if (L.j == 0) out[0] = flag_mul(a0, b0);
-  __syncwarp(L.mask);
-}
-
-// out = A B (slots)
-__device__ __noinline__ void imp_mul(double2 *out, const double2 *A, const double2 *B, int N,
-                                     const Lane &L) {
-  const double2 a0 = A[0], b0 = B[0];
-  const int c = L.c;
-  product<MO, false>(LeftS{A}, a0, B, b0, N, L,
-                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
-  if (L.j == 0) out[0] = flag_mul(a0, b0);
-  __syncwarp(L.mask);
-}
-
-// W (+)= A B; first: W = A B.  Returns the product's flag.
-__device__ __noinline__ double2 imp_acc(double2 *Wacc, const double2 *A, const double2 *B, bool first,
-                                        int N, const Lane &L) {
-  const double2 a0 = A[0], b0 = B[0];
-  const int c = L.c;
-  product<MO, false>(LeftS{A}, a0, B, b0, N, L, [&](int k, int r, double2 v) {
+  product<MO, false>(LeftS{T}, a0, Y, b0, N, L, [&](int k, int r, double2 v) {
     double2 &w = Wacc[sidx(k, r, c)];
     w = first ? v : cadd(w, v);
   });
   __syncwarp(L.mask);
   return flag_mul(a0, b0);
+}
+
+// Wacc (+)= l[0] l[1] ... l[n-1]; returns the flag of the chain
+template <int NL>
+__device__ __forceinline__ double2 imp_chain(const SweepArgs &a, double2 *T, double2 *Y,
+                                             double2 *Wacc, const ImpLink (&l)[NL], bool first,
+                                             const Lane &L) {
+  imp_stage(a, T, l[0], L);
+#pragma unroll
+  for (int m = 1; m < NL - 1; m++) {
+    imp_stage(a, Y, l[m], L);
+    imp_mul(T, Y, a.N, L);
+  }
+  imp_stage(a, Y, l[NL - 1], L);
+  return imp_acc(Wacc, T, Y, first, a.N, L);
 }
 
 __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
@@ -534,10 +513,10 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
   int g;
   if (!make_lane(L, g)) return;
   const int warp = threadIdx.x >> 5;
-  const int N = a.N, SS = a.SS, c = L.c;
+  const int N = a.N, SS = a.SS;
   const size_t V = (size_t)a.g.V;
-  double2 *T = sm + (size_t)(warp * LPW + g) * (IMP_SLOTS * SS + RING), *Y = T + SS;
-  double2 *E = Y + SS, *STG = E + SS, *W = STG + SS, *W2 = W + SS, *ring = W2 + SS;
+  double2 *T = sm + (size_t)(warp * LPW + g) * (IMP_SLOTS * SS), *Y = T + SS;
+  double2 *W = Y + SS, *W2 = W + SS;
   bool valid;
   const long link = group_unit(g, 4L * a.g.V, valid);
   if (!valid) return;
@@ -545,15 +524,6 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
   const int site = (int)(link - (long)mu * a.g.V);
   int x[4];
   coords(a.g, site, x);
-  ImpCtx q;
-  q.U = a.U;
-  q.Uf = a.Uf;
-  q.STG = STG;
-  q.ring = ring;
-  q.V = V;
-  q.plane = (size_t)9 * N * V;
-  q.N = N;
-  q.g = a.g;
 
   // site x + i mu + j nu (periodic)
   int nu = 0;
@@ -563,109 +533,79 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
     y[nu] = ((y[nu] + j) % a.g.L[nu] + a.g.L[nu]) % a.g.L[nu];
     return y[0] * a.g.s0 + y[1] * a.g.s1 + y[2] * a.g.s2 + y[3];
   };
-  double2 w2flag = cz();
-  bool first2 = true;
-  auto acc2 = [&](const double2 *A, const double2 *B) {
-    const double2 f = imp_acc(W2, A, B, first2, N, L);
+  double2 wflag = cz(), w2flag = cz();
+  bool first = true, first2 = true;
+  auto acc = [&](double2 f) {
+    wflag = first ? f : cadd(wflag, f);
+    first = false;
+  };
+  auto acc2 = [&](double2 f) {
     w2flag = first2 ? f : cadd(w2flag, f);
     first2 = false;
   };
-
-  double2 wflag = cz();
-  bool first = true;
   for (nu = 0; nu < 4; nu++) {
     if (nu == mu) continue;
-    // ---- Wilson staples, as in k_sweep (QCDenvNODEpt_test.h:554-557)
+    const int m = mu, n = nu;
+    // ---- Wilson staples (QCDenvNODEpt_test.h:554-557):
+    // U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag and
+    // U_nu(x+mu-nu)^dag U_mu(x-nu)^dag U_nu(x-nu)
     {
-      imp_stage(q, Y, mu, at(0, 1), L);
-      const double2 a0 = __ldg(a.Uf + (size_t)nu * V + site);
-      product<MO, false>(LeftG{a.U + nu * q.plane + site, V, ring}, a0, Y, Y[0], N, L,
-                         [&](int k, int r, double2 v) { T[sidx(k, c, r)] = cconj(v); });
-      if (L.j == 0) T[0] = cconj(flag_mul(a0, Y[0]));
-      __syncwarp(L.mask);
-      imp_stage(q, Y, nu, at(1, 0), L);
-      const double2 y0 = Y[0], t0 = T[0];
-      const bool f0 = first;
-      product<MO, false>(LeftS{Y}, y0, T, t0, N, L, [&](int k, int r, double2 v) {
-        double2 &w = W[sidx(k, r, c)];
-        w = f0 ? v : cadd(w, v);
-      });
-      wflag = first ? flag_mul(y0, t0) : cadd(wflag, flag_mul(y0, t0));
-      first = false;
-      __syncwarp(L.mask);
+      const ImpLink up[3] = {{n, at(1, 0), false}, {m, at(0, 1), true}, {n, site, true}};
+      acc(imp_chain(a, T, Y, W, up, first, L));
+      const ImpLink lo[3] = {{n, at(1, -1), true}, {m, at(0, -1), true}, {n, at(0, -1), false}};
+      acc(imp_chain(a, T, Y, W, lo, first, L));
     }
+    // ---- the six rectangles of staple2x1, each as its chain of five links
     {
-      imp_stage(q, Y, nu, at(1, -1), L);
-      imp_stage(q, T, mu, at(0, -1), L);
-      const double2 a0 = T[0], y0 = Y[0];
-      product<MO, false>(LeftS{T}, a0, Y, y0, N, L,
-                         [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
-      if (L.j == 0) T[0] = flag_mul(a0, y0);
-      __syncwarp(L.mask);
-      imp_stage(q, Y, nu, at(0, -1), L);
-      const double2 ta = cconj(T[0]);
-      product<MO, true>(LeftS{T}, ta, Y, Y[0], N, L, [&](int k, int r, double2 v) {
-        double2 &w = W[sidx(k, r, c)];
-        w = cadd(w, v);
-      });
-      wflag = cadd(wflag, flag_mul(ta, Y[0]));
-      __syncwarp(L.mask);
+      // U_nu(a) U_nu(b) dag(U_nu(x) U_nu(c) U_mu(d)),  a=x+mu b=x+mu+nu c=x+nu d=x+2nu
+      const ImpLink r1[5] = {{n, at(1, 0), false}, {n, at(1, 1), false}, {m, at(0, 2), true},
+                             {n, at(0, 1), true}, {n, site, true}};
+      acc2(imp_chain(a, T, Y, W2, r1, first2, L));
+      // U_mu(a) U_nu(e) dag(U_nu(x) U_mu(c) U_mu(b)),  e=x+2mu
+      const ImpLink r2[5] = {{m, at(1, 0), false}, {n, at(2, 0), false}, {m, at(1, 1), true},
+                             {m, at(0, 1), true}, {n, site, true}};
+      acc2(imp_chain(a, T, Y, W2, r2, first2, L));
+      // U_nu(a) dag(U_nu(f) U_mu(g) U_mu(c)) U_mu(f),  f=x-mu g=x-mu+nu
+      const ImpLink r3[5] = {{n, at(1, 0), false}, {m, at(0, 1), true}, {m, at(-1, 1), true},
+                             {n, at(-1, 0), true}, {m, at(-1, 0), false}};
+      acc2(imp_chain(a, T, Y, W2, r3, first2, L));
+      // dag(U_mu(d) U_nu(e) U_nu(b)) U_nu(d) U_nu(c),
+      // b=x+mu-nu c=x-nu d=x-2nu e=x+mu-2nu
+      const ImpLink r4[5] = {{n, at(1, -1), true}, {n, at(1, -2), true}, {m, at(0, -2), true},
+                             {n, at(0, -2), false}, {n, at(0, -1), false}};
+      acc2(imp_chain(a, T, Y, W2, r4, first2, L));
+      // U_mu(a) dag(U_mu(c) U_mu(b) U_nu(f)) U_nu(c),  f=x+2mu-nu
+      const ImpLink r5[5] = {{m, at(1, 0), false}, {n, at(2, -1), true}, {m, at(1, -1), true},
+                             {m, at(0, -1), true}, {n, at(0, -1), false}};
+      acc2(imp_chain(a, T, Y, W2, r5, first2, L));
+      // dag(U_mu(g) U_mu(c) U_nu(b)) U_nu(g) U_mu(h),  g=x-mu-nu h=x-mu
+      const ImpLink r6[5] = {{n, at(1, -1), true}, {m, at(0, -1), true}, {m, at(-1, -1), true},
+                             {n, at(-1, -1), false}, {m, at(-1, 0), false}};
+      acc2(imp_chain(a, T, Y, W2, r6, first2, L));
     }
-    // ---- the six rectangles of staple2x1
-    // U_nu(a) U_nu(b) dag(U_nu(x) U_nu(c) U_mu(d)),  a=x+mu b=x+mu+nu c=x+nu d=x+2nu
-    imp_two(q, T, nu, site, nu, at(0, 1), L);
-    imp_dag_path(q, Y, T, mu, at(0, 2), L);
-    imp_two(q, E, nu, at(1, 0), nu, at(1, 1), L);
-    acc2(E, Y);
-    // U_mu(a) U_nu(e) dag(U_nu(x) U_mu(c) U_mu(b)),  e=x+2mu
-    imp_two(q, T, nu, site, mu, at(0, 1), L);
-    imp_dag_path(q, Y, T, mu, at(1, 1), L);
-    imp_two(q, E, mu, at(1, 0), nu, at(2, 0), L);
-    acc2(E, Y);
-    // U_nu(a) dag(U_nu(f) U_mu(g) U_mu(c)) U_mu(f),  f=x-mu g=x-mu+nu
-    imp_two(q, T, nu, at(-1, 0), mu, at(-1, 1), L);
-    imp_dag_path(q, Y, T, mu, at(0, 1), L);
-    imp_link_times(q, E, nu, at(1, 0), Y, L);
-    imp_stage(q, Y, mu, at(-1, 0), L);
-    acc2(E, Y);
-    // dag(U_mu(d) U_nu(e) U_nu(b)) U_nu(d) U_nu(c),  b=x+mu-nu c=x-nu d=x-2nu e=x+mu-2nu
-    imp_two(q, T, mu, at(0, -2), nu, at(1, -2), L);
-    imp_dag_path(q, Y, T, nu, at(1, -1), L);
-    imp_stage(q, STG, nu, at(0, -2), L);
-    imp_mul(E, Y, STG, N, L);
-    imp_stage(q, Y, nu, at(0, -1), L);
-    acc2(E, Y);
-    // U_mu(a) dag(U_mu(c) U_mu(b) U_nu(f)) U_nu(c),  f=x+2mu-nu
-    imp_two(q, T, mu, at(0, -1), mu, at(1, -1), L);
-    imp_dag_path(q, Y, T, nu, at(2, -1), L);
-    imp_link_times(q, E, mu, at(1, 0), Y, L);
-    imp_stage(q, Y, nu, at(0, -1), L);
-    acc2(E, Y);
-    // dag(U_mu(g) U_mu(c) U_nu(b)) U_nu(g) U_mu(h),  g=x-mu-nu h=x-mu
-    imp_two(q, T, mu, at(-1, -1), mu, at(0, -1), L);
-    imp_dag_path(q, Y, T, nu, at(1, -1), L);
-    imp_stage(q, STG, nu, at(-1, -1), L);
-    imp_mul(E, Y, STG, N, L);
-    imp_stage(q, Y, mu, at(-1, 0), L);
-    acc2(E, Y);
   }
   if (L.j == 0) {
     W[0] = wflag;
     W2[0] = w2flag;
   }
-  // ---- U W and U W2 (nspt.cc:286-303), traces, force c0 U W + c1 U W2
+  __syncwarp(L.mask);
+  // ---- U W into T and U W2 into W2 in place (nspt.cc:286-303), traces,
+  // force c0 U W + c1 U W2
   Nb self;
   self.site = site;
   self.fwd = self.bwd = 0;
   stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
   const double2 pflag = flag_mul(Y[0], wflag), p2flag = flag_mul(Y[0], w2flag);
-  product<MO, false>(LeftS{Y}, Y[0], W, wflag, N, L,
-                     [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
-  product<MO, false>(LeftS{Y}, Y[0], W2, w2flag, N, L,
-                     [&](int k, int r, double2 v) { E[sidx(k, r, c)] = v; });
+  {
+    const int c = L.c;
+    product<MO, false>(LeftS{Y}, Y[0], W, wflag, N, L,
+                       [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+    product<MO, false>(LeftS{Y}, Y[0], W2, w2flag, N, L,
+                       [&](int k, int r, double2 v) { W2[sidx(k, r, c)] = v; });
+  }
   if (L.j == 0) {
     T[0] = pflag;
-    E[0] = p2flag;
+    W2[0] = p2flag;
   }
   __syncwarp(L.mask);
   {
@@ -678,7 +618,7 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
       a.obs_tr[(size_t)k * nl4 + link] =
           cadd(cadd(T[sidx(k, 0, 0)], T[sidx(k, 1, 1)]), T[sidx(k, 2, 2)]);
       a.obs_tr2[(size_t)k * nl4 + link] =
-          cadd(cadd(E[sidx(k, 0, 0)], E[sidx(k, 1, 1)]), E[sidx(k, 2, 2)]);
+          cadd(cadd(W2[sidx(k, 0, 0)], W2[sidx(k, 1, 1)]), W2[sidx(k, 2, 2)]);
       double nrm = 0.0;
 #pragma unroll
       for (int i = 0; i < 3; i++) {
@@ -698,7 +638,7 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
   __syncwarp(L.mask);
   // W1 = c0 W1 + c1 W2 (ptSU3 operator*(double) and +, flags included)
   for (int e = L.j; e < 1 + 9 * N; e += GROUP)
-    T[e] = cadd(cscale(T[e], a.c0), cscale(E[e], a.c1));
+    T[e] = cadd(cscale(T[e], a.c0), cscale(W2[e], a.c1));
   __syncwarp(L.mask);
   update_link(a, T, Y, W, link, mu, site, self, L);
 }
