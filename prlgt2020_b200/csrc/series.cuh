@@ -166,9 +166,11 @@ struct LeftS {
 // QCDpt.h:92-114); op = dagger when DA.  a0 = flag of op(A), b0 = flag of B,
 // supplied by the caller (the result's flag is the caller's business).
 // emit(k, r, v) is called by the lane owning (k, column c) for r = 0..2.
+// i0 > 1 skips left-operand orders below i0, for a caller whose left
+// operand is exactly zero there (X^2 of a flag-0 series has no order 1).
 template <int MO, bool DA, class Left, class Emit>
 __device__ __forceinline__ void product(const Left &A, double2 a0, const double2 *B, double2 b0,
-                                        int M, const Lane &L, Emit emit) {
+                                        int M, const Lane &L, Emit emit, int i0 = 1) {
   const int c = L.c;
   constexpr int PASS = 3 * MO;
   const int npass = (M + PASS - 1) / PASS;
@@ -182,13 +184,13 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
       for (int r = 0; r < 3; r++) acc[q][r] = cz();
     double2 a[9];
     if constexpr (Left::kRing) {
-      // orders 1 and 2 in flight before the loop; one commit group per order
-      if (1 < kend) A.issue(1, L.j);
+      // orders i0 and i0+1 in flight before the loop; one commit group per order
+      if (i0 < kend) A.issue(i0, L.j);
       cp_commit();
-      if (2 < kend) A.issue(2, L.j);
+      if (i0 + 1 < kend) A.issue(i0 + 1, L.j);
       cp_commit();
     }
-    for (int i = 1; i < kend; i++) {
+    for (int i = i0; i < kend; i++) {
       if constexpr (Left::kRing) {
         cp_wait1();               // this lane's copy of order i has landed
         __syncwarp(L.mask);       // ... and every lane's; order i-1 is free
@@ -435,21 +437,23 @@ __device__ __forceinline__ void ser_horner2(const double2 *X, const double2 *Y, 
     __syncwarp(L.mask);
     return;
   }
+  // Y = X^2 has no order 1 (X has flag 0): the products start at Y's order 2
   const LeftS Yl{Y};
   for (int j = J - 1; j >= 0; --j) {
     const int M = N - 2 * j;
     const double2 sf = S[0];
     const double cx = coef(2 * j + 1);
     if (j > 0) {
-      product<MO, false>(Yl, cz(), S, sf, M, L, [&](int k, int r, double2 v) {
-        S[sidx(k, r, c)] = cadd(v, cscale(X[sidx(k, r, c)], cx));
-      });
+      product<MO, false>(
+          Yl, cz(), S, sf, M, L,
+          [&](int k, int r, double2 v) { S[sidx(k, r, c)] = cadd(v, cscale(X[sidx(k, r, c)], cx)); },
+          2);
       if (L.j == 0) S[0] = make_double2(coef(2 * j), 0.0);
       __syncwarp(L.mask);
     } else {
-      product<MO, false>(Yl, cz(), S, sf, M, L, [&](int k, int r, double2 v) {
-        last(k, r, cadd(v, cscale(X[sidx(k, r, c)], cx)));
-      });
+      product<MO, false>(
+          Yl, cz(), S, sf, M, L,
+          [&](int k, int r, double2 v) { last(k, r, cadd(v, cscale(X[sidx(k, r, c)], cx))); }, 2);
     }
   }
 }
