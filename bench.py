@@ -660,6 +660,50 @@ def run_imp(args, world, rank, local):
     eng.close()
 
 
+def run_loops(args, world, rank, local):
+    """Wilson loops (ComputeLoops, nspt.cc:1148-1312) of a 16^4 x 20 periodic
+    field: the 1x2, 2x2, 2x4 and 4x4 loops of every plane and site, traced
+    per order.  Canonical work as the reference multiplies: per (plane,
+    site) 28 path products and 6 closing products W += P Q^dag, 34 P(N) x
+    216 flop; the engine replaces each closing product by a trace (a sixth
+    of its flops)."""
+    import numpy as np
+    import torch
+
+    import prlgt2020_b200 as P
+    from prlgt2020_b200.replicas import max_over_ranks, replica_seed, whole_job_rate
+    torch.cuda.set_device(local)
+    L, N, dt = (16, 16, 16, 16), 20, 0.01
+    V = int(np.prod(L))
+    peak = P.fp64_peak_tflops()
+    eng = P.NsptEngine(L, N, zero_modes=True)
+    eng.seed(replica_seed(7000, rank), 0)
+    eng.NsptEvolve(dt, 3, 1)
+    for _ in range(args.warmup):
+        eng.ComputeLoops()
+    ms = 0.0
+    for _ in range(args.steps):
+        eng.ComputeLoops()
+        ms += eng.last_step_ms()
+    ms = max_over_ranks(ms) / args.steps
+    Pn = N * (N - 1) // 2
+    flops = 34 * Pn * 216.0 * 6 * V
+    if rank == 0:
+        ach = flops / (ms * 1e-3) / 1e12
+        line = {
+            "metric": "ComputeLoops calls/s at 16^4 x 20 orders (FP64)",
+            "value": whole_job_rate(1, world, ms * 1e-3), "unit": "calls/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (cold start + 3 sweeps, device Philox noise)",
+            "config": {"workload": "loops_16^4_N20", "L": list(L), "N": N, "bc": "periodic"},
+            "roofline": {"bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                         "frac": ach / peak, "kernel": "k_loops", "flops_per_call": flops},
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -672,13 +716,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-gf", action="store_true", help="skip the gauge-fixing figure")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "c2", "c4", "c5", "imp"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "c2", "c4", "c5", "imp", "loops"],
                     help="sweep: 32^4 x 24 twisted (the headline); c2: 16^4 x 20 periodic "
                          "with zero modes and FA gauge fixing every step, per pass; c4: 64 "
                          "replicas of 6^4..10^4 x 12, batched in one CUDA graph vs plain; "
                          "c5: 24^4 x 40 float-float products vs FP64, speed and per-order "
                          "error after 1/100/1000 steps; imp: 16^4 x 20 tree-level "
-                         "Symanzik sweep")
+                         "Symanzik sweep; loops: Wilson loops of a 16^4 x 20 field")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -695,6 +739,9 @@ def main():
         return
     if args.workload == "imp":
         run_imp(args, world, rank, local)
+        return
+    if args.workload == "loops":
+        run_loops(args, world, rank, local)
         return
     run_ours(args, world, rank, local)
 

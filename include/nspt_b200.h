@@ -184,9 +184,9 @@ int nspt_load_config(nspt_ctx *ctx, const char *path, int allocORD,
                      double *plaq_trailer);
 
 /* Device time of the last nspt_step, nspt_gauge_wilson,
- * nspt_zero_modes_subtraction, nspt_fa_gauge_fixing or
- * nspt_local_gauge_fixing call (CUDA events on the context's stream around
- * all of its launches), milliseconds. */
+ * nspt_zero_modes_subtraction, nspt_fa_gauge_fixing,
+ * nspt_local_gauge_fixing, nspt_wilson_loops or nspt_wl2x2 call (CUDA
+ * events on the context's stream around all of its launches), milliseconds. */
 double nspt_last_step_ms(const nspt_ctx *ctx);
 /* Average device time of one sweep-kernel launch in the last nspt_step or
  * nspt_gauge_wilson call (CUDA events around each of the first 64

@@ -339,7 +339,7 @@ class NsptEngine:
         return SweepObservables(plaq, norm, tru)
 
     def last_step_ms(self) -> float:
-        """Device time of the last step / sweep / zero-mode / gauge-fixing call."""
+        """Device time of the last step / sweep / zero-mode / gauge-fixing / loops call."""
         return float(load_library().nspt_last_step_ms(self._h))
 
     def last_kernel_ms(self) -> float:
