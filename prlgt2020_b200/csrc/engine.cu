@@ -746,7 +746,7 @@ extern "C" int nspt_fa_gauge_fixing(nspt_ctx *ctx, double alpha) {
 // h[q * (N+1) + k], un-normalised (k_loops, then its per-CTA rows summed)
 static int loop_sums(nspt_ctx *ctx, std::vector<double2> &h) {
   const int N = ctx->N, row = 4 * (N + 1);
-  const size_t gb = ((size_t)LOOP_SLOTS * ctx->SS + RING + row) * sizeof(double2);
+  const size_t gb = ((size_t)LOOP_SLOTS * ctx->SS + row) * sizeof(double2);
   const int warps = (int)std::min<size_t>(8, ctx->smem_optin / (LPW * gb));
   if (warps < 1) return NSPT_ERR_ORDER;
   const long units = 6L * ctx->V;

@@ -6,15 +6,14 @@
 // One 9-lane group per (plane, site).  The reference closes each loop with a
 // product by a daggered path, W += P Q^dag; only Tr W is printed, so the last
 // product is replaced by Tr(P Q^dag) = sum over cells of P_ij conj(Q_ij),
-// order by order: 28 series products and 5 such traces per (plane, site).
-// Nine slots per group (eight paths and a staging slot), the ring for the
-// streamed left link, and the group's four trace accumulators.  CTAs sum
-// their groups, and a last kernel their rows, in a fixed order.
+// order by order.  Three slots per group (two paths and a staging slot) and
+// the group's four trace accumulators; CTAs sum their groups, and a last
+// kernel their rows, in a fixed order.
 #pragma once
 
 namespace nspt {
 
-constexpr int LOOP_SLOTS = 9;
+constexpr int LOOP_SLOTS = 3;
 
 // acc[k] += Tr(X Y^dag)_k, k = 0..N (flags are multiples of the identity)
 __device__ __forceinline__ void trace_dag_acc(const double2 *X, const double2 *Y, int N,
@@ -45,51 +44,71 @@ __device__ __forceinline__ void trace_dag_acc(const double2 *X, const double2 *Y
   __syncwarp(L.mask);
 }
 
-// Loop paths, each one instance (the kernel calls them many times).
+// A path of the loops: a chain of forward links, link m in direction
+// dir[m] at the site reached by the steps of the links before it.
+struct LoopPath {
+  int n;         // links
+  int dir[8];    // 0: mu, 1: nu
+};
+
 struct LoopCtx {
   const double2 *U, *Uf;
-  double2 *STG, *ring;
-  size_t V, plane;
-  int N;
+  int N, mu, nu;
+  int X[4];
   Geo geo;
 };
 
-// out = U_d1(s1) U_d2(s2): the left link streamed, the right one staged
-__device__ __noinline__ void loop_two(const LoopCtx &q, double2 *out, int d1, int s1, int d2,
-                                      int s2, const Lane &L) {
+// site X + i mu + j nu (periodic)
+__device__ __forceinline__ int loop_site(const LoopCtx &q, int i, int j) {
+  int y[4] = {q.X[0], q.X[1], q.X[2], q.X[3]};
+  y[q.mu] = (y[q.mu] + i) % q.geo.L[q.mu];
+  y[q.nu] = (y[q.nu] + j) % q.geo.L[q.nu];
+  return y[0] * q.geo.s0 + y[1] * q.geo.s1 + y[2] * q.geo.s2 + y[3];
+}
+
+__device__ __forceinline__ void loop_stage(const LoopCtx &q, double2 *slot, int dir, int i, int j,
+                                           const Lane &L) {
   Nb n;
-  n.site = s2;
+  n.site = loop_site(q, i, j);
   n.fwd = n.bwd = 0;
-  stage(q.STG, q.U, q.Uf, d2, n, q.geo, q.N, L);
-  const double2 a0 = __ldg(q.Uf + (size_t)d1 * q.V + s1), b0 = q.STG[0];
+  stage(slot, q.U, q.Uf, dir ? q.nu : q.mu, n, q.geo, q.N, L);
+}
+
+// A <- A S, in place
+__device__ __noinline__ void loop_mul(double2 *A, const double2 *S, int N, const Lane &L) {
+  const double2 a0 = A[0], b0 = S[0];
   const int c = L.c;
-  product<MO, false>(LeftG{q.U + d1 * q.plane + s1, q.V, q.ring}, a0, q.STG, b0, q.N, L,
-                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
-  if (L.j == 0) out[0] = flag_mul(a0, b0);
+  product<MO, false>(LeftS{A}, a0, S, b0, N, L,
+                     [&](int k, int r, double2 v) { A[sidx(k, r, c)] = v; });
+  if (L.j == 0) A[0] = flag_mul(a0, b0);
   __syncwarp(L.mask);
 }
 
-// out = A B (slots)
-__device__ __noinline__ void loop_mul(double2 *out, const double2 *A, const double2 *B, int N,
-                                      const Lane &L) {
-  const double2 a0 = A[0], b0 = B[0];
-  const int c = L.c;
-  product<MO, false>(LeftS{A}, a0, B, b0, N, L,
-                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
-  if (L.j == 0) out[0] = flag_mul(a0, b0);
-  __syncwarp(L.mask);
+// A <- path[from..n) applied to A (from = 0: A is formed from the first
+// link); (i, j) is the site where link `from` starts, updated to the end
+__device__ __forceinline__ void loop_chain(const LoopCtx &q, double2 *A, double2 *S,
+                                           const LoopPath &p, int from, int &i, int &j,
+                                           const Lane &L) {
+  for (int m = from; m < p.n; m++) {
+    loop_stage(q, m == 0 ? A : S, p.dir[m], i, j, L);
+    if (m > 0) loop_mul(A, S, q.N, L);
+    if (p.dir[m]) j++; else i++;
+  }
 }
 
-// out = A U_d(s)
-__device__ __noinline__ void loop_mul_link(const LoopCtx &q, double2 *out, const double2 *A, int d,
-                                           int s, const Lane &L) {
-  Nb n;
-  n.site = s;
-  n.fwd = n.bwd = 0;
-  stage(q.STG, q.U, q.Uf, d, n, q.geo, q.N, L);
-  loop_mul(out, A, q.STG, q.N, L);
-}
-
+// Per (plane, site), the loops of ComputeLoops as pairs of paths P, Q from
+// x, traced as Tr(P Q^dag) (bl = mu mu from x, ld = nu nu from x, cd the
+// two nu links after bl, and so on, as named in nspt.cc:1160-1270):
+//   2x2        P = bl cd           Q = ld ml
+//   2x4 up     P = bl cd cu        Q = ld lu tl
+//   4x4        P = bl br rd ru     Q = ld lu tl tr
+//   2x4 right  P = bl br rd        Q = ld ml mr
+//   1x2        P = bl U_nu         Q = U_nu U_mu U_mu
+//   1x2        P = U_mu U_nu U_nu  Q = ld U_mu
+// Three slots per group: P and Q (paths, each extended in place link by
+// link) and S (the staged link).  A path is extended when the next loop's
+// path starts with it (bl cd -> bl cd cu, ld lu tl -> ld lu tl tr) and
+// formed afresh otherwise: 40 products and 6 traces per (plane, site).
 __global__ void __launch_bounds__(256, 1)
     k_loops(const double2 *U, const double2 *Uf, int N, int SS, Geo geo, double2 *partial) {
   extern __shared__ double2 sm[];
@@ -98,79 +117,62 @@ __global__ void __launch_bounds__(256, 1)
   const bool grouped = make_lane(L, g);
   const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
   const int row = 4 * (N + 1);
-  const size_t gsz = (size_t)LOOP_SLOTS * SS + RING + row;
+  const size_t gsz = (size_t)LOOP_SLOTS * SS + row;
   double2 *base = sm + (size_t)(warp * LPW + g) * gsz;
-  double2 *acc = base + (size_t)LOOP_SLOTS * SS + RING;
+  double2 *acc = base + (size_t)LOOP_SLOTS * SS;
   if (grouped) {
-    LoopCtx q;
-    q.U = U;
-    q.Uf = Uf;
-    q.STG = base + (size_t)8 * SS;
-    q.ring = q.STG + SS;
-    q.V = (size_t)geo.V;
-    q.plane = (size_t)9 * N * q.V;
-    q.N = N;
-    q.geo = geo;
-    double2 *S0 = base, *S1 = base + SS, *S2 = base + 2 * SS, *S3 = base + 3 * SS;
-    double2 *S4 = base + 4 * SS, *S5 = base + 5 * SS, *S6 = base + 6 * SS, *S7 = base + 7 * SS;
+    double2 *P = base, *Q = base + SS, *S = base + 2 * SS;
     for (int e = L.j; e < row; e += GROUP) acc[e] = cz();
     __syncwarp(L.mask);
     double2 *a21 = acc, *a22 = acc + (N + 1), *a42 = acc + 2 * (N + 1), *a44 = acc + 3 * (N + 1);
+    LoopCtx q;
+    q.U = U;
+    q.Uf = Uf;
+    q.N = N;
+    q.geo = geo;
+    const LoopPath p22{4, {0, 0, 1, 1}}, q22{4, {1, 1, 0, 0}};
+    const LoopPath p42u{6, {0, 0, 1, 1, 1, 1}}, q42u{6, {1, 1, 1, 1, 0, 0}};
+    const LoopPath p44{8, {0, 0, 0, 0, 1, 1, 1, 1}}, q44{8, {1, 1, 1, 1, 0, 0, 0, 0}};
+    const LoopPath p42r{6, {0, 0, 0, 0, 1, 1}}, q42r{6, {1, 1, 0, 0, 0, 0}};
+    const LoopPath p21a{3, {0, 0, 1}}, q21a{3, {1, 0, 0}};
+    const LoopPath p21b{3, {0, 1, 1}}, q21b{3, {1, 1, 0}};
     const long units = 6L * geo.V;
     const long stride = (long)gridDim.x * nw * LPW;
     for (long u = ((long)blockIdx.x * nw + warp) * LPW + g; u < units; u += stride) {
       const int pl = (int)(u / geo.V);
       const int x = (int)(u - (long)pl * geo.V);
-      const int mu = pl < 3 ? 0 : (pl < 5 ? 1 : 2);
-      const int nu = pl < 3 ? pl + 1 : (pl < 5 ? pl - 1 : 3);
-      int X[4];
-      coords(geo, x, X);
-      // site x + i mu + j nu
-      auto at = [&](int i, int j) {
-        int y[4] = {X[0], X[1], X[2], X[3]};
-        y[mu] = (y[mu] + i) % geo.L[mu];
-        y[nu] = (y[nu] + j) % geo.L[nu];
-        return y[0] * geo.s0 + y[1] * geo.s1 + y[2] * geo.s2 + y[3];
-      };
-      loop_two(q, S0, mu, x, mu, at(1, 0), L);           // bl
-      loop_two(q, S1, nu, x, nu, at(0, 1), L);           // ld
-      // 2x2: bl cd (ld ml)^dag
-      loop_two(q, S2, nu, at(2, 0), nu, at(2, 1), L);    // cd
-      loop_mul(S3, S0, S2, N, L);                        // T1 = bl cd
-      loop_two(q, S2, mu, at(0, 2), mu, at(1, 2), L);    // ml
-      loop_mul(S4, S1, S2, N, L);                        // T2 = ld ml
-      trace_dag_acc(S3, S4, N, L, a22);
-      // 2x4, upper: bl cd cu (ld lu tl)^dag
-      loop_two(q, S2, nu, at(2, 2), nu, at(2, 3), L);    // cu
-      loop_mul(S5, S3, S2, N, L);
-      loop_two(q, S2, nu, at(0, 2), nu, at(0, 3), L);    // lu
-      loop_mul(S6, S1, S2, N, L);
-      loop_two(q, S2, mu, at(0, 4), mu, at(1, 4), L);    // tl
-      loop_mul(S7, S6, S2, N, L);                        // ld lu tl
-      trace_dag_acc(S5, S7, N, L, a42);
-      // 2x4, right: bl br rd (ld ml mr)^dag
-      loop_two(q, S2, mu, at(2, 0), mu, at(3, 0), L);    // br
-      loop_mul(S3, S0, S2, N, L);
-      loop_two(q, S2, nu, at(4, 0), nu, at(4, 1), L);    // rd
-      loop_mul(S5, S3, S2, N, L);                        // bl br rd
-      loop_two(q, S2, mu, at(2, 2), mu, at(3, 2), L);    // mr
-      loop_mul(S6, S4, S2, N, L);                        // T2 mr
-      trace_dag_acc(S5, S6, N, L, a42);
-      // 4x4: bl br rd ru (ld lu tl tr)^dag
-      loop_two(q, S2, nu, at(4, 2), nu, at(4, 3), L);    // ru
-      loop_mul(S3, S5, S2, N, L);
-      loop_two(q, S2, mu, at(2, 4), mu, at(3, 4), L);    // tr
-      loop_mul(S6, S7, S2, N, L);
-      trace_dag_acc(S3, S6, N, L, a44);
+      q.mu = pl < 3 ? 0 : (pl < 5 ? 1 : 2);
+      q.nu = pl < 3 ? pl + 1 : (pl < 5 ? pl - 1 : 3);
+      coords(geo, x, q.X);
+      int pi = 0, pj = 0, qi = 0, qj = 0;
+      // 2x2
+      loop_chain(q, P, S, p22, 0, pi, pj, L);
+      loop_chain(q, Q, S, q22, 0, qi, qj, L);
+      trace_dag_acc(P, Q, N, L, a22);
+      // 2x4 up: P = bl cd extended by cu
+      loop_chain(q, P, S, p42u, 4, pi, pj, L);
+      qi = qj = 0;
+      loop_chain(q, Q, S, q42u, 0, qi, qj, L);
+      trace_dag_acc(P, Q, N, L, a42);
+      // 4x4: Q = ld lu tl extended by tr
+      loop_chain(q, Q, S, q44, 6, qi, qj, L);
+      pi = pj = 0;
+      loop_chain(q, P, S, p44, 0, pi, pj, L);
+      trace_dag_acc(P, Q, N, L, a44);
+      // 2x4 right
+      pi = pj = qi = qj = 0;
+      loop_chain(q, P, S, p42r, 0, pi, pj, L);
+      loop_chain(q, Q, S, q42r, 0, qi, qj, L);
+      trace_dag_acc(P, Q, N, L, a42);
       // 1x2, both orientations
-      loop_mul_link(q, S3, S0, nu, at(2, 0), L);         // bl U_nu(b)
-      loop_two(q, S2, nu, x, mu, at(0, 1), L);           // U_nu(x) U_mu(e)
-      loop_mul_link(q, S5, S2, mu, at(1, 1), L);         // ... U_mu(d)
-      trace_dag_acc(S3, S5, N, L, a21);
-      loop_two(q, S2, mu, x, nu, at(1, 0), L);           // U_mu(x) U_nu(a)
-      loop_mul_link(q, S3, S2, nu, at(1, 1), L);         // ... U_nu(d)
-      loop_mul_link(q, S5, S1, mu, at(0, 2), L);         // ld U_mu(h)
-      trace_dag_acc(S3, S5, N, L, a21);
+      pi = pj = qi = qj = 0;
+      loop_chain(q, P, S, p21a, 0, pi, pj, L);
+      loop_chain(q, Q, S, q21a, 0, qi, qj, L);
+      trace_dag_acc(P, Q, N, L, a21);
+      pi = pj = qi = qj = 0;
+      loop_chain(q, P, S, p21b, 0, pi, pj, L);
+      loop_chain(q, Q, S, q21b, 0, qi, qj, L);
+      trace_dag_acc(P, Q, N, L, a21);
     }
   }
   __syncthreads();
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(256, 1)
   for (int e = threadIdx.x; e < row; e += blockDim.x) {
     double2 sum = cz();
     for (int gi = 0; gi < ngroups; gi++)
-      sum = cadd(sum, sm[(size_t)gi * gsz + (size_t)LOOP_SLOTS * SS + RING + e]);
+      sum = cadd(sum, sm[(size_t)gi * gsz + (size_t)LOOP_SLOTS * SS + e]);
     partial[(size_t)blockIdx.x * row + e] = sum;
   }
 }
