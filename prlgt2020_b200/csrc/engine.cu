@@ -319,7 +319,7 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
   rc = launch_groups(
       ctx, (const void *)k_fa_apply, 2, nl,
       [&](unsigned g, dim3 b, size_t sm) { k_fa_apply<<<g, b, sm, st>>>(U, Uf, Gx, F, Ff, N, SS, geo); },
-      "FA apply", RING);
+      "FA apply");
   if (rc) return rc;
   std::swap(ctx->U, ctx->F);
   std::swap(ctx->Uf, ctx->Ff);
@@ -502,7 +502,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->SS = 1 + 9 * N;
   while (ctx->SS % 8 != 1) ctx->SS++;
   // one warp (3 link groups of 3 slots) must fit in a CTA
-  if ((size_t)LPW * group_bytes(ctx, SWEEP_SLOTS, RING) > ctx->smem_optin) return fail(NSPT_ERR_ORDER);
+  if ((size_t)LPW * group_bytes(ctx, SWEEP_SLOTS, 0) > ctx->smem_optin) return fail(NSPT_ERR_ORDER);
   if (ctx->c1 != 0.0 && (size_t)LPW * group_bytes(ctx, IMP_SLOTS, 0) > ctx->smem_optin)
     return fail(NSPT_ERR_ORDER);
   if (cudaStreamCreateWithFlags(&ctx->st, cudaStreamNonBlocking) != cudaSuccess) return fail(NSPT_ERR_CUDA);

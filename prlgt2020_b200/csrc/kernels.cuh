@@ -756,7 +756,7 @@ __global__ void __launch_bounds__(256, 1)
   if (!make_lane(L, g)) return;
   const int warp = threadIdx.x >> 5;
   const size_t V = (size_t)geo.V;
-  double2 *T = sm + (size_t)(warp * LPW + g) * (2 * SS + RING), *Y = T + SS, *ring = Y + SS;
+  double2 *T = sm + (size_t)(warp * LPW + g) * (2 * SS), *Y = T + SS;
   bool valid;
   const long link = group_unit(g, 4L * geo.V, valid);
   const int mu = (int)(link / geo.V);
@@ -768,9 +768,11 @@ __global__ void __launch_bounds__(256, 1)
   Nb n;
   n.site = site;
   n.fwd = n.bwd = 0;
+  // T = G(x), Y = U_mu(x), then T <- T Y in place
+  stage_site(T, Gx, site, V, N, L, one);
   stage(Y, U, Uf, mu, n, geo, N, L);
   const double2 tflag = cmul(one, Y[0]);
-  product<MO, false>(LeftG{Gx + site, V, ring}, one, Y, Y[0], N, L,
+  product<MO, false>(LeftS{T}, one, Y, Y[0], N, L,
                      [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
   if (L.j == 0) T[0] = tflag;
   __syncwarp(L.mask);

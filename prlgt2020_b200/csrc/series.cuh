@@ -105,47 +105,11 @@ struct Lane {
   unsigned mask;  // the group's lanes
 };
 
-// Left operand in the global row-major planes of one link (never a twisted
-// read: those are staged).  Element (k, r, l) at p[(9(k-1) + 3r + l) * V].  The
-// product streams it through a 3-order ring in shared memory: lane j of the
-// group copies colour component j of order i+2 with cp.async while order i
-// is in use, so the L2 latency of the next coefficients is hidden.
-constexpr int RING = 32;  // double2 per group: 3 orders x 9, padded to 0 mod 8
-struct LeftG {
-  static constexpr bool kRing = true;
-  const double2 *p;
-  size_t V;
-  double2 *ring;
-  __device__ __forceinline__ void issue(int k, int j) const {
-    const double2 *src = p + (size_t)(9 * (k - 1) + j) * V;
-    const unsigned dst = (unsigned)__cvta_generic_to_shared(ring + 9 * ((k - 1) % 3) + j);
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(src) : "memory");
-  }
-  template <bool DAG>
-  __device__ __forceinline__ void from_ring(int k, double2 *a) const {
-    const double2 *q = ring + 9 * ((k - 1) % 3);
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-#pragma unroll
-      for (int l = 0; l < 3; l++) a[3 * r + l] = DAG ? cconj(q[3 * l + r]) : q[3 * r + l];
-  }
-  // column c of op(A)_k (flag terms), straight from global
-  template <bool DAG>
-  __device__ __forceinline__ void col(int k, int c, double2 *o) const {
-    const double2 *q = p + (size_t)9 * (k - 1) * V;
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-      o[r] = DAG ? cconj(__ldg(q + (size_t)(3 * c + r) * V)) : __ldg(q + (size_t)(3 * r + c) * V);
-  }
-};
-
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_wait1() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_wait0() { asm volatile("cp.async.wait_group 0;\n" ::: "memory"); }
 
 // Left operand in a slot (column major).
 struct LeftS {
-  static constexpr bool kRing = false;
   const double2 *s;
   template <bool DAG>
   __device__ __forceinline__ void load(int k, double2 *a) const {
@@ -183,23 +147,8 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
 #pragma unroll
       for (int r = 0; r < 3; r++) acc[q][r] = cz();
     double2 a[9];
-    if constexpr (Left::kRing) {
-      // orders i0 and i0+1 in flight before the loop; one commit group per order
-      if (i0 < kend) A.issue(i0, L.j);
-      cp_commit();
-      if (i0 + 1 < kend) A.issue(i0 + 1, L.j);
-      cp_commit();
-    }
     for (int i = i0; i < kend; i++) {
-      if constexpr (Left::kRing) {
-        cp_wait1();               // this lane's copy of order i has landed
-        __syncwarp(L.mask);       // ... and every lane's; order i-1 is free
-        if (i + 2 < kend) A.issue(i + 2, L.j);
-        cp_commit();
-        A.template from_ring<DA>(i, a);
-      } else {
-        A.template load<DA>(i, a);
-      }
+      A.template load<DA>(i, a);
 #pragma unroll
       for (int q = 0; q < MO; q++) {
         const int k = kb + L.s + 1 + 3 * q;
@@ -215,7 +164,6 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
         }
       }
     }
-    if constexpr (Left::kRing) cp_wait0();
     __syncwarp(L.mask);
     const bool fa = !cis0(a0), fb = !cis0(b0);
 #pragma unroll
@@ -311,22 +259,8 @@ __device__ __forceinline__ void product_ff(const Left &A, double2 a0, const doub
 #pragma unroll
       for (int r = 0; r < 3; r++) acc[q][r] = {0.f, 0.f, 0.f, 0.f};
     double2 a[9];
-    if constexpr (Left::kRing) {
-      if (1 < kend) A.issue(1, L.j);
-      cp_commit();
-      if (2 < kend) A.issue(2, L.j);
-      cp_commit();
-    }
     for (int i = 1; i < kend; i++) {
-      if constexpr (Left::kRing) {
-        cp_wait1();
-        __syncwarp(L.mask);
-        if (i + 2 < kend) A.issue(i + 2, L.j);
-        cp_commit();
-        A.template from_ring<DA>(i, a);
-      } else {
-        A.template load<DA>(i, a);
-      }
+      A.template load<DA>(i, a);
       ffc af[9];
       const double sa = pow2i(e * i);
 #pragma unroll
@@ -347,7 +281,6 @@ __device__ __forceinline__ void product_ff(const Left &A, double2 a0, const doub
         }
       }
     }
-    if constexpr (Left::kRing) cp_wait0();
     __syncwarp(L.mask);
     const bool fa = !cis0(a0), fb = !cis0(b0);
 #pragma unroll
