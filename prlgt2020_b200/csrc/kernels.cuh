@@ -320,6 +320,31 @@ __device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, doub
 constexpr int SWEEP_THREADS = NSPT_SWEEP_THREADS;
 constexpr int SWEEP_SLOTS = 3;
 
+// Slot products shared by the sweeps' staple chains (one copy of the
+// product code each, not one per call site).
+// T <- T Y, in place
+__device__ __noinline__ void slot_mul(double2 *T, const double2 *Y, int N, const Lane &L) {
+  const double2 a0 = T[0], b0 = Y[0];
+  const int c = L.c;
+  product<MO, false>(LeftS{T}, a0, Y, b0, N, L,
+                     [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+  if (L.j == 0) T[0] = flag_mul(a0, b0);
+  __syncwarp(L.mask);
+}
+
+// Wacc (+)= T Y; first: Wacc = T Y.  Returns the product's flag.
+__device__ __noinline__ double2 slot_acc(double2 *Wacc, const double2 *T, const double2 *Y,
+                                        bool first, int N, const Lane &L) {
+  const double2 a0 = T[0], b0 = Y[0];
+  const int c = L.c;
+  product<MO, false>(LeftS{T}, a0, Y, b0, N, L, [&](int k, int r, double2 v) {
+    double2 &w = Wacc[sidx(k, r, c)];
+    w = first ? v : cadd(w, v);
+  });
+  __syncwarp(L.mask);
+  return flag_mul(a0, b0);
+}
+
 template <bool MEASURE, bool FF = false>
 __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
   const int ffe = FF ? *a.ff_scale : 0;
@@ -343,68 +368,69 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
 
   double2 wflag = cz();
   bool first = true;
+  // A <- A B in place; W (+)= A B.  FP64: one out-of-line copy each;
+  // float-float: the compensated product inline.
+  auto mul = [&](double2 *A, const double2 *B) {
+    if constexpr (FF) {
+      const double2 a0 = A[0], b0 = B[0];
+      cprod<FF, MO, false>(LeftS{A}, a0, B, b0, N, L, ffe,
+                           [&](int k, int r, double2 v) { A[sidx(k, r, c)] = v; });
+      if (L.j == 0) A[0] = flag_mul(a0, b0);
+      __syncwarp(L.mask);
+    } else {
+      slot_mul(A, B, N, L);
+    }
+  };
+  auto acc = [&](const double2 *A, const double2 *B) {
+    double2 f;
+    if constexpr (FF) {
+      const double2 a0 = A[0], b0 = B[0];
+      const bool f0 = first;
+      cprod<FF, MO, false>(LeftS{A}, a0, B, b0, N, L, ffe, [&](int k, int r, double2 v) {
+        double2 &w = W[sidx(k, r, c)];
+        w = f0 ? v : cadd(w, v);
+      });
+      __syncwarp(L.mask);
+      f = flag_mul(a0, b0);
+    } else {
+      f = slot_acc(W, A, B, first, N, L);
+    }
+    wflag = first ? f : cadd(wflag, f);
+    first = false;
+  };
+  Nb self;
+  self.site = site;
+  self.fwd = self.bwd = 0;
   for (int nu = 0; nu < 4; nu++) {
     if (nu == mu) continue;
-    // ---- upper staple U_nu(x+mu) [U_nu(x) U_mu(x+nu)]^dag (QCDenvNODEpt_test.h:555),
-    // formed as (U_nu(x+mu) U_mu(x+nu)^dag) U_nu(x)^dag: the same truncated
-    // series (the product is associative), with every operand staged
+    // Each staple as its chain of links, multiplied left to right in T with
+    // the next link staged into Y (the truncated product is associative):
+    // upper U_nu(x+mu) [U_nu(x) U_mu(x+nu)]^dag
+    //     = U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag      (QCDenvNODEpt_test.h:555),
+    // lower [U_mu(x-nu) U_nu(x-nu+mu)]^dag U_nu(x-nu)
+    //     = U_nu(x+mu-nu)^dag U_mu(x-nu)^dag U_nu(x-nu)  (QCDenvNODEpt_test.h:556).
+    // Links that cross a twisted face are staged twisted.
     {
-      // U_nu(x+mu) into T (twisted when it crosses a twisted face), then
-      // T <- T U_mu(x+nu)^dag in place
       const Nb m = neighbour(a.g, x, mu, 1);
       const Nb b = neighbour(a.g, x, nu, 1);
       stage(T, a.U, a.Uf, nu, m, a.g, N, L);
       stage(Y, a.U, a.Uf, mu, b, a.g, N, L, true);
-      const double2 a0 = T[0], y0 = Y[0];
-      cprod<FF, MO, false>(LeftS{T}, a0, Y, y0, N, L, ffe,
-                           [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
-      if (L.j == 0) T[0] = flag_mul(a0, y0);
-      __syncwarp(L.mask);
-    }
-    {
-      Nb self;
-      self.site = site;
-      self.fwd = self.bwd = 0;
+      mul(T, Y);
       stage(Y, a.U, a.Uf, nu, self, a.g, N, L, true);
-      const double2 a0 = T[0];
-      const double2 b0 = Y[0];
-      const bool f0 = first;
-      cprod<FF, MO, false>(LeftS{T}, a0, Y, b0, N, L, ffe, [&](int k, int r, double2 v) {
-        double2 &w = W[sidx(k, r, c)];
-        w = f0 ? v : cadd(w, v);
-      });
-      const double2 f = flag_mul(a0, b0);
-      wflag = first ? f : cadd(wflag, f);
-      first = false;
+      acc(T, Y);
     }
-    // ---- lower staple [U_mu(x-nu) U_nu(x-nu+mu)]^dag U_nu(x-nu) (QCDenvNODEpt_test.h:556)
     {
       const Nb d = neighbour(a.g, x, nu, -1);
       const Nb dm = neighbour(a.g, x, nu, -1, mu, 1);
-      stage(Y, a.U, a.Uf, nu, dm, a.g, N, L);
-      // U_mu(x-nu) is staged into T and the product overwrites it in place:
-      // every lane reads a pass before any lane writes it, and the flag term
-      // of a result cell reads only that cell's own column of the left operand
-      stage(T, a.U, a.Uf, mu, d, a.g, N, L);
-      const double2 a0 = T[0], y0 = Y[0];
-      cprod<FF, MO, false>(LeftS{T}, a0, Y, y0, N, L, ffe,
-                         [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
-      if (L.j == 0) T[0] = flag_mul(a0, y0);
-      __syncwarp(L.mask);
+      stage(T, a.U, a.Uf, nu, dm, a.g, N, L, true);
+      stage(Y, a.U, a.Uf, mu, d, a.g, N, L, true);
+      mul(T, Y);
       stage(Y, a.U, a.Uf, nu, d, a.g, N, L);
-      const double2 ta = cconj(T[0]);
-      cprod<FF, MO, true>(LeftS{T}, ta, Y, Y[0], N, L, ffe, [&](int k, int r, double2 v) {
-        double2 &w = W[sidx(k, r, c)];
-        w = cadd(w, v);
-      });
-      wflag = cadd(wflag, flag_mul(ta, Y[0]));
+      acc(T, Y);
     }
   }
   if (L.j == 0) W[0] = wflag;
   // ---- P = U_mu(x) * staples (nspt.cc:392) into T; U_mu(x) in Y
-  Nb self;
-  self.site = site;
-  self.fwd = self.bwd = 0;
   stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
   const double2 pflag = flag_mul(Y[0], wflag);
   cprod<FF, MO, false>(LeftS{Y}, Y[0], W, wflag, N, L, ffe,
@@ -469,29 +495,6 @@ __device__ __forceinline__ void imp_stage(const SweepArgs &a, double2 *slot, con
   stage(slot, a.U, a.Uf, l.d, n, a.g, a.N, L, l.dag);
 }
 
-// T <- T Y, in place
-__device__ __noinline__ void imp_mul(double2 *T, const double2 *Y, int N, const Lane &L) {
-  const double2 a0 = T[0], b0 = Y[0];
-  const int c = L.c;
-  product<MO, false>(LeftS{T}, a0, Y, b0, N, L,
-                     [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
-  if (L.j == 0) T[0] = flag_mul(a0, b0);
-  __syncwarp(L.mask);
-}
-
-// Wacc (+)= T Y; first: Wacc = T Y.  Returns the product's flag.
-__device__ __noinline__ double2 imp_acc(double2 *Wacc, const double2 *T, const double2 *Y,
-                                        bool first, int N, const Lane &L) {
-  const double2 a0 = T[0], b0 = Y[0];
-  const int c = L.c;
-  product<MO, false>(LeftS{T}, a0, Y, b0, N, L, [&](int k, int r, double2 v) {
-    double2 &w = Wacc[sidx(k, r, c)];
-    w = first ? v : cadd(w, v);
-  });
-  __syncwarp(L.mask);
-  return flag_mul(a0, b0);
-}
-
 // Wacc (+)= l[0] l[1] ... l[n-1]; returns the flag of the chain
 template <int NL>
 __device__ __forceinline__ double2 imp_chain(const SweepArgs &a, double2 *T, double2 *Y,
@@ -501,10 +504,10 @@ __device__ __forceinline__ double2 imp_chain(const SweepArgs &a, double2 *T, dou
 #pragma unroll
   for (int m = 1; m < NL - 1; m++) {
     imp_stage(a, Y, l[m], L);
-    imp_mul(T, Y, a.N, L);
+    slot_mul(T, Y, a.N, L);
   }
   imp_stage(a, Y, l[NL - 1], L);
-  return imp_acc(Wacc, T, Y, first, a.N, L);
+  return slot_acc(Wacc, T, Y, first, a.N, L);
 }
 
 __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
