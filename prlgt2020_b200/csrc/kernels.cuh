@@ -332,6 +332,16 @@ __device__ __noinline__ void slot_mul(double2 *T, const double2 *Y, int N, const
   __syncwarp(L.mask);
 }
 
+// out <- A B, orders 1..N (out may be B: the product works in place); the
+// flag is the caller's
+__device__ __noinline__ void slot_mul_to(double2 *out, const double2 *A, const double2 *B, int N,
+                                         const Lane &L) {
+  const int c = L.c;
+  product<MO, false>(LeftS{A}, A[0], B, B[0], N, L,
+                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
+  __syncwarp(L.mask);
+}
+
 // Wacc (+)= T Y; first: Wacc = T Y.  Returns the product's flag.
 __device__ __noinline__ double2 slot_acc(double2 *Wacc, const double2 *T, const double2 *Y,
                                         bool first, int N, const Lane &L) {
@@ -599,13 +609,8 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
   self.fwd = self.bwd = 0;
   stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
   const double2 pflag = flag_mul(Y[0], wflag), p2flag = flag_mul(Y[0], w2flag);
-  {
-    const int c = L.c;
-    product<MO, false>(LeftS{Y}, Y[0], W, wflag, N, L,
-                       [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
-    product<MO, false>(LeftS{Y}, Y[0], W2, w2flag, N, L,
-                       [&](int k, int r, double2 v) { W2[sidx(k, r, c)] = v; });
-  }
+  slot_mul_to(T, Y, W, N, L);
+  slot_mul_to(W2, Y, W2, N, L);
   if (L.j == 0) {
     T[0] = pflag;
     W2[0] = p2flag;
