@@ -559,16 +559,47 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
   for (nu = 0; nu < 4; nu++) {
     if (nu == mu) continue;
     const int m = mu, n = nu;
-    // ---- Wilson staples (QCDenvNODEpt_test.h:554-557):
-    // U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag and
-    // U_nu(x+mu-nu)^dag U_mu(x-nu)^dag U_nu(x-nu)
+    auto st = [&](double2 *slot, int d, int st_site, bool dag) {
+      imp_stage(a, slot, ImpLink{d, st_site, dag}, L);
+    };
+    // ---- Wilson staples (QCDenvNODEpt_test.h:554-557) and the two
+    // rectangles that begin with a Wilson staple's first two links, which
+    // are formed once for both:
+    //   upper U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag, and
+    //   U_nu(a) dag(U_nu(f) U_mu(g) U_mu(c)) U_mu(f)
+    //     = U_nu(a) U_mu(c)^dag U_mu(g)^dag U_nu(f)^dag U_mu(f),
+    //     a=x+mu c=x+nu f=x-mu g=x-mu+nu;
+    //   lower U_nu(x+mu-nu)^dag U_mu(x-nu)^dag U_nu(x-nu), and
+    //   dag(U_mu(g) U_mu(c) U_nu(b)) U_nu(g) U_mu(h)
+    //     = U_nu(b)^dag U_mu(c)^dag U_mu(g)^dag U_nu(g) U_mu(h),
+    //     b=x+mu-nu c=x-nu g=x-mu-nu h=x-mu
     {
-      const ImpLink up[3] = {{n, at(1, 0), false}, {m, at(0, 1), true}, {n, site, true}};
-      acc(imp_chain(a, T, Y, W, up, first, L));
-      const ImpLink lo[3] = {{n, at(1, -1), true}, {m, at(0, -1), true}, {n, at(0, -1), false}};
-      acc(imp_chain(a, T, Y, W, lo, first, L));
+      st(T, n, at(1, 0), false);
+      st(Y, m, at(0, 1), true);
+      slot_mul(T, Y, N, L);
+      st(Y, n, site, true);
+      acc(slot_acc(W, T, Y, first, N, L));
+      st(Y, m, at(-1, 1), true);
+      slot_mul(T, Y, N, L);
+      st(Y, n, at(-1, 0), true);
+      slot_mul(T, Y, N, L);
+      st(Y, m, at(-1, 0), false);
+      acc2(slot_acc(W2, T, Y, first2, N, L));
     }
-    // ---- the six rectangles of staple2x1, each as its chain of five links
+    {
+      st(T, n, at(1, -1), true);
+      st(Y, m, at(0, -1), true);
+      slot_mul(T, Y, N, L);
+      st(Y, n, at(0, -1), false);
+      acc(slot_acc(W, T, Y, first, N, L));
+      st(Y, m, at(-1, -1), true);
+      slot_mul(T, Y, N, L);
+      st(Y, n, at(-1, -1), false);
+      slot_mul(T, Y, N, L);
+      st(Y, m, at(-1, 0), false);
+      acc2(slot_acc(W2, T, Y, first2, N, L));
+    }
+    // ---- the other four rectangles of staple2x1, each its chain of five links
     {
       // U_nu(a) U_nu(b) dag(U_nu(x) U_nu(c) U_mu(d)),  a=x+mu b=x+mu+nu c=x+nu d=x+2nu
       const ImpLink r1[5] = {{n, at(1, 0), false}, {n, at(1, 1), false}, {m, at(0, 2), true},
@@ -578,10 +609,6 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
       const ImpLink r2[5] = {{m, at(1, 0), false}, {n, at(2, 0), false}, {m, at(1, 1), true},
                              {m, at(0, 1), true}, {n, site, true}};
       acc2(imp_chain(a, T, Y, W2, r2, first2, L));
-      // U_nu(a) dag(U_nu(f) U_mu(g) U_mu(c)) U_mu(f),  f=x-mu g=x-mu+nu
-      const ImpLink r3[5] = {{n, at(1, 0), false}, {m, at(0, 1), true}, {m, at(-1, 1), true},
-                             {n, at(-1, 0), true}, {m, at(-1, 0), false}};
-      acc2(imp_chain(a, T, Y, W2, r3, first2, L));
       // dag(U_mu(d) U_nu(e) U_nu(b)) U_nu(d) U_nu(c),
       // b=x+mu-nu c=x-nu d=x-2nu e=x+mu-2nu
       const ImpLink r4[5] = {{n, at(1, -1), true}, {n, at(1, -2), true}, {m, at(0, -2), true},
@@ -591,10 +618,6 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
       const ImpLink r5[5] = {{m, at(1, 0), false}, {n, at(2, -1), true}, {m, at(1, -1), true},
                              {m, at(0, -1), true}, {n, at(0, -1), false}};
       acc2(imp_chain(a, T, Y, W2, r5, first2, L));
-      // dag(U_mu(g) U_mu(c) U_nu(b)) U_nu(g) U_mu(h),  g=x-mu-nu h=x-mu
-      const ImpLink r6[5] = {{n, at(1, -1), true}, {m, at(0, -1), true}, {m, at(-1, -1), true},
-                             {n, at(-1, -1), false}, {m, at(-1, 0), false}};
-      acc2(imp_chain(a, T, Y, W2, r6, first2, L));
     }
   }
   if (L.j == 0) {
