@@ -110,11 +110,13 @@ static size_t group_bytes(const nspt_ctx *ctx, int slots, int extra) {
 }
 
 static KernelShape choose_shape(const nspt_ctx *ctx, int slots, long units, int extra = 0,
-                                int max_warps = 8) {
+                                int max_warps = 8, int ctas_per_sm = 1) {
   KernelShape k;
   k.slots = slots;
   const size_t per_warp = (size_t)LPW * group_bytes(ctx, slots, extra);
-  int wmax = (int)std::min<size_t>(max_warps, ctx->smem_optin / per_warp);
+  // shared memory per SM: 228 KB, of which up to smem_optin for one CTA
+  const size_t budget = ctas_per_sm > 1 ? (size_t)228 * 1024 / ctas_per_sm - 1024 : ctx->smem_optin;
+  int wmax = (int)std::min<size_t>(max_warps, std::min(budget, ctx->smem_optin) / per_warp);
   if (wmax < 1) wmax = 1;
   // spread small lattices over the SMs: about two CTAs per SM if possible
   const long want = (units + (long)LPW * 2 * ctx->nsm - 1) / ((long)LPW * 2 * ctx->nsm);
@@ -122,26 +124,33 @@ static KernelShape choose_shape(const nspt_ctx *ctx, int slots, long units, int 
   return k;
 }
 
-template <bool MEASURE, bool FF>
+template <bool MEASURE, bool FF, bool LOW = false>
 static void sweep_kernel(dim3 grid, dim3 blk, size_t smem, cudaStream_t st, const SweepArgs &a) {
-  cudaFuncSetAttribute(k_sweep<MEASURE, FF>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_sweep<MEASURE, FF><<<grid, blk, smem, st>>>(a);
+  cudaFuncSetAttribute(k_sweep<MEASURE, FF, LOW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  k_sweep<MEASURE, FF, LOW><<<grid, blk, smem, st>>>(a);
 }
 
 static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
   const long nl = 4 * ctx->V;
+  const bool ff = (ctx->flags & NSPT_PRECISION_FF) != 0;
+  // low orders: the lighter variant, two CTAs per SM
+  const bool low = !measure && !ff && ctx->N <= 3 * MO_LOW;
+  const int max_warps = (low ? SWEEP_THREADS_LOW : SWEEP_THREADS) / 32;
   KernelShape k = choose_shape(ctx, SWEEP_SLOTS, nl, 0,
-                               ctx->sweep_warps > 0 ? std::min(ctx->sweep_warps, SWEEP_THREADS / 32)
-                                                    : SWEEP_THREADS / 32);
+                               ctx->sweep_warps > 0 ? std::min(ctx->sweep_warps, max_warps)
+                                                    : max_warps,
+                               low ? 2 : 1);
   const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, SWEEP_SLOTS, 0);
   const long per_cta = (long)k.warps * LPW;
   const unsigned grid = (unsigned)((nl + per_cta - 1) / per_cta);
   const dim3 blk(32 * k.warps);
-  const bool ff = (ctx->flags & NSPT_PRECISION_FF) != 0;
   if (measure)
     sweep_kernel<true, false>(grid, blk, smem, ctx->st, a);
   else if (ff)
     sweep_kernel<false, true>(grid, blk, smem, ctx->st, a);
+  else if (low)
+    sweep_kernel<false, false, true>(grid, blk, smem, ctx->st, a);
   else
     sweep_kernel<false, false>(grid, blk, smem, ctx->st, a);
   CK(cudaGetLastError());

@@ -253,6 +253,7 @@ __device__ __forceinline__ long group_unit(int g, long nunits, bool &valid) {
 // U_mu(x) in slot Y, observables written: W1 = reH(W1) tau_g - stau eta,
 // F = exp(W1) U_mu(x), and the per-link log for the zero modes.  W is a
 // free slot.  Shared by the Wilson and the improved-action sweeps.
+template <int MOx = MO>
 __device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, double2 *Y, double2 *W,
                                             long link, int mu, int site, const Nb &self,
                                             const Lane &L) {
@@ -289,11 +290,11 @@ __device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, doub
   }
   // ---- F = exp(W1) * U  (nspt.cc:429): exp into Y (W holds the square of
   // W1), U_mu(x) restaged into W
-  ser_exp<MO>(T, W, Y, N, L);
+  ser_exp<MOx>(T, W, Y, N, L);
   stage(W, a.U, a.Uf, mu, self, a.g, N, L);
   const bool zm = a.Lg != nullptr;
   double2 *Fc = a.F + (size_t)mu * plane_mu + site;
-  product<MO, false>(LeftS{Y}, make_double2(1.0, 0.0), W, W[0], N, L,
+  product<MOx, false>(LeftS{Y}, make_double2(1.0, 0.0), W, W[0], N, L,
                      [&](int k, int r, double2 v) {
                        Fc[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
                        if (zm) W[sidx(k, r, c)] = v;
@@ -303,7 +304,7 @@ __device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, doub
   __syncwarp(L.mask);
   // ---- MM[mu] += log(F[link])  (nspt.cc:432-439): logs stored per link
   double2 *Lo = a.Lg + (size_t)mu * plane_mu + site;
-  ser_log<MO>(W, T, Y, N, L, [&](int k, int r, double2 v) {
+  ser_log<MOx>(W, T, Y, N, L, [&](int k, int r, double2 v) {
     Lo[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
   });
 }
@@ -323,10 +324,11 @@ constexpr int SWEEP_SLOTS = 3;
 // Slot products shared by the sweeps' staple chains (one copy of the
 // product code each, not one per call site).
 // T <- T Y, in place
+template <int MOx = MO>
 __device__ __noinline__ void slot_mul(double2 *T, const double2 *Y, int N, const Lane &L) {
   const double2 a0 = T[0], b0 = Y[0];
   const int c = L.c;
-  product<MO, false>(LeftS{T}, a0, Y, b0, N, L,
+  product<MOx, false>(LeftS{T}, a0, Y, b0, N, L,
                      [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
   if (L.j == 0) T[0] = flag_mul(a0, b0);
   __syncwarp(L.mask);
@@ -343,11 +345,12 @@ __device__ __noinline__ void slot_mul_to(double2 *out, const double2 *A, const d
 }
 
 // Wacc (+)= T Y; first: Wacc = T Y.  Returns the product's flag.
+template <int MOx = MO>
 __device__ __noinline__ double2 slot_acc(double2 *Wacc, const double2 *T, const double2 *Y,
                                         bool first, int N, const Lane &L) {
   const double2 a0 = T[0], b0 = Y[0];
   const int c = L.c;
-  product<MO, false>(LeftS{T}, a0, Y, b0, N, L, [&](int k, int r, double2 v) {
+  product<MOx, false>(LeftS{T}, a0, Y, b0, N, L, [&](int k, int r, double2 v) {
     double2 &w = Wacc[sidx(k, r, c)];
     w = first ? v : cadd(w, v);
   });
@@ -355,8 +358,17 @@ __device__ __noinline__ double2 slot_acc(double2 *Wacc, const double2 *T, const 
   return flag_mul(a0, b0);
 }
 
-template <bool MEASURE, bool FF = false>
-__global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
+// LOW: the variant for N <= 3 * MO_LOW: products with MO_LOW orders per lane
+// and pass in CTAs of at most 6 warps, two CTAs per SM (about 168
+// registers a thread), so that an SM holds 12 warps where shared memory
+// allows.
+constexpr int MO_LOW = 4;
+constexpr int SWEEP_THREADS_LOW = 192;
+
+template <bool MEASURE, bool FF = false, bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ? 2 : 1)
+    k_sweep(SweepArgs a) {
+  constexpr int MOK = LOW ? MO_LOW : MO;
   const int ffe = FF ? *a.ff_scale : 0;
   extern __shared__ double2 sm[];
   Lane L;
@@ -388,7 +400,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
       if (L.j == 0) A[0] = flag_mul(a0, b0);
       __syncwarp(L.mask);
     } else {
-      slot_mul(A, B, N, L);
+      slot_mul<MOK>(A, B, N, L);
     }
   };
   auto acc = [&](const double2 *A, const double2 *B) {
@@ -403,7 +415,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
       __syncwarp(L.mask);
       f = flag_mul(a0, b0);
     } else {
-      f = slot_acc(W, A, B, first, N, L);
+      f = slot_acc<MOK>(W, A, B, first, N, L);
     }
     wflag = first ? f : cadd(wflag, f);
     first = false;
@@ -443,7 +455,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
   // ---- P = U_mu(x) * staples (nspt.cc:392) into T; U_mu(x) in Y
   stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
   const double2 pflag = flag_mul(Y[0], wflag);
-  cprod<FF, MO, false>(LeftS{Y}, Y[0], W, wflag, N, L, ffe,
+  cprod<FF, MOK, false>(LeftS{Y}, Y[0], W, wflag, N, L, ffe,
                      [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
   if (L.j == 0) T[0] = pflag;
   __syncwarp(L.mask);
@@ -474,7 +486,7 @@ __global__ void __launch_bounds__(SWEEP_THREADS, 1) k_sweep(SweepArgs a) {
   }
   if constexpr (MEASURE) return;
   __syncwarp(L.mask);
-  update_link(a, T, Y, W, link, mu, site, self, L);
+  update_link<MOK>(a, T, Y, W, link, mu, site, self, L);
 }
 
 // ---------------- improved gauge actions ----------------
