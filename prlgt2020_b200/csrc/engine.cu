@@ -170,10 +170,13 @@ static int launch_sweep_imp(nspt_ctx *ctx, const SweepArgs &a) {
 }
 
 // Launch a per-link (or per-site) group kernel with `slots` series per group.
+// low: the kernel's low-order instantiation (N <= 3 MO_LOW; 6-warp CTAs,
+// two per SM).
 template <class Fn>
 static int launch_groups(nspt_ctx *ctx, const void *fn, int slots, long units, Fn launch,
-                         const char *what, int extra = 0) {
-  KernelShape k = choose_shape(ctx, slots, units, extra);
+                         const char *what, int extra = 0, bool low = false) {
+  KernelShape k = low ? choose_shape(ctx, slots, units, extra, SWEEP_THREADS_LOW / 32, 2)
+                      : choose_shape(ctx, slots, units, extra);
   const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, slots, extra);
   const long per_cta = (long)k.warps * LPW;
   const unsigned grid = (unsigned)((units + per_cta - 1) / per_cta);
@@ -271,10 +274,16 @@ static int do_zero_modes(nspt_ctx *ctx) {
   const int SS = ctx->SS;
   const Geo geo = ctx->geo;
   cudaStream_t st = ctx->st;
+  const bool low = N <= 3 * MO_LOW;
   return launch_groups(
-      ctx, (const void *)k_zero_modes, 3, nl,
-      [&](unsigned g, dim3 b, size_t sm) { k_zero_modes<<<g, b, sm, st>>>(U, Uf, Lg, MM, N, SS, geo); },
-      "zero modes");
+      ctx, low ? (const void *)k_zero_modes<true> : (const void *)k_zero_modes<false>, 3, nl,
+      [&](unsigned g, dim3 b, size_t sm) {
+        if (low)
+          k_zero_modes<true><<<g, b, sm, st>>>(U, Uf, Lg, MM, N, SS, geo);
+        else
+          k_zero_modes<false><<<g, b, sm, st>>>(U, Uf, Lg, MM, N, SS, geo);
+      },
+      "zero modes", 0, low);
 }
 
 static int fft4d(nspt_ctx *ctx, double2 *data, int sign) {
@@ -307,10 +316,16 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
   cudaStream_t st = ctx->st;
   double2 *U = ctx->U, *Uf = ctx->Uf, *F = ctx->F, *Ff = ctx->Ff, *Lg = ctx->Lg, *Wg = ctx->Wg,
           *Gx = ctx->Gx;
+  const bool low = N <= 3 * MO_LOW;
   int rc = launch_groups(
-      ctx, (const void *)k_log_links, 3, nl,
-      [&](unsigned g, dim3 b, size_t sm) { k_log_links<<<g, b, sm, st>>>(U, Uf, Lg, N, SS, geo); },
-      "FA logs");
+      ctx, low ? (const void *)k_log_links<true> : (const void *)k_log_links<false>, 3, nl,
+      [&](unsigned g, dim3 b, size_t sm) {
+        if (low)
+          k_log_links<true><<<g, b, sm, st>>>(U, Uf, Lg, N, SS, geo);
+        else
+          k_log_links<false><<<g, b, sm, st>>>(U, Uf, Lg, N, SS, geo);
+      },
+      "FA logs", 0, low);
   if (rc) return rc;
   const size_t tot = (size_t)9 * N * ctx->V;
   const unsigned eg = (unsigned)std::min<size_t>((tot + 255) / 256, (size_t)ctx->nsm * 32);
@@ -321,14 +336,24 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
   CK(cudaGetLastError());
   if ((rc = fft4d(ctx, Wg, +1))) return rc;
   rc = launch_groups(
-      ctx, (const void *)k_fa_gt, 3, ctx->V,
-      [&](unsigned g, dim3 b, size_t sm) { k_fa_gt<<<g, b, sm, st>>>(Wg, Gx, N, SS, geo); },
-      "FA gauge transform");
+      ctx, low ? (const void *)k_fa_gt<true> : (const void *)k_fa_gt<false>, 3, ctx->V,
+      [&](unsigned g, dim3 b, size_t sm) {
+        if (low)
+          k_fa_gt<true><<<g, b, sm, st>>>(Wg, Gx, N, SS, geo);
+        else
+          k_fa_gt<false><<<g, b, sm, st>>>(Wg, Gx, N, SS, geo);
+      },
+      "FA gauge transform", 0, low);
   if (rc) return rc;
   rc = launch_groups(
-      ctx, (const void *)k_fa_apply, 2, nl,
-      [&](unsigned g, dim3 b, size_t sm) { k_fa_apply<<<g, b, sm, st>>>(U, Uf, Gx, F, Ff, N, SS, geo); },
-      "FA apply");
+      ctx, low ? (const void *)k_fa_apply<true> : (const void *)k_fa_apply<false>, 2, nl,
+      [&](unsigned g, dim3 b, size_t sm) {
+        if (low)
+          k_fa_apply<true><<<g, b, sm, st>>>(U, Uf, Gx, F, Ff, N, SS, geo);
+        else
+          k_fa_apply<false><<<g, b, sm, st>>>(U, Uf, Gx, F, Ff, N, SS, geo);
+      },
+      "FA apply", 0, low);
   if (rc) return rc;
   std::swap(ctx->U, ctx->F);
   std::swap(ctx->Uf, ctx->Ff);

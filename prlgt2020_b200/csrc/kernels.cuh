@@ -692,7 +692,8 @@ __global__ void k_inc(unsigned long long *c) { *c += 1ull; }
 
 // U = exp(reH(log U - MM[mu]/V)) per link: zero_modes_subtraction,
 // nspt.cc:605-654 (log U is the per-link log stored by the sweep).
-__global__ void __launch_bounds__(256, 1)
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
     k_zero_modes(double2 *U, double2 *Uf, const double2 *Lg, const double2 *MMs, int N, int SS,
                  Geo geo) {
   extern __shared__ double2 sm[];
@@ -722,7 +723,7 @@ __global__ void __launch_bounds__(256, 1)
   __syncwarp(L.mask);
   ser_reH(P, N, L);
   __syncwarp(L.mask);
-  ser_exp<MO>(P, Y2, R, N, L);
+  ser_exp<(LOW ? MO_LOW : MO)>(P, Y2, R, N, L);
   double2 *dst = U + (size_t)mu * 9 * N * V + site;
   const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
   for (int k = 1; k <= N; k++) dst[(size_t)(9 * (k - 1) + L.j) * V] = R[sidx(k, r, c)];
@@ -730,7 +731,8 @@ __global__ void __launch_bounds__(256, 1)
 }
 
 // Lg = log(U) per link (the logs FAstochastic_gauge_fixing needs, nspt.cc:874-875).
-__global__ void __launch_bounds__(256, 1)
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
     k_log_links(const double2 *U, const double2 *Uf, double2 *Lg, int N, int SS, Geo geo) {
   extern __shared__ double2 sm[];
   Lane L;
@@ -750,13 +752,14 @@ __global__ void __launch_bounds__(256, 1)
   stage(X, U, Uf, mu, n, geo, N, L);
   double2 *dst = Lg + (size_t)mu * 9 * N * V + site;
   const int c = L.c;
-  ser_log<MO>(X, Y2, Sc, N, L, [&](int k, int r, double2 v) {
+  ser_log<(LOW ? MO_LOW : MO)>(X, Y2, Sc, N, L, [&](int k, int r, double2 v) {
     dst[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
   });
 }
 
 // G(x) = exp(reH(Wg(x) / V))  (nspt.cc:902-906), one group per site.
-__global__ void __launch_bounds__(256, 1)
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
     k_fa_gt(const double2 *Wg, double2 *Gx, int N, int SS, Geo geo) {
   extern __shared__ double2 sm[];
   Lane L;
@@ -785,12 +788,13 @@ __global__ void __launch_bounds__(256, 1)
   __syncwarp(L.mask);
   ser_reH(P, N, L);
   __syncwarp(L.mask);
-  ser_exp<MO>(P, Y2, R, N, L);
+  ser_exp<(LOW ? MO_LOW : MO)>(P, Y2, R, N, L);
   for (int k = 1; k <= N; k++) Gx[(size_t)(9 * (k - 1) + L.j) * V + site] = R[sidx(k, r, c)];
 }
 
 // U_mu(x) <- G(x) U_mu(x) G(x+mu)^dag  (nspt.cc:912-916), written to F.
-__global__ void __launch_bounds__(256, 1)
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
     k_fa_apply(const double2 *U, const double2 *Uf, const double2 *Gx, double2 *F, double2 *Ff,
                int N, int SS, Geo geo) {
   extern __shared__ double2 sm[];
@@ -815,14 +819,14 @@ __global__ void __launch_bounds__(256, 1)
   stage_site(T, Gx, site, V, N, L, one);
   stage(Y, U, Uf, mu, n, geo, N, L);
   const double2 tflag = cmul(one, Y[0]);
-  product<MO, false>(LeftS{T}, one, Y, Y[0], N, L,
+  product<(LOW ? MO_LOW : MO), false>(LeftS{T}, one, Y, Y[0], N, L,
                      [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
   if (L.j == 0) T[0] = tflag;
   __syncwarp(L.mask);
   const Nb up = neighbour(geo, x, mu, 1);
   stage_site(Y, Gx, up.site, V, N, L, one, true);
   double2 *dst = F + (size_t)mu * 9 * N * V + site;
-  product<MO, false>(LeftS{T}, tflag, Y, one, N, L, [&](int k, int r, double2 v) {
+  product<(LOW ? MO_LOW : MO), false>(LeftS{T}, tflag, Y, one, N, L, [&](int k, int r, double2 v) {
     if (valid) dst[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
   });
   if (L.j == 0 && valid) Ff[(size_t)mu * V + site] = cmul(tflag, one);
