@@ -704,6 +704,38 @@ def run_loops(args, world, rank, local):
     eng.close()
 
 
+def run_qcfg(args, world, rank, local):
+    """The reference's shipped Quench.cfg run: 12^4, PTORD 8, tau_g 0.005,
+    alpha -0.05, periodic, Wilson action, zero-mode subtraction and local
+    stochastic gauge fixing every step (the default build's NsptEvolve,
+    nspt.cc:953-1039, Jacobi here).  Steps/s of the whole step."""
+    import numpy as np
+    import torch
+
+    import prlgt2020_b200 as P
+    from prlgt2020_b200.replicas import max_over_ranks, replica_seed, whole_job_rate
+    torch.cuda.set_device(local)
+    L, N, dt, alpha = (12, 12, 12, 12), 8, 0.005, -0.05
+    eng = P.NsptEngine(L, N, zero_modes=True, local_gf=True, alpha=alpha)
+    eng.seed(replica_seed(8000, rank), 0)
+    eng.NsptEvolve(dt, args.warmup, 1)
+    eng.NsptEvolve(dt, args.steps, 1)
+    step_ms = max_over_ranks(eng.last_step_ms()) / args.steps
+    if rank == 0:
+        line = {
+            "metric": "Langevin steps/s, the reference's Quench.cfg run (12^4 x 8 orders, ZM + "
+                      "local gauge fixing every step)",
+            "value": whole_job_rate(1, world, step_ms * 1e-3), "unit": "steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (cold start + warm-up, device Philox noise)",
+            "config": {"workload": "qcfg_12^4_N8_zm_localgf", "L": list(L), "N": N, "dt": dt,
+                       "alpha": alpha, "bc": "periodic", "gf_every": 1},
+        }
+        print(json.dumps(line), flush=True)
+    eng.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -716,13 +748,14 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-gf", action="store_true", help="skip the gauge-fixing figure")
-    ap.add_argument("--workload", default="sweep", choices=["sweep", "c2", "c4", "c5", "imp", "loops"],
+    ap.add_argument("--workload", default="sweep", choices=["sweep", "c2", "c4", "c5", "imp", "loops", "qcfg"],
                     help="sweep: 32^4 x 24 twisted (the headline); c2: 16^4 x 20 periodic "
                          "with zero modes and FA gauge fixing every step, per pass; c4: 64 "
                          "replicas of 6^4..10^4 x 12, batched in one CUDA graph vs plain; "
                          "c5: 24^4 x 40 float-float products vs FP64, speed and per-order "
                          "error after 1/100/1000 steps; imp: 16^4 x 20 tree-level "
-                         "Symanzik sweep; loops: Wilson loops of a 16^4 x 20 field")
+                         "Symanzik sweep; loops: Wilson loops of a 16^4 x 20 field; qcfg: the "
+                         "reference's shipped Quench.cfg run, 12^4 x 8 with ZM and local GF")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -742,6 +775,9 @@ def main():
         return
     if args.workload == "loops":
         run_loops(args, world, rank, local)
+        return
+    if args.workload == "qcfg":
+        run_qcfg(args, world, rank, local)
         return
     run_ours(args, world, rank, local)
 

@@ -159,12 +159,19 @@ static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
 
 static int launch_sweep_imp(nspt_ctx *ctx, const SweepArgs &a) {
   const long nl = 4 * ctx->V;
-  KernelShape k = choose_shape(ctx, IMP_SLOTS, nl, 0);
+  const bool low = ctx->N <= 3 * MO_LOW;
+  KernelShape k = low ? choose_shape(ctx, IMP_SLOTS, nl, 0, SWEEP_THREADS_LOW / 32, 2)
+                      : choose_shape(ctx, IMP_SLOTS, nl, 0);
   const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, IMP_SLOTS, 0);
   const long per_cta = (long)k.warps * LPW;
   const unsigned grid = (unsigned)((nl + per_cta - 1) / per_cta);
-  cudaFuncSetAttribute(k_sweep_imp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_sweep_imp<<<grid, 32 * k.warps, smem, ctx->st>>>(a);
+  if (low) {
+    cudaFuncSetAttribute(k_sweep_imp<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_sweep_imp<true><<<grid, 32 * k.warps, smem, ctx->st>>>(a);
+  } else {
+    cudaFuncSetAttribute(k_sweep_imp<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_sweep_imp<false><<<grid, 32 * k.warps, smem, ctx->st>>>(a);
+  }
   CK(cudaGetLastError());
   return NSPT_OK;
 }
@@ -384,13 +391,17 @@ static int do_local_gf(nspt_ctx *ctx, double alpha) {
   const Geo geo = ctx->geo;
   cudaStream_t st = ctx->st;
   double2 *U = ctx->U, *Uf = ctx->Uf;
+  const bool low = N <= 3 * MO_LOW;
   for (long p = 0; p < steps; p++) {
     int rc = launch_groups(
-        ctx, (const void *)k_local_gf, 4, gr.nthr,
+        ctx, low ? (const void *)k_local_gf<true> : (const void *)k_local_gf<false>, 4, gr.nthr,
         [&](unsigned g, dim3 b, size_t sm) {
-          k_local_gf<<<g, b, sm, st>>>(U, Uf, N, SS, geo, alpha, gr, p);
+          if (low)
+            k_local_gf<true><<<g, b, sm, st>>>(U, Uf, N, SS, geo, alpha, gr, p);
+          else
+            k_local_gf<false><<<g, b, sm, st>>>(U, Uf, N, SS, geo, alpha, gr, p);
         },
-        "local gauge fixing");
+        "local gauge fixing", 0, low);
     if (rc) return rc;
   }
   return NSPT_OK;

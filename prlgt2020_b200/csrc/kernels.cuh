@@ -336,10 +336,11 @@ __device__ __noinline__ void slot_mul(double2 *T, const double2 *Y, int N, const
 
 // out <- A B, orders 1..N (out may be B: the product works in place); the
 // flag is the caller's
+template <int MOx = MO>
 __device__ __noinline__ void slot_mul_to(double2 *out, const double2 *A, const double2 *B, int N,
                                          const Lane &L) {
   const int c = L.c;
-  product<MO, false>(LeftS{A}, A[0], B, B[0], N, L,
+  product<MOx, false>(LeftS{A}, A[0], B, B[0], N, L,
                      [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
   __syncwarp(L.mask);
 }
@@ -518,7 +519,7 @@ __device__ __forceinline__ void imp_stage(const SweepArgs &a, double2 *slot, con
 }
 
 // Wacc (+)= l[0] l[1] ... l[n-1]; returns the flag of the chain
-template <int NL>
+template <int NL, int MOx = MO>
 __device__ __forceinline__ double2 imp_chain(const SweepArgs &a, double2 *T, double2 *Y,
                                              double2 *Wacc, const ImpLink (&l)[NL], bool first,
                                              const Lane &L) {
@@ -526,13 +527,16 @@ __device__ __forceinline__ double2 imp_chain(const SweepArgs &a, double2 *T, dou
 #pragma unroll
   for (int m = 1; m < NL - 1; m++) {
     imp_stage(a, Y, l[m], L);
-    slot_mul(T, Y, a.N, L);
+    slot_mul<MOx>(T, Y, a.N, L);
   }
   imp_stage(a, Y, l[NL - 1], L);
-  return slot_acc(Wacc, T, Y, first, a.N, L);
+  return slot_acc<MOx>(Wacc, T, Y, first, a.N, L);
 }
 
-__global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
+    k_sweep_imp(SweepArgs a) {
+  constexpr int MOK = LOW ? MO_LOW : MO;
   extern __shared__ double2 sm[];
   Lane L;
   int g;
@@ -588,48 +592,48 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
     {
       st(T, n, at(1, 0), false);
       st(Y, m, at(0, 1), true);
-      slot_mul(T, Y, N, L);
+      slot_mul<MOK>(T, Y, N, L);
       st(Y, n, site, true);
-      acc(slot_acc(W, T, Y, first, N, L));
+      acc(slot_acc<MOK>(W, T, Y, first, N, L));
       st(Y, m, at(-1, 1), true);
-      slot_mul(T, Y, N, L);
+      slot_mul<MOK>(T, Y, N, L);
       st(Y, n, at(-1, 0), true);
-      slot_mul(T, Y, N, L);
+      slot_mul<MOK>(T, Y, N, L);
       st(Y, m, at(-1, 0), false);
-      acc2(slot_acc(W2, T, Y, first2, N, L));
+      acc2(slot_acc<MOK>(W2, T, Y, first2, N, L));
     }
     {
       st(T, n, at(1, -1), true);
       st(Y, m, at(0, -1), true);
-      slot_mul(T, Y, N, L);
+      slot_mul<MOK>(T, Y, N, L);
       st(Y, n, at(0, -1), false);
-      acc(slot_acc(W, T, Y, first, N, L));
+      acc(slot_acc<MOK>(W, T, Y, first, N, L));
       st(Y, m, at(-1, -1), true);
-      slot_mul(T, Y, N, L);
+      slot_mul<MOK>(T, Y, N, L);
       st(Y, n, at(-1, -1), false);
-      slot_mul(T, Y, N, L);
+      slot_mul<MOK>(T, Y, N, L);
       st(Y, m, at(-1, 0), false);
-      acc2(slot_acc(W2, T, Y, first2, N, L));
+      acc2(slot_acc<MOK>(W2, T, Y, first2, N, L));
     }
     // ---- the other four rectangles of staple2x1, each its chain of five links
     {
       // U_nu(a) U_nu(b) dag(U_nu(x) U_nu(c) U_mu(d)),  a=x+mu b=x+mu+nu c=x+nu d=x+2nu
       const ImpLink r1[5] = {{n, at(1, 0), false}, {n, at(1, 1), false}, {m, at(0, 2), true},
                              {n, at(0, 1), true}, {n, site, true}};
-      acc2(imp_chain(a, T, Y, W2, r1, first2, L));
+      acc2(imp_chain<5, MOK>(a, T, Y, W2, r1, first2, L));
       // U_mu(a) U_nu(e) dag(U_nu(x) U_mu(c) U_mu(b)),  e=x+2mu
       const ImpLink r2[5] = {{m, at(1, 0), false}, {n, at(2, 0), false}, {m, at(1, 1), true},
                              {m, at(0, 1), true}, {n, site, true}};
-      acc2(imp_chain(a, T, Y, W2, r2, first2, L));
+      acc2(imp_chain<5, MOK>(a, T, Y, W2, r2, first2, L));
       // dag(U_mu(d) U_nu(e) U_nu(b)) U_nu(d) U_nu(c),
       // b=x+mu-nu c=x-nu d=x-2nu e=x+mu-2nu
       const ImpLink r4[5] = {{n, at(1, -1), true}, {n, at(1, -2), true}, {m, at(0, -2), true},
                              {n, at(0, -2), false}, {n, at(0, -1), false}};
-      acc2(imp_chain(a, T, Y, W2, r4, first2, L));
+      acc2(imp_chain<5, MOK>(a, T, Y, W2, r4, first2, L));
       // U_mu(a) dag(U_mu(c) U_mu(b) U_nu(f)) U_nu(c),  f=x+2mu-nu
       const ImpLink r5[5] = {{m, at(1, 0), false}, {n, at(2, -1), true}, {m, at(1, -1), true},
                              {m, at(0, -1), true}, {n, at(0, -1), false}};
-      acc2(imp_chain(a, T, Y, W2, r5, first2, L));
+      acc2(imp_chain<5, MOK>(a, T, Y, W2, r5, first2, L));
     }
   }
   if (L.j == 0) {
@@ -644,8 +648,8 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
   self.fwd = self.bwd = 0;
   stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
   const double2 pflag = flag_mul(Y[0], wflag), p2flag = flag_mul(Y[0], w2flag);
-  slot_mul_to(T, Y, W, N, L);
-  slot_mul_to(W2, Y, W2, N, L);
+  slot_mul_to<MOK>(T, Y, W, N, L);
+  slot_mul_to<MOK>(W2, Y, W2, N, L);
   if (L.j == 0) {
     T[0] = pflag;
     W2[0] = p2flag;
@@ -683,7 +687,7 @@ __global__ void __launch_bounds__(256, 1) k_sweep_imp(SweepArgs a) {
   for (int e = L.j; e < 1 + 9 * N; e += GROUP)
     T[e] = cadd(cscale(T[e], a.c0), cscale(W2[e], a.c1));
   __syncwarp(L.mask);
-  update_link(a, T, Y, W, link, mu, site, self, L);
+  update_link<MOK>(a, T, Y, W, link, mu, site, self, L);
 }
 
 // Advance a device step counter by one (a kernel, so that it replays
@@ -879,7 +883,8 @@ __device__ __forceinline__ void ser_aherm_trless(double2 *P, int N, const Lane &
 // U_mu(x) <- exp(alpha W) U_mu(x), U_mu(x-mu) <- U_mu(x-mu) exp(-alpha W)
 // (twist_mu(exp(-alpha W)) = Omega W2 Omega^dag when x-mu wraps a twisted
 // face, nspt.cc:690-719).  Four slots per group.
-__global__ void __launch_bounds__(256, 1)
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
     k_local_gf(double2 *U, double2 *Uf, int N, int SS, Geo geo, double alpha, LgfGrid gr,
                long step) {
   extern __shared__ double2 sm[];
@@ -933,10 +938,10 @@ __global__ void __launch_bounds__(256, 1)
     for (int e = L.j; e < 1 + 9 * N; e += GROUP) A[e] = cscale(A[e], alpha);
     __syncwarp(L.mask);
     // E1 = exp(alpha W), E2 = exp(-alpha W), sharing (alpha W)^2
-    ser_square<MO>(A, Y2, N, L);
-    ser_horner2<MO>(A, Y2, E1, N, L, [](int n) { return inv_factorial(n); },
+    ser_square<(LOW ? MO_LOW : MO)>(A, Y2, N, L);
+    ser_horner2<(LOW ? MO_LOW : MO)>(A, Y2, E1, N, L, [](int n) { return inv_factorial(n); },
                     [&](int k, int rr, double2 v) { E1[sidx(k, rr, c)] = v; });
-    ser_horner2<MO>(A, Y2, E2, N, L,
+    ser_horner2<(LOW ? MO_LOW : MO)>(A, Y2, E2, N, L,
                     [](int n) { return (n & 1) ? -inv_factorial(n) : inv_factorial(n); },
                     [&](int k, int rr, double2 v) { E2[sidx(k, rr, c)] = v; });
     if (L.j == 0) E1[0] = E2[0] = one;
@@ -947,7 +952,7 @@ __global__ void __launch_bounds__(256, 1)
       {
         double2 *dst = U + mu * plane + self.site;
         const double2 yf = Y2[0];
-        product<MO, false>(LeftS{E1}, one, Y2, yf, N, L, [&](int k, int rr, double2 v) {
+        product<(LOW ? MO_LOW : MO), false>(LeftS{E1}, one, Y2, yf, N, L, [&](int k, int rr, double2 v) {
           dst[(size_t)(9 * (k - 1) + 3 * rr + c) * V] = v;
         });
         if (L.j == 0) Uf[(size_t)mu * V + self.site] = flag_mul(one, yf);
@@ -981,7 +986,7 @@ __global__ void __launch_bounds__(256, 1)
       {
         double2 *dst = U + mu * plane + back.site;
         const double2 af = A[0], rf = R[0];
-        product<MO, false>(LeftS{A}, af, R, rf, N, L, [&](int k, int rr, double2 v) {
+        product<(LOW ? MO_LOW : MO), false>(LeftS{A}, af, R, rf, N, L, [&](int k, int rr, double2 v) {
           dst[(size_t)(9 * (k - 1) + 3 * rr + c) * V] = v;
         });
         if (L.j == 0) Uf[(size_t)mu * V + back.site] = flag_mul(af, rf);
