@@ -58,7 +58,8 @@ def check_obs(eo, oo, tol):
 
 @pytest.mark.parametrize("L,N", [((4, 4, 4, 4), 8), ((4, 4, 4, 4), 12), ((2, 4, 2, 4), 24),
                                  ((4, 2, 2, 2), 3), ((2, 2, 2, 2), 1), ((2, 4, 2, 4), 40),
-                                 ((2, 2, 4, 2), 48)])
+                                 ((2, 2, 4, 2), 48), ((4, 2, 4, 2), 13), ((2, 4, 4, 2), 16),
+                                 ((2, 2, 4, 4), 20)])
 def test_one_sweep_random_start(engine_mod, oracle_mod, L, N):
     e, o = make_pair(engine_mod, oracle_mod, L, N, start=1234 + N)
     rng = oracle_mod.Rand55(42)
