@@ -145,10 +145,14 @@ def host_cpu() -> dict:
     return {"model": model, "nproc": os.cpu_count()}
 
 
-def cpu_reference_sample(N: int, L_sample, steps: int, threads_cap: int | None = None):
-    """Time the reference's own code (oracle/_ref) on a bounded sample with the
-    largest OpenMP grid the sample and the host allow; returns (seconds per
-    sweep, threads, kind, sample description)."""
+def cpu_reference_sample(N: int, L_sample, sweeps: int, warmup: int = 1,
+                         threads_cap: int | None = None):
+    """Time the reference's own code (oracle/_ref) on a bounded sample: the
+    same plain Jacobi sweep the GPU arm times (gauge_wilson, Umu = Fmu,
+    twist_boundary; no gauge fixing), twisted y,z, with the largest OpenMP
+    grid the sample and the host allow.  `warmup` untimed sweeps, then
+    `sweeps` timed ones in the same process.  Returns (seconds of each timed
+    sweep, threads, kind, binary)."""
     from oracle import oracle as O
     ncpu = os.cpu_count() or 1
     if threads_cap:
@@ -167,19 +171,42 @@ def cpu_reference_sample(N: int, L_sample, steps: int, threads_cap: int | None =
             binary = None
     if binary and os.path.exists(binary):
         with tempfile.TemporaryDirectory() as d:
-            r = O.run_reference(binary, L_sample, steps, 0.005, 0.0, 1, d, noise=False,
-                                timing=True)
-        tok = r["stdout"].split()
-        spp = float(tok[tok.index("seconds_per_sweep") + 1])
-        return spp, best[0] * best[1] * best[2], "reference", binary
+            r = O.run_reference(binary, L_sample, warmup + sweeps, 0.005, 0.0, 1, d, noise=False,
+                                timing=True, sweep_only=True)
+        return r["step_seconds"][warmup:], best[0] * best[1] * best[2], "reference", binary
     # the reference binary cannot be built here: time the oracle port
     o = O.Oracle(L_sample, N, twist_mask=6)
     rng = O.Rand55(1)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        o.sweep(0.005, rng.gauss(o.V * 32))
-    spp = (time.perf_counter() - t0) / steps
-    return spp, ncpu, "port", "oracle/liboracle.so"
+    per = []
+    for s in range(warmup + sweeps):
+        nz = rng.gauss(o.V * 32)
+        t0 = time.perf_counter()
+        o.sweep(0.005, nz)
+        if s >= warmup:
+            per.append(time.perf_counter() - t0)
+    return per, 1, "port", "oracle/liboracle.so"
+
+
+# The CPU sample of the benchmark workload: the same 24-order twisted sweep on
+# 16^4 (1/16 of the 32^4 volume; the cost is exactly linear in V at fixed N).
+CPU_SAMPLE_L = (16, 16, 16, 16)
+
+
+def cpu_baseline_line(N: int, V: int, sweeps: int, warmup: int) -> dict:
+    """cpu_baseline of the workload: median, min and max over `sweeps` timed
+    16^4 sweeps (after `warmup`), scaled by V to the full lattice."""
+    per, threads, kind, _b = cpu_reference_sample(N, CPU_SAMPLE_L, sweeps, warmup)
+    Vs = 1
+    for x in CPU_SAMPLE_L:
+        Vs *= x
+    scale = V / Vs
+    med = statistics.median(per)
+    return {"value": 1.0 / (med * scale), "unit": "sweeps/s", "cores": threads, "kind": kind,
+            "min": 1.0 / (max(per) * scale), "max": 1.0 / (min(per) * scale),
+            "sample": "%d sweeps of 16^4 x %d orders (twisted y,z; gauge_wilson + Umu = Fmu + "
+                      "twist_boundary, the GPU arm's timed work) after %d untimed, median "
+                      "scaled by V to 32^4" % (len(per), N, warmup),
+            "seconds_per_sample_sweep": per}
 
 
 def run_reference_arm(args, world, rank):
@@ -189,28 +216,21 @@ def run_reference_arm(args, world, rank):
         V *= x
     if rank != 0:
         return
-    L_sample = (8, 8, 8, 8)
-    Vs = 8 ** 4
-    per = []
-    kind = threads = None
-    for _ in range(args.steps):
-        spp, threads, kind, _b = cpu_reference_sample(args.N, L_sample, 1)
-        per.append(spp)
-    spp = statistics.median(per)
-    spp_full = spp * V / Vs  # cost is exactly linear in V at fixed N
-    value = 1.0 / spp_full
+    sweeps = max(3, min(args.steps, 8))
+    cpu = cpu_baseline_line(args.N, V, sweeps, min(args.warmup, 1))
+    value = cpu["value"]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "sweeps/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": spp_full * 1e3, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (cold start)",
         "config": {"workload": "sweep_32^4_N24_twisted_yz", "L": list(L), "N": args.N,
-                   "dt": 0.005, "bc": "twisted y,z", "update": "Jacobi"},
-        "cpu_baseline": {"value": value, "unit": "sweeps/s", "cores": threads, "kind": kind,
-                         "sample": "%d sweep(s) of 8^4 x %d orders per step, scaled by V to 32^4"
-                                   % (1, args.N)},
+                   "dt": 0.005, "bc": "twisted y,z", "update": "Jacobi",
+                   "gauge_fixing": "none in the timed sweep"},
+        "cpu_baseline": cpu,
         "e2e": {"value": value, "unit": "sweeps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "host": host_cpu(),
     }
     print(json.dumps(line), flush=True)
 
@@ -319,15 +339,12 @@ def run_ours(args, world, rank, local):
         e2e = e2e_leg(args, eng, lib, _lib, P, N, V, world, field_bytes)
     cpu = None
     if rank == 0 and not args.no_cpu:
-        spp, threads, kind, _b = cpu_reference_sample(N, (8, 8, 8, 8), 1)
-        spp1, _t1, kind1, _b1 = cpu_reference_sample(N, (4, 4, 4, 4), 1, threads_cap=1)
-        cpu = {"value": 1.0 / (spp * V / 8 ** 4), "unit": "sweeps/s", "cores": threads,
-               "kind": kind,
-               "sample": "1 sweep of 8^4 x %d orders (twisted y,z), scaled by V to 32^4" % N,
-               "single_thread": {"value": 1.0 / (spp1 * V / 4 ** 4), "unit": "sweeps/s",
-                                 "cores": 1, "kind": kind1,
-                                 "sample": "1 sweep of 4^4 x %d orders, scaled by V to 32^4" % N},
-               "host": host_cpu()}
+        cpu = cpu_baseline_line(N, V, 3, 1)
+        per1, _t1, kind1, _b1 = cpu_reference_sample(N, (4, 4, 4, 4), 1, 0, threads_cap=1)
+        cpu["single_thread"] = {"value": 1.0 / (per1[0] * V / 4 ** 4), "unit": "sweeps/s",
+                                "cores": 1, "kind": kind1,
+                                "sample": "1 sweep of 4^4 x %d orders, scaled by V to 32^4" % N}
+        cpu["host"] = host_cpu()
 
     if rank == 0:
         line = {

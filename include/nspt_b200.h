@@ -250,7 +250,10 @@ int nspt_batch_tune(nspt_batch *b, int gf_every, int *warps_out);
  * Scratch: a fixed static device array of 803,600 bytes (1024 partial rows
  * plus one result row of NSPT_MAX_ORDER + 1 complex doubles).  Its address
  * is looked up once per device on the first call, with that device
- * current; make that first call before any stream capture.  No call relies
+ * current; make that first call before any stream capture.  That set-up
+ * (the address, and the twist matrices it uploads) is kept for the life of
+ * the process: a cudaDeviceReset of that device after the first call is not
+ * supported, since the module reloads and the kept values go stale.  No call relies
  * on the array's earlier contents.  Calls that overlap on one device share
  * the array and race: serialise them.  N > NSPT_MAX_ORDER (more orders than
  * the scratch rows hold) returns NSPT_ERR_ORDER; N > allocORD, a bad flag,

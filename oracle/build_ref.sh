@@ -31,7 +31,7 @@
 # `-I-` makes the generated choices.h win over the one beside the reference's
 # sources for every `#include "choices.h"`.
 set -euo pipefail
-REF=${REF:-/root/reference}
+REF=${REF:-$(cd "$(dirname "$0")/../.." && pwd)/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
 N=${1:?N}; BC=${2:?BC}; GF=${3:?GF}; NTX=${4:-1}; NTY=${5:-1}; NTZ=${6:-1}; ACT=${7:-wil}
 UPD=${8:-jacobi}

@@ -198,6 +198,15 @@ def ser_op(name: str, N: int, *args: np.ndarray) -> np.ndarray:
 # The reference's own code (oracle/_ref, built by build_ref.sh)
 # ---------------------------------------------------------------------------
 
+def reference_dir() -> str:
+    """The reference's source tree: $PRLGT_REFERENCE, else $REF, else a
+    directory named `reference` beside the repository."""
+    for var in ("PRLGT_REFERENCE", "REF"):
+        if os.environ.get(var):
+            return os.environ[var]
+    return os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
+
+
 def ref_binary(N: int, bc: str = "pbc", gf: str = "local", grid=(1, 1, 1),
                action: str = "wil", update: str = "jacobi") -> str:
     name = "ref_N%d_%s_%s_t%d%d%d" % ((N, bc, gf) + tuple(grid))
@@ -214,7 +223,7 @@ def build_reference(N: int, bc: str = "pbc", gf: str = "local", grid=(1, 1, 1),
     (the reference's default on-the-fly update, choices.h:61)."""
     subprocess.run([os.path.join(HERE, "build_ref.sh"), str(N), bc, gf] +
                    [str(g) for g in grid] + [action, update], check=True,
-                   stdout=subprocess.DEVNULL)
+                   stdout=subprocess.DEVNULL, env=dict(os.environ, REF=reference_dir()))
     return ref_binary(N, bc, gf, grid, action, update)
 
 
@@ -235,7 +244,7 @@ def write_config(path: str, links: np.ndarray, plaq: np.ndarray):
 def run_reference(binary: str, L, steps: int, dt: float, alpha: float, seed: int,
                   workdir: str, start: str = "cold", noise: bool = True,
                   twist_init: bool = False, project: bool = False, timing: bool = False,
-                  wl2x2: bool = False):
+                  wl2x2: bool = False, sweep_only: bool = False):
     """Run the reference harness; returns dict of parsed outputs."""
     out = os.path.join(workdir, "ref")
     cmd = [binary, "--L", *[str(x) for x in L], "--steps", str(steps), "--dt", repr(dt),
@@ -248,11 +257,16 @@ def run_reference(binary: str, L, steps: int, dt: float, alpha: float, seed: int
         cmd.append("--project")
     if timing:
         cmd.append("--time")
+    if sweep_only:
+        cmd.append("--sweep-only")
     if wl2x2:
         cmd += ["--wl2x2", out + ".wl2x2"]
     p = subprocess.run(cmd, check=True, capture_output=True, text=True)
     V = int(np.prod(L))
     res = {"stdout": p.stdout}
+    for ln in p.stdout.splitlines():
+        if ln.startswith("step_seconds"):
+            res["step_seconds"] = [float(x) for x in ln.split()[1:]]
     N = None
     raw = np.loadtxt(out + ".plaq")
     if raw.ndim == 2 and raw.shape[1] == 4:  # improved action: w1 and w2 (nspt.cc:586-597)

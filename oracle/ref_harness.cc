@@ -30,12 +30,19 @@
  *   --project      apply the reference's unitarisation U = exp(reH(log U))
  *                  (QCDenvNODEpt_test.h:414-417) to every link of a file start
  *                  before the run;
- *   --time         print the wall time of the NsptEvolve calls.
+ *   --time         print the wall time of the NsptEvolve calls, and each
+ *                  step's own time;
+ *   --sweep-only   each step is the Jacobi sweep part of NsptEvolve alone:
+ *                  the per-step observables zeroed (nspt.cc:965-980),
+ *                  gauge_wilson(Umu, Fmu), Umu = Fmu and, with twisted
+ *                  boundaries, twist_boundary(Umu) (nspt.cc:989-995) -- no
+ *                  zero modes and no gauge fixing.  This is the CPU side of
+ *                  the benchmark's timed sweep.
  *
  * Usage:
  *   ref_harness --L l0 l1 l2 l3 --steps S --dt DT --alpha A --seed SEED
  *               --start cold|FILE --out PREFIX [--noise FILE] [--twist-init]
- *               [--project] [--time]
+ *               [--project] [--time] [--sweep-only]
  */
 #include "nspt.h"
 
@@ -44,6 +51,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 
 #include <fftw3.h>
 
@@ -75,7 +83,7 @@ static void usage() {
   fprintf(stderr,
           "ref_harness --L l0 l1 l2 l3 --steps S --dt DT --alpha A --seed S "
           "--start cold|FILE --out PREFIX [--noise FILE] [--twist-init] "
-          "[--project] [--time] [--loops FILE] [--wl2x2 FILE]\n");
+          "[--project] [--time] [--sweep-only] [--loops FILE] [--wl2x2 FILE]\n");
   exit(2);
 }
 
@@ -85,7 +93,7 @@ int main(int argc, char **argv) {
   double dt = 0.01, alpha = 0.0;
   long seed = 12345;
   std::string start = "cold", out = "ref", noise_path, loops_path, wl2x2_path;
-  bool twist_init = false, project = false, timing = false;
+  bool twist_init = false, project = false, timing = false, sweep_only = false;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
     if (a == "--L" && i + 4 < argc) {
@@ -110,6 +118,8 @@ int main(int argc, char **argv) {
       project = true;
     } else if (a == "--time") {
       timing = true;
+    } else if (a == "--sweep-only") {
+      sweep_only = true;
     } else if (a == "--loops" && i + 1 < argc) {
       loops_path = argv[++i];
     } else if (a == "--wl2x2" && i + 1 < argc) {
@@ -269,6 +279,7 @@ int main(int argc, char **argv) {
   }
 
   double secs = 0.0;
+  std::vector<double> step_secs;
   for (int s = 0; s < steps; s++) {
     if (fnoise) {
       /* same draws, same order as gauge_wilson with one thread */
@@ -282,10 +293,27 @@ int main(int argc, char **argv) {
 #ifdef UPDATE_ONTHEFLY
     NsptEvolve(Umu);
 #else
-    NsptEvolve(Umu, Fmu);
+    if (sweep_only) {
+      /* the sweep part of NsptEvolve, nspt.cc:965-995 */
+      for (int i1 = 0; i1 < PTORD; i1++) {
+        w1[i1] = 0.0;
+        norm[i1] = 0.0;
+        for (int mu = 0; mu < dim; mu++) trU[mu][i1] = 0.0;
+      }
+      w1[PTORD] = 0.0;
+      gauge_wilson(Umu, Fmu);
+      Umu = Fmu;
+#ifdef TWISTED_BC
+      twist_boundary(Umu);
+#endif
+    } else {
+      NsptEvolve(Umu, Fmu);
+    }
 #endif
     auto t1 = std::chrono::steady_clock::now();
-    secs += std::chrono::duration<double>(t1 - t0).count();
+    const double dts = std::chrono::duration<double>(t1 - t0).count();
+    step_secs.push_back(dts);
+    secs += dts;
   }
   if (fnoise) fclose(fnoise);
 
@@ -301,9 +329,13 @@ int main(int argc, char **argv) {
   std::vector<char> name(conf.begin(), conf.end());
   name.push_back('\0');
   Umu.save(name.data(), w);
-  if (timing)
+  if (timing) {
     printf("steps %d seconds %.6f seconds_per_sweep %.6f threads %d\n", steps,
            secs, secs / (steps > 0 ? steps : 1), NTHR);
+    printf("step_seconds");
+    for (double t : step_secs) printf(" %.6f", t);
+    printf("\n");
+  }
   plaqfile.close();
   normfile.close();
   trufile.close();

@@ -12,7 +12,10 @@
 // was captured with; and the gauge fixing schedule (every gf_every steps)
 // repeats with the graph's length.  A replica stepped on its own in between
 // (an odd number of steps) changes its pointers; the next batch step sees
-// that and captures again.
+// that and captures again.  The captured kernels also hold values taken by
+// argument (the noise seed, the gauge-fixing grid, the float-float scale
+// mode): a replica context whose setters ran since the capture (its
+// launch_gen moved) is stale too, and the graph is captured again.
 #pragma once
 
 #include <vector>
@@ -29,6 +32,7 @@ struct nspt_batch {
   int graph_steps = 0, graph_gf_every = -1;
   std::vector<const void *> graph_U;
   std::vector<uint64_t> graph_phase;
+  std::vector<uint64_t> graph_gen;
   float last_ms = 0.f;
   int warps = 0;
 };
@@ -65,6 +69,7 @@ bool graph_current(const nspt_batch *b, int P, int gf_every) {
   for (int r = 0; r < b->nrep; r++) {
     if (b->graph_U[r] != b->ctx[r]->U) return false;
     if (b->graph_phase[r] != b->ctx[r]->counter % (uint64_t)P) return false;
+    if (b->graph_gen[r] != b->ctx[r]->launch_gen) return false;
   }
   return true;
 }
@@ -110,6 +115,7 @@ int capture(nspt_batch *b, int P, int gf_every) {
   for (int r = 0; r < b->nrep; r++) {
     b->graph_U[r] = b->ctx[r]->U;
     b->graph_phase[r] = counter[r] % (uint64_t)P;
+    b->graph_gen[r] = b->ctx[r]->launch_gen;
   }
   return NSPT_OK;
 }
@@ -145,6 +151,7 @@ extern "C" int nspt_batch_create(int nrep, const int *L, int N, unsigned flags, 
   b->join.assign(nrep, nullptr);
   b->graph_U.assign(nrep, nullptr);
   b->graph_phase.assign(nrep, 0);
+  b->graph_gen.assign(nrep, 0);
   for (int r = 0; r < nrep; r++) {
     b->dt.push_back(dt[r]);
     b->seed.push_back(seeds[r]);

@@ -70,6 +70,11 @@ struct nspt_ctx {
   bool noise_pending;
   bool have_obs;
   uint64_t seed, counter;
+  // bumped by every setter that changes what a step launches or the values
+  // its kernels take by argument (seed, gauge-fixing grid, sweep shape,
+  // float-float scale mode); a CUDA graph captured under another value is
+  // stale (batch.cuh)
+  uint64_t launch_gen;
   size_t bytes;
   std::string err;
 };
@@ -500,6 +505,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->p2 = nullptr;
   ctx->dcounter = nullptr;
   ctx->sweep_warps = 0;
+  ctx->launch_gen = 0;
   ctx->loop_part = nullptr;
   ctx->loop_part_n = 0;
   ctx->timeout_s = 0.0;
@@ -694,6 +700,7 @@ extern "C" int nspt_seed(nspt_ctx *ctx, uint64_t seed, uint64_t counter) {
   if (!ctx) return NSPT_ERR_ARG;
   ctx->seed = seed;
   ctx->counter = counter;
+  ctx->launch_gen++;
   const unsigned long long c = counter;
   CK(cudaMemcpyAsync(ctx->dcounter, &c, sizeof(c), cudaMemcpyHostToDevice, ctx->st));
   CK(cudaStreamSynchronize(ctx->st));
@@ -868,6 +875,7 @@ extern "C" int nspt_local_gauge_fixing(nspt_ctx *ctx, double alpha) {
 extern "C" int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]) {
   if (!ctx || !grid || !grid_ok(ctx->L, grid)) return NSPT_ERR_ARG;
   for (int d = 0; d < 4; d++) ctx->gf_grid[d] = grid[d];
+  ctx->launch_gen++;
   return NSPT_OK;
 }
 
@@ -935,6 +943,7 @@ extern "C" int nspt_set_ff_scale(nspt_ctx *ctx, int automatic, int e) {
     ctx->err = "float-float scale: context created without NSPT_PRECISION_FF";
     return NSPT_ERR_STATE;
   }
+  ctx->launch_gen++;
   if (automatic) {
     ctx->ff_auto = true;
     return NSPT_OK;

@@ -195,7 +195,10 @@ __global__ void k_plaq_noalloc_sum(const double2 *partial, int nblocks, int N, d
 namespace {
 
 // Per-device set-up, done once with that device current: the scratch
-// array's address, the launch limits and the twist matrices.
+// array's address, the launch limits and the twist matrices.  It is kept
+// until the process exits; a cudaDeviceReset after the first call reloads
+// the module and leaves these values stale, which the header documents as
+// unsupported.
 struct NoallocDevice {
   bool ready;
   double2 *scratch;

@@ -17,11 +17,30 @@ def world_info():
             int(os.environ.get("LOCAL_RANK", "0")))
 
 
+_MASK64 = (1 << 64) - 1
+
+
+def _splitmix64(x: int) -> int:
+    """SplitMix64 finaliser (Steele, Lea and Flood, OOPSLA 2014): a
+    bijection of 64-bit integers that spreads nearby inputs far apart."""
+    x = (x + 0x9E3779B97F4A7C15) & _MASK64
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & _MASK64
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & _MASK64
+    return x ^ (x >> 31)
+
+
 def replica_seed(base: int, rank: int) -> int:
-    """Noise seed of replica `rank`: distinct per rank, reproducible."""
+    """Noise seed of replica `rank`: the base itself on rank 0 (a one-GPU run
+    keeps its plain seed), otherwise a 64-bit hash of (base, rank).  For one
+    base the ranks' seeds are distinct (the hash is a bijection in its
+    argument, and that argument differs per rank), and jobs with nearby bases
+    do not share a stream, as base + c * rank would for bases c apart."""
     if rank < 0:
         raise ValueError("rank must be >= 0")
-    return int(base) + 1000003 * int(rank)
+    base = int(base) & _MASK64
+    if rank == 0:
+        return base
+    return _splitmix64(_splitmix64(base) ^ int(rank))
 
 
 def _device():

@@ -11,7 +11,10 @@ the reference's binary format and loaded by the reference harness; the
 reference's plaquette of that start is stored too, so the fixture pins the
 start as well.
 
-    python tests/golden/make_golden.py          # needs /root/reference
+    python tests/golden/make_golden.py [NAME ...]   # needs the reference's sources
+
+The reference's location comes from PRLGT_REFERENCE (or REF); with names,
+only those fixtures are written.
 """
 from __future__ import annotations
 
@@ -41,6 +44,12 @@ CASES = [
          dt=0.01, alpha=-0.05, seed=8, start=3, zm=True),
     dict(name="rand_pbc_tlsym_n4", L=(4, 4, 4, 4), N=4, bc="pbc", gf="local", steps=2,
          dt=0.01, alpha=0.0, seed=19, start=13, zm=True, action="tlsym"),
+    # the benchmark's combination: 24 orders, twisted y,z, dt = 0.005
+    dict(name="rand_tw_yz_n24", L=(4, 4, 4, 4), N=24, bc="tw", gf="local", steps=2,
+         dt=0.005, alpha=0.0, seed=2424, start=24, zm=False),
+    # the 16^4 x 20 workload's step: 20 orders, zero modes + FA every step
+    dict(name="rand_pbc_zm_fa_n20", L=(4, 4, 4, 4), N=20, bc="pbc", gf="fa", steps=2,
+         dt=0.01, alpha=0.05, seed=2020, start=20, zm=True),
 ]
 C1 = {"wil": 0.0, "tlsym": -1.0 / 12.0, "iwa": -0.331, "dbw2": -1.4088}
 
@@ -75,7 +84,10 @@ def make_case(c: dict) -> dict:
 
 def main():
     meta = []
+    only = set(sys.argv[1:])
     for c in CASES:
+        if only and c["name"] not in only:
+            continue
         res = make_case(c)
         path = os.path.join(OUT, c["name"] + ".npz")
         np.savez_compressed(path, **res, L=np.array(c["L"]), N=c["N"], steps=c["steps"],

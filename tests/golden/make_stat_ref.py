@@ -9,7 +9,7 @@ start: THERM steps, then MEAS steps whose plaquette coefficients
 (nspt.cc:570-597) are averaged per replica.  Only the per-replica averages
 are stored, so the fixture is small.
 
-    python tests/golden/make_stat_ref.py        # needs /root/reference, ~4 min on 16 cores
+    python tests/golden/make_stat_ref.py   # needs the reference sources (PRLGT_REFERENCE), ~4 min on 16 cores
 """
 from __future__ import annotations
 

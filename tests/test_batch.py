@@ -75,3 +75,24 @@ def test_batch_tune_restores_the_start(engine_mod):
         b.step(2, 1)
         for r, (links, _) in enumerate(want):
             assert np.array_equal(b.replicas[r].download(), links), r
+
+
+def test_batch_captures_again_after_a_replica_is_reseeded(engine_mod):
+    """A replica reseeded between two batch steps, at the same phase of the
+    two-step graph, gets its new noise stream: the batch equals single
+    contexts seeded alike (the captured sweep holds the seed by value)."""
+    P = engine_mod
+    N, kw = 5, dict(zero_modes=True, fa=True, alpha=-0.05)
+    with P.NsptBatch(CASES["L"], N, CASES["dt"], CASES["seeds"], **kw) as b:
+        b.step(2, 1)
+        b.replicas[1].seed(999, 2)
+        b.step(2, 1)
+        got = [e.download() for e in b.replicas]
+    for r, (L, dt, sd) in enumerate(zip(CASES["L"], CASES["dt"], CASES["seeds"])):
+        with P.NsptEngine(L, N, **kw) as e:
+            e.seed(sd, 0)
+            e.NsptEvolve(dt, 2, 1)
+            if r == 1:
+                e.seed(999, 2)
+            e.NsptEvolve(dt, 2, 1)
+            assert np.array_equal(got[r], e.download()), r

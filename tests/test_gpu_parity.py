@@ -133,6 +133,69 @@ def test_twisted_boundaries(engine_mod, oracle_mod, twist, N):
     assert per_order_rel(e.download(), o.links, N).max() <= 1e-11
 
 
+@pytest.mark.parametrize("L", [(4, 4, 4, 4), (8, 8, 4, 4)])
+def test_headline_combination_one_sweep(engine_mod, oracle_mod, L):
+    """The benchmark's combination -- 24 orders, twisted y and z, dt = 0.005 --
+    on lattices with every extent >= 4 (so x + mu and x - mu are distinct
+    sites) and, at 8 x 8 x 4 x 4, extents above 4 in a twisted direction.
+    One sweep from a random start: <= 1e-12 per order, flags exact
+    (gauge_wilson nspt.cc:362-439, twist nspt.cc:163-255)."""
+    N = 24
+    e, o = make_pair(engine_mod, oracle_mod, L, N, twist="yz", start=2400 + L[0])
+    rng = oracle_mod.Rand55(2424)
+    eo, oo = step_both(e, o, 0.005, rng)
+    got = e.download()
+    rel = per_order_rel(got, o.links, N)
+    assert rel.max() <= 1e-12, rel
+    assert flag_diff(got, o.links, N) == 0.0
+    check_obs(eo, oo, 1e-12)
+
+
+def test_headline_combination_100_steps(engine_mod, oracle_mod):
+    """100 sweeps of the benchmark's combination (24 orders, twisted y,z,
+    dt = 0.005) from a random start on 4^4: <= 1e-9 per order at the end,
+    observables within 1e-9 at every step."""
+    L, N = (4, 4, 4, 4), 24
+    e, o = make_pair(engine_mod, oracle_mod, L, N, twist="yz", start=2401)
+    rng = oracle_mod.Rand55(99)
+    for s in range(100):
+        eo, oo = step_both(e, o, 0.005, rng)
+        check_obs(eo, oo, 1e-9)
+        if s == 0:
+            assert per_order_rel(e.download(), o.links, N).max() <= 1e-12
+    rel = per_order_rel(e.download(), o.links, N)
+    assert rel.max() <= 1e-9, rel
+
+
+@pytest.mark.parametrize("L", [(4, 4, 4, 4), (8, 4, 4, 4)])
+def test_c2_combination_zero_modes_and_fa(engine_mod, oracle_mod, L):
+    """The 16^4 x 20 workload's step at a size the oracle runs in seconds:
+    20 orders, random start, sweep + zero modes + FA gauge fixing every
+    step (nspt.cc:605-654, 866-948).  One step <= 1e-12 per order."""
+    N, alpha = 20, 0.05
+    e, o = make_pair(engine_mod, oracle_mod, L, N, zm=True, fa=True, alpha=alpha, start=2000 + L[0])
+    rng = oracle_mod.Rand55(2020)
+    eo, oo = step_both(e, o, 0.01, rng, zm=True, fa=True, alpha=alpha)
+    check_obs(eo, oo, 1e-12)
+    got = e.download()
+    rel = per_order_rel(got, o.links, N)
+    assert rel.max() <= 1e-12, rel
+    assert flag_diff(got, o.links, N) == 0.0
+
+
+def test_c2_combination_100_steps(engine_mod, oracle_mod):
+    """100 steps of sweep + zero modes + FA gauge fixing (alpha = +0.05, the
+    damping sign) from a random start, 20 orders on 4^4: <= 1e-9 per order."""
+    L, N, alpha = (4, 4, 4, 4), 20, 0.05
+    e, o = make_pair(engine_mod, oracle_mod, L, N, zm=True, fa=True, alpha=alpha, start=2002)
+    rng = oracle_mod.Rand55(7)
+    for s in range(100):
+        eo, oo = step_both(e, o, 0.01, rng, zm=True, fa=True, alpha=alpha)
+        check_obs(eo, oo, 1e-9)
+    rel = per_order_rel(e.download(), o.links, N)
+    assert rel.max() <= 1e-9, rel
+
+
 @pytest.mark.parametrize("path", sorted(glob.glob(os.path.join(GOLDEN, "*.npz"))),
                          ids=lambda p: os.path.basename(p)[:-4])
 def test_reference_golden_fixture(engine_mod, oracle_mod, path):

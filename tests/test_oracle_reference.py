@@ -9,14 +9,11 @@ import pytest
 
 from helpers import obs_close, per_order_rel
 
-REF = os.environ.get("PRLGT_REFERENCE", "/root/reference")
-
-
 def ref_binary(O, N, bc, gf):
     b = O.ref_binary(N, bc, gf)
     if os.path.exists(b):
         return b
-    if not os.path.exists(os.path.join(REF, "nspt.cc")):
+    if not os.path.exists(os.path.join(O.reference_dir(), "nspt.cc")):
         pytest.skip("reference sources not available")
     return O.build_reference(N, bc, gf)
 
@@ -68,7 +65,7 @@ def test_oracle_local_gauge_fixing_matches_reference_thread_grid(oracle_mod, cas
     N, grid, alpha, steps = case["N"], case["grid"], -0.08, 2
     b = O.ref_binary(N, case["bc"], "local", grid)
     if not os.path.exists(b):
-        if not os.path.exists(os.path.join(REF, "nspt.cc")):
+        if not os.path.exists(os.path.join(O.reference_dir(), "nspt.cc")):
             pytest.skip("reference sources not available")
         b = O.build_reference(N, case["bc"], "local", grid)
     tw = 6 if case["bc"] == "tw" else 0
@@ -98,7 +95,7 @@ def test_oracle_wilson_loops_match_reference(oracle_mod, L, N, start):
     b = O.ref_binary(N, "pbc", "local")
     if not os.path.exists(b) or os.path.getmtime(b) < os.path.getmtime(
             os.path.join(os.path.dirname(O.__file__), "ref_harness.cc")):
-        if not os.path.exists(os.path.join(REF, "nspt.cc")):
+        if not os.path.exists(os.path.join(O.reference_dir(), "nspt.cc")):
             pytest.skip("reference sources not available")
         b = O.build_reference(N, "pbc", "local")
     o = O.Oracle(L, N)
@@ -133,7 +130,7 @@ def test_oracle_improved_action_matches_reference(oracle_mod, action, c1):
     L, N, steps, dt = (4, 4, 4, 4), 4, 2, 0.01
     b = O.ref_binary(N, "pbc", "local", (1, 1, 1), action)
     if not os.path.exists(b):
-        if not os.path.exists(os.path.join(REF, "nspt.cc")):
+        if not os.path.exists(os.path.join(O.reference_dir(), "nspt.cc")):
             pytest.skip("reference sources not available")
         b = O.build_reference(N, "pbc", "local", (1, 1, 1), action)
     o = O.Oracle(L, N)

@@ -67,5 +67,18 @@ def test_single_process_fallbacks():
     assert R.max_over_ranks(3.5) == 3.5
     assert R.gather_series([1.0, 2.0]) == [[1.0, 2.0]]
     assert R.replica_seed(5, 0) == 5
+
+
+def test_replica_seeds_of_nearby_jobs_do_not_collide():
+    """Jobs whose base seeds are close (or c apart, for any small c) never
+    give two (base, rank) pairs the same noise seed."""
+    seen = {}
+    for base in range(1000, 1064):
+        for rank in range(16):
+            s = R.replica_seed(base, rank)
+            assert 0 <= s < 2 ** 64
+            assert s not in seen, (base, rank, seen.get(s))
+            seen[s] = (base, rank)
+    assert R.replica_seed(1000 + 1000003, 0) != R.replica_seed(1000, 1)
     with pytest.raises(ValueError):
         R.whole_job_rate(1.0, 1, 0.0)

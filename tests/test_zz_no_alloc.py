@@ -31,7 +31,10 @@ def _noalloc(lib, dev_ptr, A, L, N, flags):
 
 
 @pytest.mark.parametrize("twist,L,N,A", [("", (4, 4, 4, 6), 10, 10), ("yz", (4, 4, 4, 4), 7, 9),
-                                         ("t", (2, 4, 2, 4), 24, 24)])
+                                         ("t", (2, 4, 2, 4), 24, 24),
+                                         # 4V = 82944 links: more CTAs than the 1024 partial
+                                         # rows, so each CTA loops over many links
+                                         ("yz", (12, 12, 12, 12), 2, 3)])
 def test_noalloc_plaquette_matches_context_entry(engine_mod, oracle_mod, twist, L, N, A):
     import torch
     P, O = engine_mod, oracle_mod
@@ -72,6 +75,18 @@ def test_noalloc_rejects_what_its_scratch_or_arguments_cannot_hold(engine_mod):
     assert _noalloc(lib, p + 8, 5, L, 5, 0)[0] == P._lib.NSPT_ERR_ARG    # misaligned
     assert _noalloc(lib, 0, 5, L, 5, 0)[0] == P._lib.NSPT_ERR_ARG        # null field
     assert _noalloc(lib, p, 5, (2, 0, 2, 2), 5, 0)[0] == P._lib.NSPT_ERR_ARG
-    # a rejected call leaves the next good one intact
+    # a rejected call leaves the next good one intact: a random field gives
+    # what the context entry point gives (stale or unwritten scratch would not)
+    from oracle import oracle as O
+    o = O.Oracle(L, 5)
+    o.random_start(313, 0.5)
+    with P.NsptEngine(L, 5) as e:
+        e.upload(o.links)
+        want = e.plaquette_measure()
+    host = np.asarray(o.links).reshape(-1)
+    dev[: host.size] = torch.from_numpy(host).to("cuda")
+    torch.cuda.synchronize()
     rc, out = _noalloc(lib, p, 5, L, 5, 0)
-    assert rc == 0 and np.all(out == 0.0)
+    assert rc == 0
+    ok, worst = obs_close(out, want, 1e-12)
+    assert ok, worst
