@@ -124,6 +124,12 @@ struct LeftS {
 #pragma unroll
     for (int r = 0; r < 3; r++) o[r] = DAG ? cconj(s[sidx(k, c, r)]) : s[sidx(k, r, c)];
   }
+  // row r of order k
+  template <bool DAG>
+  __device__ __forceinline__ void row(int k, int r, double2 *o) const {
+#pragma unroll
+    for (int l = 0; l < 3; l++) o[l] = DAG ? cconj(s[sidx(k, l, r)]) : s[sidx(k, r, l)];
+  }
 };
 
 // C = op(A) * B, orders 1..M (truncated Cauchy product, ptSU3::operator*,
@@ -193,6 +199,188 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
     }
     __syncwarp(L.mask);
   }
+}
+
+// ---------------- paired-run form of the same product ----------------
+//
+// For M = NR * R result orders with NR in {5, 6} (R set by the caller's
+// orders-per-lane budget), the triangle is cut into NR runs of R consecutive
+// orders, run r holding orders (r-1)R+1 .. rR.  Lane (c, s) of the group
+// owns column c of two runs: lo = s + 1 and hi = 6 - s (NR = 6), or lo = s
+// (none for s = 0) and hi = 5 - s (NR = 5).  A run ending at order b takes
+// b - 1 steps (left orders i = 1 .. b-1; the lo run is padded to a whole
+// number of R-step blocks), so a lane's two runs take (NR + 1) R - 1 or
+// NR R - 1 steps whatever s is: every lane walks the same number of steps
+// and the same straight-line code, without the per-order branches of
+// product().  A step is one left order i and all R orders of the run:
+// acc[q] += A_i w[q], 9 R complex FMAs per lane, where w holds the R right
+// columns B_{a+q-i}[:, c] in registers.  From one step to the next every
+// column moves up one order, so a step loads only one new column; the
+// window is circular (slot (q - u) mod R at step u of an R-step block), so
+// it needs no register moves.  Right columns below order 1 read as zero,
+// which pads a run's first R-1 steps and the lo run's last step with exact
+// zero terms; the hi run's last R-1 steps (common to all lanes) skip them.
+// The sum over i runs in the same (ascending) order as in product(), so
+// both forms give the same values.  Every lane finishes reading before any
+// writes, so the result may overwrite either operand.
+template <int R, bool DA, class Left>
+__device__ __forceinline__ void pr_step(const Left &A, int i, int u, int qlo,
+                                        double2 (&acc)[R][3], const double2 (&w)[R][3]) {
+#pragma unroll
+  for (int r = 0; r < 3; r++) {
+    double2 a[3];  // row r of op(A_i): one row at a time keeps registers low
+    A.template row<DA>(i, r, a);
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+      if (q < qlo) continue;
+      const int sl = (q - u + R) % R;
+      cfma(acc[q][r], a[0], w[sl][0]);
+      cfma(acc[q][r], a[1], w[sl][1]);
+      cfma(acc[q][r], a[2], w[sl][2]);
+    }
+  }
+}
+
+// column c of order j of a slot; zero below order 1
+__device__ __forceinline__ void pr_col(const double2 *B, int j, int c, double2 (&o)[3]) {
+  if (j >= 1) {
+    const double2 *bj = B + 1 + 9 * (j - 1) + 3 * c;
+    o[0] = bj[0];
+    o[1] = bj[1];
+    o[2] = bj[2];
+  } else {
+    o[0] = o[1] = o[2] = cz();
+  }
+}
+
+__device__ __forceinline__ bool pr_fits(int R, int M) {
+  return R > 0 && (M == 5 * R || M == 6 * R);
+}
+
+// Run length of the paired-run form for a kernel built for MO orders per
+// lane and pass (0: not used).
+template <int MO>
+struct PrRun {
+  static constexpr int R = MO >= 8 ? 4 : (MO >= 4 ? 2 : 0);
+};
+
+// C = op(A) * B, orders 1..M, M = NR R with NR in {5, 6}: product()'s
+// result and interface (no i0: a zero left order adds exact zeros).
+template <int R, bool DA, class Left, class Emit>
+__device__ __forceinline__ void product_pr(const Left &A, double2 a0, const double2 *B, double2 b0,
+                                           int M, const Lane &L, Emit emit) {
+  const int c = L.c, s = L.s;
+  const int NR = M / R;
+  const int rlo = (NR == 6) ? s + 1 : s;  // 0: no lo run
+  const int rhi = NR - s;
+  const int alo = (rlo - 1) * R + 1;
+  const int ahi = (rhi - 1) * R + 1;
+  const int nblk = rlo + rhi - 1;  // R-step blocks; then the hi run's last R-1 steps
+  double2 acc[R][3], lo[R][3], w[R][3];
+#pragma unroll
+  for (int q = 0; q < R; q++)
+#pragma unroll
+    for (int r = 0; r < 3; r++) acc[q][r] = lo[q][r] = cz();
+  int a = rlo > 0 ? alo : ahi;
+#pragma unroll
+  for (int q = 1; q < R; q++) pr_col(B, a + q - 1, c, w[q]);
+  int i = 0;
+  for (int b = 0; b < nblk; b++) {
+    if (b == rlo) {  // the lo run (rlo blocks) is done: on to the hi run
+#pragma unroll
+      for (int q = 0; q < R; q++)
+#pragma unroll
+        for (int r = 0; r < 3; r++) {
+          lo[q][r] = acc[q][r];
+          acc[q][r] = cz();
+        }
+      a = ahi;
+      i = 0;
+#pragma unroll
+      for (int q = 1; q < R; q++) pr_col(B, a + q - 1, c, w[q]);
+    }
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      ++i;
+      pr_col(B, a - i, c, w[(R - u) % R]);
+      pr_step<R, DA>(A, i, u, 0, acc, w);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < R - 1; u++) {  // order q of the hi run is active while q > u
+    ++i;
+    pr_step<R, DA>(A, i, u, u + 1, acc, w);
+  }
+  __syncwarp(L.mask);
+  const bool fa = !cis0(a0), fb = !cis0(b0);
+  auto out = [&](int k, const double2(&v3)[3]) {
+    double2 ak[3];
+    if (fb) A.template col<DA>(k, c, ak);
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      double2 v = v3[r];
+      if (fa || fb) {
+        double2 t;
+        if (!fa)
+          t = cmul(b0, ak[r]);
+        else if (!fb)
+          t = cmul(a0, B[sidx(k, r, c)]);
+        else
+          t = cadd(cmul(b0, ak[r]), cmul(a0, B[sidx(k, r, c)]));
+        v = cadd(v, t);
+      }
+      emit(k, r, v);
+    }
+  };
+  if (rlo > 0) {
+#pragma unroll
+    for (int q = 0; q < R; q++) out(alo + q, lo[q]);
+  }
+#pragma unroll
+  for (int q = 0; q < R; q++) out(ahi + q, acc[q]);
+  __syncwarp(L.mask);
+}
+
+// product() or, where M fits, product_pr(): for the out-of-line slot
+// helpers, which hold one copy of each.
+template <int MO, bool DA, class Left, class Emit>
+__device__ __forceinline__ void product_any(const Left &A, double2 a0, const double2 *B, double2 b0,
+                                            int M, const Lane &L, Emit emit, int i0 = 1) {
+  constexpr int R = PrRun<MO>::R;
+#ifndef NSPT_NO_PAIRED_RUNS
+  if constexpr (R > 0) {
+    if (pr_fits(R, M)) {
+      product_pr<R, DA>(A, a0, B, b0, M, L, emit);
+      return;
+    }
+  }
+#endif
+  product<MO, DA>(A, a0, B, b0, M, L, emit, i0);
+}
+
+// out <- A B, orders 1..M, with a0 and b0 taken as the operands' flags
+// (out may be A or B: the products work in place); the result's flag is
+// the caller's
+template <int MO>
+__device__ __noinline__ void slot_mul_to(double2 *out, const double2 *A, double2 a0,
+                                         const double2 *B, double2 b0, int M, const Lane &L) {
+  const int c = L.c;
+  product_any<MO, false>(LeftS{A}, a0, B, b0, M, L,
+                         [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
+  __syncwarp(L.mask);
+}
+
+// One Horner step of ser_poly2: S <- Y S + cx X, orders 1..M, in place (Y
+// has flag 0 and no order 1; S's flag is sf).  The flag is the caller's.
+template <int MO>
+__device__ __noinline__ void slot_horner(double2 *S, const double2 *Y, double2 sf, const double2 *X,
+                                         double cx, int M, const Lane &L) {
+  const int c = L.c;
+  product_any<MO, false>(
+      LeftS{Y}, cz(), S, sf, M, L,
+      [&](int k, int r, double2 v) { S[sidx(k, r, c)] = cadd(v, cscale(X[sidx(k, r, c)], cx)); },
+      2);
+  __syncwarp(L.mask);
 }
 
 // ---------------- compensated float-float Cauchy product ----------------
@@ -334,20 +522,20 @@ __device__ __forceinline__ void cprod(const Left &A, double2 a0, const double2 *
 // with S_j needed only to order N - 2j (Y^j starts at order 2j).  X^n starts
 // at order n, so this is the same truncated sum as Horner in X, with
 // 1 + N/2 series products of sizes 2, 4, ..., N instead of N products of
-// sizes 1..N (1354 instead of 2300 3x3 products at N = 24).  The last step
-// goes to last(k, r, v) instead of S.  X, Y and S are slots.
+// sizes 1..N (1354 instead of 2300 3x3 products at N = 24).  The result
+// (S_0, flag coef(0)) is left in S.  X, Y and S are slots.
 template <int MO>
 __device__ __forceinline__ void ser_square(const double2 *X, double2 *Y, int N, const Lane &L) {
-  const int c = L.c;
-  // Y = X X (order 1 comes out as an exact zero)
-  product<MO, false>(LeftS{X}, cz(), X, cz(), N, L,
-                     [&](int k, int r, double2 v) { Y[sidx(k, r, c)] = v; });
+  // Y = X X (order 1 comes out as an exact zero); X's flag is not used (the
+  // log passes U, whose flag 1 is the X = U - 1 it leaves out)
+  slot_mul_to<MO>(Y, X, cz(), X, cz(), N, L);
 }
 
-// The Horner part of ser_poly2, for a Y = X^2 already formed.
-template <int MO, class Coef, class Last>
+// The Horner part of ser_poly2, for a Y = X^2 already formed: S <- p(X),
+// orders 1..N and flag coef(0).
+template <int MO, class Coef>
 __device__ __forceinline__ void ser_horner2(const double2 *X, const double2 *Y, double2 *S, int N,
-                                            const Lane &L, Coef coef, Last last) {
+                                            const Lane &L, Coef coef) {
   const int c = L.c;
   const int J = N / 2;
   // S_J = coef(2J) + coef(2J+1) X to order N - 2J; higher orders zero (they
@@ -362,40 +550,20 @@ __device__ __forceinline__ void ser_horner2(const double2 *X, const double2 *Y, 
     if (L.j == 0) S[0] = make_double2(coef(2 * J), 0.0);
     __syncwarp(L.mask);
   }
-  if (J == 0) {  // N = 1: S_0 is the result
-    for (int k = L.s + 1; k <= N; k += 3) {
-#pragma unroll
-      for (int r = 0; r < 3; r++) last(k, r, S[sidx(k, r, c)]);
-    }
-    __syncwarp(L.mask);
-    return;
-  }
   // Y = X^2 has no order 1 (X has flag 0): the products start at Y's order 2
-  const LeftS Yl{Y};
   for (int j = J - 1; j >= 0; --j) {
-    const int M = N - 2 * j;
     const double2 sf = S[0];
-    const double cx = coef(2 * j + 1);
-    if (j > 0) {
-      product<MO, false>(
-          Yl, cz(), S, sf, M, L,
-          [&](int k, int r, double2 v) { S[sidx(k, r, c)] = cadd(v, cscale(X[sidx(k, r, c)], cx)); },
-          2);
-      if (L.j == 0) S[0] = make_double2(coef(2 * j), 0.0);
-      __syncwarp(L.mask);
-    } else {
-      product<MO, false>(
-          Yl, cz(), S, sf, M, L,
-          [&](int k, int r, double2 v) { last(k, r, cadd(v, cscale(X[sidx(k, r, c)], cx))); }, 2);
-    }
+    slot_horner<MO>(S, Y, sf, X, coef(2 * j + 1), N - 2 * j, L);
+    if (L.j == 0) S[0] = make_double2(coef(2 * j), 0.0);
+    __syncwarp(L.mask);
   }
 }
 
-template <int MO, class Coef, class Last>
+template <int MO, class Coef>
 __device__ __forceinline__ void ser_poly2(const double2 *X, double2 *Y, double2 *S, int N,
-                                          const Lane &L, Coef coef, Last last) {
+                                          const Lane &L, Coef coef) {
   ser_square<MO>(X, Y, N, L);
-  ser_horner2<MO>(X, Y, S, N, L, coef, last);
+  ser_horner2<MO>(X, Y, S, N, L, coef);
 }
 
 __device__ __forceinline__ double inv_factorial(int n) {
@@ -409,21 +577,24 @@ __device__ __forceinline__ double inv_factorial(int n) {
 template <int MO>
 __device__ __forceinline__ void ser_exp(const double2 *P, double2 *Y, double2 *R, int N,
                                         const Lane &L) {
-  const int c = L.c;
-  ser_poly2<MO>(P, Y, R, N, L, [](int n) { return inv_factorial(n); },
-                [&](int k, int r, double2 v) { R[sidx(k, r, c)] = v; });
-  if (L.j == 0) R[0] = make_double2(1.0, 0.0);
-  __syncwarp(L.mask);
+  ser_poly2<MO>(P, Y, R, N, L, [](int n) { return inv_factorial(n); });
 }
 
 // log(U) for U with flag 1 (log(const ptSU3&), QCDpt.h:176-198): with
 // X = U - 1, sum_{n<=N} (-1)^{n+1} X^n / n, flag 0.  U, Y and Sc are slots
-// (Y, Sc scratch); emit(k, r, v) receives log_k[r][c].
+// (Y scratch); the result is left in Sc, and emit(k, r, v) receives
+// log_k[r][c] from it.
 template <int MO, class Emit>
 __device__ __forceinline__ void ser_log(const double2 *U, double2 *Y, double2 *Sc, int N,
                                         const Lane &L, Emit emit) {
   ser_poly2<MO>(U, Y, Sc, N, L,
-                [](int n) { return n == 0 ? 0.0 : ((n & 1) ? 1.0 : -1.0) / (double)n; }, emit);
+                [](int n) { return n == 0 ? 0.0 : ((n & 1) ? 1.0 : -1.0) / (double)n; });
+  const int c = L.c;
+  for (int k = L.s + 1; k <= N; k += 3) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) emit(k, r, Sc[sidx(k, r, c)]);
+  }
+  __syncwarp(L.mask);
 }
 
 // reH on a slot (ptSU3::reH, QCDpt.cc:197-209): per order (M - M^dag)/2
