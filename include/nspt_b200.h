@@ -182,6 +182,19 @@ int nspt_get_ff_scale(nspt_ctx *ctx, int *e);
 int nspt_save_config(nspt_ctx *ctx, const char *path, int allocORD);
 int nspt_load_config(nspt_ctx *ctx, const char *path, int allocORD,
                      double *plaq_trailer);
+/* loadlowerorder (ptGluon_fld::loadlowerorder, QCDenvNODEpt_test.h:376-426):
+ * start a run at N orders from a configuration file saved with loworder <=
+ * N orders (reference format: V*4 series of 1 + 9*loworder complex, then
+ * loworder + 1 complex plaquette values).  Orders 1..loworder come from the
+ * file, every order above is zero, and each link is then unitarised, U =
+ * exp(reH(log U)) with flag 1.  plaq_trailer (may be NULL) receives the
+ * file's (loworder + 1) * 2 plaquette doubles.  loworder outside 1..N:
+ * NSPT_ERR_ORDER; a missing file or a byte count that does not match:
+ * NSPT_ERR_IO.  (The reference's zeroing loop starts at ptU[loworder+1], so
+ * there order loworder + 1 keeps whatever the field held, zero after a cold
+ * start; here it is always zero.) */
+int nspt_load_lower_order(nspt_ctx *ctx, const char *path, int loworder,
+                          double *plaq_trailer);
 
 /* Device time of the last nspt_step, nspt_gauge_wilson,
  * nspt_zero_modes_subtraction, nspt_fa_gauge_fixing,

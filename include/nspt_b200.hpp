@@ -90,6 +90,12 @@ class ptGluon_fld {
     return nspt_load_config(ctx_, path, allocORD, &plaq_trailer[0].re);
   }
   int save(const char *path, int allocORD) { return nspt_save_config(ctx_, path, allocORD); }
+  /* ptGluon_fld::loadlowerorder (QCDenvNODEpt_test.h:376-426): a file with
+   * loworder <= N orders, upper orders zero, links unitarised;
+   * plaquette: loworder + 1 values */
+  int loadlowerorder(const char *path, int loworder, Cplx *plaquette) {
+    return nspt_load_lower_order(ctx_, path, loworder, plaquette ? &plaquette[0].re : nullptr);
+  }
 
   /* the field in the reference's AoS bytes: V x ptGluon<allocORD> */
   template <int allocORD>

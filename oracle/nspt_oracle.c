@@ -475,7 +475,13 @@ void oracle_random_start(oracle_ctx *c, long seed, double sigma) {
     }
   free(buf);
   oracle_rng_destroy(g);
-  /* unitarise: U = exp(reH(log U)), QCDenvNODEpt_test.h:414-417 */
+  oracle_unitarise(c);
+}
+
+/* U = exp(reH(log U)) for every link, the rule the reference applies to a
+   configuration loaded with fewer orders (QCDenvNODEpt_test.h:414-417) */
+void oracle_unitarise(oracle_ctx *c) {
+  int N = c->N;
   long nl = c->V * 4;
 #pragma omp parallel
   {

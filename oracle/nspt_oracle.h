@@ -33,6 +33,8 @@ long oracle_volume(oracle_ctx *c);
 void oracle_cold_start(oracle_ctx *c);
 /* order-k real components ~ N(0, sigma^k), then U = exp(reH(log U)) */
 void oracle_random_start(oracle_ctx *c, long seed, double sigma);
+/* U = exp(reH(log U)) per link (QCDenvNODEpt_test.h:414-417) */
+void oracle_unitarise(oracle_ctx *c);
 
 /* One Jacobi Langevin sweep (gauge_wilson, nspt.cc:258-600, Jacobi branch).
  * noise: V*4*8 Gaussians in the reference's draw order (site, mu, 8).

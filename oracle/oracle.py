@@ -45,6 +45,7 @@ def lib():
         L.oracle_volume.argtypes = [P]
         L.oracle_cold_start.argtypes = [P]
         L.oracle_random_start.argtypes = [P, ctypes.c_long, ctypes.c_double]
+        L.oracle_unitarise.argtypes = [P]
         L.oracle_sweep.argtypes = [P, ctypes.c_double, D, D, D, D, ctypes.c_int]
         L.oracle_zero_modes.argtypes = [P]
         L.oracle_fa_gauge_fix.argtypes = [P, ctypes.c_double]
@@ -139,6 +140,28 @@ class Oracle:
 
     def random_start(self, seed: int, sigma: float = 0.5):
         lib().oracle_random_start(self._h, int(seed), float(sigma))
+
+    def unitarise(self):
+        """U = exp(reH(log U)) per link (QCDenvNODEpt_test.h:414-417)."""
+        lib().oracle_unitarise(self._h)
+
+    def load_lower_order(self, path: str, loworder: int) -> np.ndarray:
+        """loadlowerorder (QCDenvNODEpt_test.h:376-426): a configuration
+        file holding `loworder` <= N orders fills orders 1..loworder, the
+        orders above are zero, and every link is unitarised.  Returns the
+        file's loworder + 1 plaquette values.  (The reference's zeroing loop
+        starts one order too high, at ptU[loworder+1]: order loworder + 1
+        keeps what the field held before the call, zero after a cold start,
+        which is what this restatement gives.)"""
+        lo = int(loworder)
+        if not 1 <= lo <= self.N:
+            raise ValueError("loworder must be in 1..N")
+        links, plaq = read_config(path, self.V, lo)
+        full = np.zeros(self.links.shape)
+        full[:, :, : series_len(lo)] = links
+        self.set_links(full)
+        self.unitarise()
+        return plaq
 
     def sweep(self, dt: float, noise: np.ndarray, zero_modes: bool = False) -> SweepObs:
         N = self.N
@@ -244,7 +267,7 @@ def write_config(path: str, links: np.ndarray, plaq: np.ndarray):
 def run_reference(binary: str, L, steps: int, dt: float, alpha: float, seed: int,
                   workdir: str, start: str = "cold", noise: bool = True,
                   twist_init: bool = False, project: bool = False, timing: bool = False,
-                  wl2x2: bool = False, sweep_only: bool = False):
+                  wl2x2: bool = False, sweep_only: bool = False, lower: int = 0):
     """Run the reference harness; returns dict of parsed outputs."""
     out = os.path.join(workdir, "ref")
     cmd = [binary, "--L", *[str(x) for x in L], "--steps", str(steps), "--dt", repr(dt),
@@ -259,6 +282,8 @@ def run_reference(binary: str, L, steps: int, dt: float, alpha: float, seed: int
         cmd.append("--time")
     if sweep_only:
         cmd.append("--sweep-only")
+    if lower:
+        cmd += ["--lower", str(lower)]
     if wl2x2:
         cmd += ["--wl2x2", out + ".wl2x2"]
     p = subprocess.run(cmd, check=True, capture_output=True, text=True)
@@ -267,6 +292,11 @@ def run_reference(binary: str, L, steps: int, dt: float, alpha: float, seed: int
     for ln in p.stdout.splitlines():
         if ln.startswith("step_seconds"):
             res["step_seconds"] = [float(x) for x in ln.split()[1:]]
+    if steps == 0:  # a load only: the start's plaquette and the saved field
+        p0 = np.loadtxt(out + ".plaq0").reshape(-1, 2)
+        res["plaq0"] = p0
+        res["links"], res["plaq_final"] = read_config(out + ".dat", V, p0.shape[0] - 1)
+        return res
     N = None
     raw = np.loadtxt(out + ".plaq")
     if raw.ndim == 2 and raw.shape[1] == 4:  # improved action: w1 and w2 (nspt.cc:586-597)

@@ -27,6 +27,9 @@
  *   --twist-init   refresh the twisted copy sites once after a file start
  *                  (Quenched.cc does not; the copies would otherwise hold the
  *                  identity for the first step);
+ *   --lower LO     the --start file holds LO <= allocORD orders: load it with
+ *                  the reference's ptGluon_fld::loadlowerorder
+ *                  (QCDenvNODEpt_test.h:376-426) after a cold start;
  *   --project      apply the reference's unitarisation U = exp(reH(log U))
  *                  (QCDenvNODEpt_test.h:414-417) to every link of a file start
  *                  before the run;
@@ -42,7 +45,7 @@
  * Usage:
  *   ref_harness --L l0 l1 l2 l3 --steps S --dt DT --alpha A --seed SEED
  *               --start cold|FILE --out PREFIX [--noise FILE] [--twist-init]
- *               [--project] [--time] [--sweep-only]
+ *               [--project] [--time] [--sweep-only] [--lower LO]
  */
 #include "nspt.h"
 
@@ -83,7 +86,7 @@ static void usage() {
   fprintf(stderr,
           "ref_harness --L l0 l1 l2 l3 --steps S --dt DT --alpha A --seed S "
           "--start cold|FILE --out PREFIX [--noise FILE] [--twist-init] "
-          "[--project] [--time] [--sweep-only] [--loops FILE] [--wl2x2 FILE]\n");
+          "[--project] [--time] [--sweep-only] [--lower LO] [--loops FILE] [--wl2x2 FILE]\n");
   exit(2);
 }
 
@@ -94,6 +97,7 @@ int main(int argc, char **argv) {
   long seed = 12345;
   std::string start = "cold", out = "ref", noise_path, loops_path, wl2x2_path;
   bool twist_init = false, project = false, timing = false, sweep_only = false;
+  int lower = 0;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
     if (a == "--L" && i + 4 < argc) {
@@ -120,6 +124,8 @@ int main(int argc, char **argv) {
       timing = true;
     } else if (a == "--sweep-only") {
       sweep_only = true;
+    } else if (a == "--lower" && i + 1 < argc) {
+      lower = atoi(argv[++i]);
     } else if (a == "--loops" && i + 1 < argc) {
       loops_path = argv[++i];
     } else if (a == "--wl2x2" && i + 1 < argc) {
@@ -234,6 +240,14 @@ int main(int argc, char **argv) {
   if (start == "cold") {
     for (int i = 0; i < LL.TSize; i++)
       for (int mu = 0; mu < dim; mu++) Umu.W[i].U[mu].id();
+  } else if (lower > 0) {
+    for (int i = 0; i < LL.TSize; i++)
+      for (int mu = 0; mu < dim; mu++) Umu.W[i].U[mu].id();
+    std::vector<Cplx> plq(allocORD + 1);
+    if (Umu.loadlowerorder(start.c_str(), lower, plq.data())) {
+      fprintf(stderr, "ref_harness: loadlowerorder %s failed\n", start.c_str());
+      return 1;
+    }
   } else {
     if (Umu.load(start.c_str(), w1)) {
       fprintf(stderr, "ref_harness: cannot load %s\n", start.c_str());

@@ -223,6 +223,17 @@ class NsptEngine:
                     "nspt_load_config")
         return trailer
 
+    def loadlowerorder(self, path: str, loworder: int) -> np.ndarray:
+        """ptGluon_fld::loadlowerorder (QCDenvNODEpt_test.h:376-426): start
+        from a file saved with loworder <= N orders; the orders above are
+        zero and every link is unitarised, U = exp(reH(log U)).  Returns the
+        file's loworder + 1 plaquette values."""
+        lo = int(loworder)
+        trailer = np.zeros((max(lo, 0) + 1, 2))
+        self._check(load_library().nspt_load_lower_order(self._h, path.encode(), lo, _dp(trailer)),
+                    "nspt_load_lower_order")
+        return trailer
+
     # -- noise ------------------------------------------------------------
     def set_noise(self, eta: np.ndarray):
         """Inject the 8 Gaussians per link SU3rand draws (V, 4, 8) for the next sweep."""

@@ -70,6 +70,7 @@ SIGNATURES = {
     "nspt_get_ff_scale": (_I, [_P, ctypes.POINTER(_I)]),
     "nspt_save_config": (_I, [_P, ctypes.c_char_p, _I]),
     "nspt_load_config": (_I, [_P, ctypes.c_char_p, _I, _D]),
+    "nspt_load_lower_order": (_I, [_P, ctypes.c_char_p, _I, _D]),
     "nspt_last_step_ms": (ctypes.c_double, [_P]),
     "nspt_last_kernel_ms": (ctypes.c_double, [_P]),
     "nspt_measure_fp64_peak": (_I, [_D]),

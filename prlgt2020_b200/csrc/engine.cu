@@ -1049,6 +1049,55 @@ extern "C" int nspt_load_config(nspt_ctx *ctx, const char *path, int A, double *
   return nspt_upload_links(ctx, host.data(), A);
 }
 
+extern "C" int nspt_load_lower_order(nspt_ctx *ctx, const char *path, int loworder,
+                                     double *plaq_trailer) {
+  if (!ctx || !path) return NSPT_ERR_ARG;
+  // QCDenvNODEpt_test.h:377-380: no more orders than the field holds
+  if (loworder < 1 || loworder > ctx->N) return NSPT_ERR_ORDER;
+  const int lo = loworder, N = ctx->N;
+  FILE *f = fopen(path, "rb");
+  if (!f) return NSPT_ERR_IO;
+  const size_t ser_lo = 2 * (1 + 9 * (size_t)lo), ser_n = 2 * (1 + 9 * (size_t)N);
+  std::vector<double> file((size_t)ctx->V * 4 * ser_lo);
+  std::vector<double> trailer(2 * (lo + 1));
+  // the exact byte count of a loworder file (QCDenvNODEpt_test.h:387-390)
+  fseek(f, 0, SEEK_END);
+  const long sz = ftell(f);
+  fseek(f, 0, SEEK_SET);
+  const long want = (long)((file.size() + trailer.size()) * sizeof(double));
+  bool ok = sz == want && fread(file.data(), sizeof(double), file.size(), f) == file.size() &&
+            fread(trailer.data(), sizeof(double), trailer.size(), f) == trailer.size();
+  fclose(f);
+  if (!ok) return NSPT_ERR_IO;
+  // orders 1..lo from the file, every order above zero (QCDenvNODEpt_test.h:396-411)
+  std::vector<double> host((size_t)ctx->V * 4 * ser_n, 0.0);
+  for (size_t l = 0; l < (size_t)ctx->V * 4; l++)
+    std::copy(file.begin() + l * ser_lo, file.begin() + (l + 1) * ser_lo, host.begin() + l * ser_n);
+  std::vector<double>().swap(file);
+  int rc = nspt_upload_links(ctx, host.data(), N);
+  if (rc) return rc;
+  // U = exp(reH(log U)) per link (QCDenvNODEpt_test.h:414-417)
+  double2 *U = ctx->U, *Uf = ctx->Uf;
+  const int SS = ctx->SS;
+  const Geo geo = ctx->geo;
+  cudaStream_t st = ctx->st;
+  const bool low = N <= 3 * MO_LOW;
+  rc = launch_groups(
+      ctx, low ? (const void *)k_unitarise<true> : (const void *)k_unitarise<false>, 3, 4 * ctx->V,
+      [&](unsigned g, dim3 b, size_t sm) {
+        if (low)
+          k_unitarise<true><<<g, b, sm, st>>>(U, Uf, N, SS, geo);
+        else
+          k_unitarise<false><<<g, b, sm, st>>>(U, Uf, N, SS, geo);
+      },
+      "unitarise", 0, low);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(ctx->st));
+  ctx->have_obs = false;
+  if (plaq_trailer) std::copy(trailer.begin(), trailer.end(), plaq_trailer);
+  return NSPT_OK;
+}
+
 extern "C" int nspt_measure_fp64_peak(double *tflops) {
   nspt_ctx *ctx = nullptr;
   if (!tflops) return NSPT_ERR_ARG;

@@ -728,6 +728,41 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
   if (L.j == 0) Uf[(size_t)mu * V + site] = make_double2(1.0, 0.0);
 }
 
+// U = exp(reH(log U)) per link: the unitarisation the reference applies to
+// a configuration loaded with fewer orders than it evolves
+// (ptGluon_fld::loadlowerorder, QCDenvNODEpt_test.h:414-417).  Flag 1.
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
+    k_unitarise(double2 *U, double2 *Uf, int N, int SS, Geo geo) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5;
+  const size_t V = (size_t)geo.V;
+  double2 *X = sm + (size_t)(warp * LPW + g) * 3 * SS, *Sc = X + SS, *Y2 = Sc + SS;
+  bool valid;
+  const long link = group_unit(g, 4L * geo.V, valid);
+  if (!valid) return;
+  const int mu = (int)(link / geo.V);
+  const int site = (int)(link - (long)mu * geo.V);
+  Nb n;
+  n.site = site;
+  n.fwd = n.bwd = 0;
+  stage(X, U, Uf, mu, n, geo, N, L);
+  ser_log<(LOW ? MO_LOW : MO)>(X, Y2, Sc, N, L, [](int, int, double2) {});
+  ser_reH(Sc, N, L);
+  __syncwarp(L.mask);
+  ser_exp<(LOW ? MO_LOW : MO)>(Sc, Y2, X, N, L);
+  double2 *dst = U + (size_t)mu * 9 * N * V + site;
+  const int c = L.c;
+  for (int k = L.s + 1; k <= N; k += 3) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) dst[(size_t)(9 * (k - 1) + 3 * r + c) * V] = X[sidx(k, r, c)];
+  }
+  if (L.j == 0) Uf[(size_t)mu * V + site] = make_double2(1.0, 0.0);
+}
+
 // Lg = log(U) per link (the logs FAstochastic_gauge_fixing needs, nspt.cc:874-875).
 template <bool LOW = false>
 __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)

@@ -82,9 +82,32 @@ def make_case(c: dict) -> dict:
     return out
 
 
+# loadlowerorder (QCDenvNODEpt_test.h:376-426): the reference at N orders
+# starts from a file saved with LO < N orders (an oracle random start)
+LOWER = dict(name="lower_n3_to_n6", L=(4, 4, 2, 4), N=6, LO=3, start=33)
+
+
+def make_lower(c: dict) -> dict:
+    binary = O.build_reference(c["N"], "pbc", "fa", (1, 1, 1))
+    with tempfile.TemporaryDirectory() as d:
+        o = O.Oracle(c["L"], c["LO"])
+        o.random_start(c["start"], 0.5)
+        path = os.path.join(d, "lower.dat")
+        O.write_config(path, o.links, o.plaquette())
+        r = O.run_reference(binary, c["L"], 0, 0.01, 0.0, 1, d, start=path, noise=False,
+                            lower=c["LO"])
+    return dict(links=r["links"][:LINK_SITES], plaq_final=r["plaq_final"],
+                L=np.array(c["L"]), N=c["N"], LO=c["LO"], start=c["start"])
+
+
 def main():
     meta = []
     only = set(sys.argv[1:])
+    if not only or LOWER["name"] in only:
+        os.makedirs(os.path.join(OUT, "lower"), exist_ok=True)
+        path = os.path.join(OUT, "lower", LOWER["name"] + ".npz")
+        np.savez_compressed(path, **make_lower(LOWER))
+        meta.append((LOWER["name"], os.path.getsize(path)))
     for c in CASES:
         if only and c["name"] not in only:
             continue
