@@ -446,6 +446,38 @@ def run_c2(args, world, rank, local):
     eng.close()
 
 
+def dt_extrapolation(rep_means, L, dts, orders=(2,)):
+    """dt -> 0 of the plaquette coefficients: rep_means[r, k] is replica r's
+    time-averaged order-k plaquette; replicas are grouped by volume and dt,
+    and per volume P_k(dt) = P0 + c dt is fitted by weighted least squares
+    (weights 1 / standard error^2 of each dt's replica mean)."""
+    import numpy as np
+    out = {}
+    vols = sorted(set(tuple(l) for l in L))
+    for vol in vols:
+        key = "x".join(str(v) for v in vol)
+        res = {}
+        for k in orders:
+            xs, ys, es = [], [], []
+            for dt in sorted(set(dts)):
+                idx = [r for r in range(len(L)) if tuple(L[r]) == vol and dts[r] == dt]
+                v = rep_means[idx, k]
+                xs.append(dt)
+                ys.append(float(v.mean()))
+                es.append(float(v.std(ddof=1) / np.sqrt(len(v))) if len(v) > 1 else float("nan"))
+            x, y, e = np.array(xs), np.array(ys), np.array(es)
+            w = 1.0 / np.maximum(e, 1e-300) ** 2
+            A = np.stack([np.ones_like(x), x], axis=1)
+            cov = np.linalg.inv(A.T @ (A * w[:, None]))
+            p0, c = cov @ (A.T @ (w * y))
+            chi2 = float(np.sum(w * (y - (p0 + c * x)) ** 2))
+            res["order_%d" % k] = {"P0": float(p0), "P0_err": float(np.sqrt(cov[0, 0])),
+                                   "slope": float(c), "chi2": chi2, "dof": len(x) - 2,
+                                   "per_dt": {str(a): [b, d] for a, b, d in zip(xs, ys, es)}}
+        out["L=" + key] = res
+    return out
+
+
 def run_c4(args, world, rank, local):
     """64 independent replicas, 12 orders, periodic, zero modes + FA gauge
     fixing every step: replica r has L = {6,8,10}[r mod 3]^4, dt =
@@ -483,7 +515,7 @@ def run_c4(args, world, rank, local):
         e.close()
     # batched
     b = P.NsptBatch(L, N, dts, seeds, **kw)
-    warps = b.tune(1)
+    warps, shape_mo, tune_ms = b.tune_shape(1)
     b.step(max(2, args.warmup - args.warmup % 2), 1)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -491,8 +523,22 @@ def run_c4(args, world, rank, local):
     torch.cuda.synchronize()
     batch_s = max_over_ranks(time.perf_counter() - t0)
     batch_dev_ms = max_over_ranks(b.last_step_ms())
-    plaq = b.plaquettes()
     b.close()
+    # dt -> 0: a fresh batch, thermalised, then the plaquette series of every
+    # replica averaged over the measured steps (read every 2 steps)
+    b = P.NsptBatch(L, N, dts, seeds, **kw)
+    b.tune_shape(1)
+    therm, meas = args.c4_therm - args.c4_therm % 2, max(2, args.c4_meas - args.c4_meas % 2)
+    t_phys = time.perf_counter()
+    if therm:
+        b.step(therm, 1)
+    acc = np.zeros((nrep, N + 1))
+    for _ in range(meas // 2):
+        b.step(2, 1)
+        acc += b.plaquettes()[:, :, 0]
+    t_phys = time.perf_counter() - t_phys
+    b.close()
+    rep_means = acc / (meas // 2)
     Pn = N * (N - 1) // 2
     E = (N - 1) * N * (N + 1) // 6
     links = sum(4 * int(np.prod(l)) for l in L)
@@ -502,7 +548,14 @@ def run_c4(args, world, rank, local):
         series = {}
         for dt in (0.005, 0.01, 0.02):
             idx = [r for r in range(nrep) if dts[r] == dt]
-            series[str(dt)] = plaq[idx, :, 0].mean(axis=0).tolist()
+            series[str(dt)] = rep_means[idx].mean(axis=0).tolist()
+        extrap = dt_extrapolation(rep_means, L, dts, orders=(2, 4))
+        extrap["how"] = ("per replica the plaquette series averaged over %d measured steps (every "
+                         "2nd) after %d thermalisation steps; per (L, dt) the mean over replicas "
+                         "and its standard error; per L a weighted least-squares fit "
+                         "P(dt) = P0 + c dt (the Euler update's O(dt) error), P0 +- its error"
+                         % (meas, therm))
+        extrap["seconds"] = t_phys
         line = {
             "metric": "replica Langevin steps/s, 64 replicas of 6^4/8^4/10^4 x 12 orders "
                       "(FP64, ZM + FA every step)",
@@ -516,10 +569,15 @@ def run_c4(args, world, rank, local):
             "plain": {"value": whole_job_rate(nrep * K, world, plain_s), "unit": "replica steps/s",
                       "how": "replicas one after another, nspt_step each"},
             "batched_over_plain": plain_s / batch_s,
-            "batched_device_ms": batch_dev_ms, "tuned_warps": warps,
+            "batched_device_ms": batch_dev_ms,
+            "tuned": {"warps_per_cta": warps, "orders_per_lane": shape_mo,
+                      "run_length": shape_mo // 2,
+                      "ms_per_2_steps": {"orders_per_lane_8": tune_ms[0].tolist(),
+                                         "orders_per_lane_4": tune_ms[1].tolist()}},
             "roofline": {"bound": "fp64", "achieved": flops / batch_s / 1e12, "peak": peak,
                          "unit": "TFLOP/s", "frac": flops / batch_s / 1e12 / peak},
             "plaquette_per_dt": series,
+            "dt_to_0": extrap,
         }
         print(json.dumps(line), flush=True)
 

@@ -236,9 +236,17 @@ int nspt_batch_step(nspt_batch *b, int nsteps, int gf_every);
 double nspt_batch_last_step_ms(const nspt_batch *b);
 /* Plaquette series of every replica's last sweep: plaq[nrep][(N+1)*2]. */
 int nspt_batch_observables(nspt_batch *b, double *plaq);
-/* Autotuner: times the batch step for every sweep shape (warps per CTA)
- * and keeps the fastest in *warps_out; the trial steps are undone (every
+/* Autotuner over the tile shape of the series kernels: orders per lane and
+ * pass (8, or 4 where N <= 12; in the paired-run product the run length is
+ * half of it) and the sweep's warps per CTA (3 links each).  Every candidate
+ * is timed on the batch step itself and the fastest kept: *warps_out,
+ * *mo_out (orders per lane and pass); ms_table (may be NULL) gets [2][8]
+ * times, row 0 for 8 orders per lane, row 1 for 4, column w-1 for w warps,
+ * 0 where a candidate does not exist.  The trial steps are undone (every
  * replica back to a cold start with its seed).  Call before stepping. */
+int nspt_batch_tune_shape(nspt_batch *b, int gf_every, int *warps_out, int *mo_out,
+                          float *ms_table);
+/* nspt_batch_tune_shape reporting the warps only. */
 int nspt_batch_tune(nspt_batch *b, int gf_every, int *warps_out);
 
 /* Static plaquette of a field the caller already holds in device memory,

@@ -406,6 +406,16 @@ class NsptBatch:
               "nspt_batch_tune")
         return w.value
 
+    def tune_shape(self, gf_every: int = 1):
+        """Autotune the tile shape: (warps per CTA, orders per lane and pass,
+        table of step times in ms [orders 8 / 4][warps 1..8], 0 = not tried)."""
+        w, mo = ctypes.c_int(), ctypes.c_int()
+        table = (ctypes.c_float * 16)()
+        check(load_library().nspt_batch_tune_shape(self._h, int(gf_every), ctypes.byref(w),
+                                                   ctypes.byref(mo), table),
+              "nspt_batch_tune_shape")
+        return w.value, mo.value, np.array(list(table), dtype=np.float64).reshape(2, 8)
+
     def close(self):
         if getattr(self, "_h", None):
             for e in self.replicas:

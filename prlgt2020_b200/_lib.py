@@ -82,6 +82,7 @@ SIGNATURES = {
     "nspt_batch_last_step_ms": (ctypes.c_double, [_P]),
     "nspt_batch_observables": (_I, [_P, _D]),
     "nspt_batch_tune": (_I, [_P, _I, ctypes.POINTER(_I)]),
+    "nspt_batch_tune_shape": (_I, [_P, _I, ctypes.POINTER(_I), ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_float)]),
     "nspt_plaquette_measure_noalloc": (_I, [ctypes.c_void_p, _I, ctypes.POINTER(ctypes.c_int), _I,
                                            ctypes.c_uint, _D, ctypes.c_void_p]),
 }

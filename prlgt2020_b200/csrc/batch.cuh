@@ -217,27 +217,49 @@ extern "C" int nspt_batch_observables(nspt_batch *b, double *plaq) {
   return NSPT_OK;
 }
 
-// Autotuner: time the batch step with each candidate number of sweep warps
-// per CTA and keep the fastest.  The trial steps change the fields, so every
-// replica is put back to a cold start with its seed (counter 0) afterwards.
-extern "C" int nspt_batch_tune(nspt_batch *b, int gf_every, int *warps_out) {
+// Autotuner over the tile shape of the series kernels: orders per lane and
+// pass (MO, or MO_LOW where N <= 3 MO_LOW; in the paired-run product this
+// is the run length, MO/2) and, for the sweep, warps per CTA (3 links per
+// warp: the links, i.e. sites x directions, per block).  Every candidate is
+// captured and timed on the batch itself; the fastest is kept.  The trial
+// steps change the fields, so every replica is put back to a cold start
+// with its seed (counter 0) afterwards.  ms_table (may be NULL) receives
+// [2][8] times: row 0 the MO shape, row 1 MO_LOW, column w-1 for w warps,
+// 0 where the candidate does not exist.
+extern "C" int nspt_batch_tune_shape(nspt_batch *b, int gf_every, int *warps_out, int *mo_out,
+                                     float *ms_table) {
   if (!b) return NSPT_ERR_ARG;
   const int P = graph_length(gf_every);
+  if (ms_table)
+    for (int i = 0; i < 16; i++) ms_table[i] = 0.f;
   float best = 0.f;
-  int best_w = 0;
-  for (int w = 1; w <= SWEEP_THREADS / 32; w++) {
-    for (nspt_ctx *c : b->ctx) c->sweep_warps = w;
-    drop_graph(b);
-    int rc = nspt_batch_step(b, P, gf_every);  // capture + warm-up
-    if (!rc) rc = nspt_batch_step(b, 2 * P, gf_every);
-    if (rc) return rc;
-    if (!best_w || b->last_ms < best) {
-      best = b->last_ms;
-      best_w = w;
+  int best_w = 0, best_mo = 0;
+  for (int row = 0; row < 2; row++) {
+    const int mo = row == 0 ? MO : MO_LOW;
+    if (mo == MO_LOW && b->N > 3 * MO_LOW) continue;
+    const int wmax = (mo == MO ? SWEEP_THREADS : SWEEP_THREADS_LOW) / 32;
+    for (int w = 1; w <= wmax; w++) {
+      for (nspt_ctx *c : b->ctx) {
+        c->sweep_warps = w;
+        c->shape_mo = mo;
+        c->launch_gen++;
+      }
+      drop_graph(b);
+      int rc = nspt_batch_step(b, P, gf_every);  // capture + warm-up
+      if (!rc) rc = nspt_batch_step(b, 2 * P, gf_every);
+      if (rc) return rc;
+      if (ms_table) ms_table[row * 8 + (w - 1)] = b->last_ms;
+      if (!best_w || b->last_ms < best) {
+        best = b->last_ms;
+        best_w = w;
+        best_mo = mo;
+      }
     }
   }
   for (int r = 0; r < b->nrep; r++) {
     b->ctx[r]->sweep_warps = best_w;
+    b->ctx[r]->shape_mo = best_mo;
+    b->ctx[r]->launch_gen++;
     int rc = nspt_cold_start(b->ctx[r]);
     if (!rc) rc = nspt_seed(b->ctx[r], b->seed[r], 0);
     if (rc) return rc;
@@ -246,5 +268,11 @@ extern "C" int nspt_batch_tune(nspt_batch *b, int gf_every, int *warps_out) {
   drop_graph(b);
   b->warps = best_w;
   if (warps_out) *warps_out = best_w;
+  if (mo_out) *mo_out = best_mo;
   return NSPT_OK;
+}
+
+// The same tuner, reporting the warps only.
+extern "C" int nspt_batch_tune(nspt_batch *b, int gf_every, int *warps_out) {
+  return nspt_batch_tune_shape(b, gf_every, warps_out, nullptr, nullptr);
 }

@@ -57,6 +57,10 @@ struct nspt_ctx {
   int gf_grid[4]; // local gauge fixing: the reference's thread grid (ntt, ntx, nty, ntz)
   unsigned long long *dcounter;  // Philox step counter on the device (advanced by k_inc)
   int sweep_warps;               // warps per CTA of the sweep, 0 = as many as fit
+  // orders per lane and pass of the series kernels: 0 = by N (the low-order
+  // shape, MO_LOW, for N <= 3 MO_LOW), MO = the 24-order shape everywhere,
+  // MO_LOW = the low-order shape (only where N <= 3 MO_LOW)
+  int shape_mo;
   double c1;                     // improved action weight (0: Wilson), c0 = 1 - 8 c1
   double2 *obs_tr2;              // [(N+1)][4V] rectangle traces (improved actions)
   int *ff_e;                     // float-float scale exponent used by the sweep (device)
@@ -114,6 +118,13 @@ static size_t group_bytes(const nspt_ctx *ctx, int slots, int extra) {
   return ((size_t)slots * ctx->SS + extra) * sizeof(double2);
 }
 
+// the low-order kernel shape (MO_LOW orders per lane and pass, 6-warp CTAs,
+// two per SM) for this context's series kernels
+static bool use_low(const nspt_ctx *ctx) {
+  if (ctx->N > 3 * MO_LOW) return false;
+  return ctx->shape_mo != MO;
+}
+
 static KernelShape choose_shape(const nspt_ctx *ctx, int slots, long units, int extra = 0,
                                 int max_warps = 8, int ctas_per_sm = 1) {
   KernelShape k;
@@ -140,7 +151,7 @@ static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
   const long nl = 4 * ctx->V;
   const bool ff = (ctx->flags & NSPT_PRECISION_FF) != 0;
   // low orders: the lighter variant, two CTAs per SM
-  const bool low = !measure && !ff && ctx->N <= 3 * MO_LOW;
+  const bool low = !measure && !ff && use_low(ctx);
   const int max_warps = (low ? SWEEP_THREADS_LOW : SWEEP_THREADS) / 32;
   KernelShape k = choose_shape(ctx, SWEEP_SLOTS, nl, 0,
                                ctx->sweep_warps > 0 ? std::min(ctx->sweep_warps, max_warps)
@@ -164,7 +175,7 @@ static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
 
 static int launch_sweep_imp(nspt_ctx *ctx, const SweepArgs &a) {
   const long nl = 4 * ctx->V;
-  const bool low = ctx->N <= 3 * MO_LOW;
+  const bool low = use_low(ctx);
   KernelShape k = low ? choose_shape(ctx, IMP_SLOTS, nl, 0, SWEEP_THREADS_LOW / 32, 2)
                       : choose_shape(ctx, IMP_SLOTS, nl, 0);
   const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, IMP_SLOTS, 0);
@@ -286,7 +297,7 @@ static int do_zero_modes(nspt_ctx *ctx) {
   const int SS = ctx->SS;
   const Geo geo = ctx->geo;
   cudaStream_t st = ctx->st;
-  const bool low = N <= 3 * MO_LOW;
+  const bool low = use_low(ctx);
   return launch_groups(
       ctx, low ? (const void *)k_zero_modes<true> : (const void *)k_zero_modes<false>, 3, nl,
       [&](unsigned g, dim3 b, size_t sm) {
@@ -328,7 +339,7 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
   cudaStream_t st = ctx->st;
   double2 *U = ctx->U, *Uf = ctx->Uf, *F = ctx->F, *Ff = ctx->Ff, *Lg = ctx->Lg, *Wg = ctx->Wg,
           *Gx = ctx->Gx;
-  const bool low = N <= 3 * MO_LOW;
+  const bool low = use_low(ctx);
   int rc = launch_groups(
       ctx, low ? (const void *)k_log_links<true> : (const void *)k_log_links<false>, 3, nl,
       [&](unsigned g, dim3 b, size_t sm) {
@@ -396,7 +407,7 @@ static int do_local_gf(nspt_ctx *ctx, double alpha) {
   const Geo geo = ctx->geo;
   cudaStream_t st = ctx->st;
   double2 *U = ctx->U, *Uf = ctx->Uf;
-  const bool low = N <= 3 * MO_LOW;
+  const bool low = use_low(ctx);
   for (long p = 0; p < steps; p++) {
     int rc = launch_groups(
         ctx, low ? (const void *)k_local_gf<true> : (const void *)k_local_gf<false>, 4, gr.nthr,
@@ -505,6 +516,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->p2 = nullptr;
   ctx->dcounter = nullptr;
   ctx->sweep_warps = 0;
+  ctx->shape_mo = 0;
   ctx->launch_gen = 0;
   ctx->loop_part = nullptr;
   ctx->loop_part_n = 0;
@@ -1081,7 +1093,7 @@ extern "C" int nspt_load_lower_order(nspt_ctx *ctx, const char *path, int loword
   const int SS = ctx->SS;
   const Geo geo = ctx->geo;
   cudaStream_t st = ctx->st;
-  const bool low = N <= 3 * MO_LOW;
+  const bool low = use_low(ctx);
   rc = launch_groups(
       ctx, low ? (const void *)k_unitarise<true> : (const void *)k_unitarise<false>, 3, 4 * ctx->V,
       [&](unsigned g, dim3 b, size_t sm) {

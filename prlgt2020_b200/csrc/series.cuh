@@ -206,10 +206,11 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
 // For M = NR * R result orders with NR in {5, 6} (R set by the caller's
 // orders-per-lane budget), the triangle is cut into NR runs of R consecutive
 // orders, run r holding orders (r-1)R+1 .. rR.  Lane (c, s) of the group
-// owns column c of two runs: lo = s + 1 and hi = 6 - s (NR = 6), or lo = s
-// (none for s = 0) and hi = 5 - s (NR = 5).  A run ending at order b takes
-// b - 1 steps (left orders i = 1 .. b-1; the lo run is padded to a whole
-// number of R-step blocks), so a lane's two runs take (NR + 1) R - 1 or
+// owns column c of two runs: hi = NR - s and lo = s + 1 (NR = 6) or lo = s
+// (NR = 5; none for s = 0).  A run ending at order b takes b - 1 steps
+// (left orders i = 1 .. b-1).  The hi run goes first, padded to rhi R steps
+// (a whole number of R-step blocks) when a lo run follows it; the lo run
+// ends the lane's walk.  A lane's two runs then take (NR + 1) R - 1 or
 // NR R - 1 steps whatever s is: every lane walks the same number of steps
 // and the same straight-line code, without the per-order branches of
 // product().  A step is one left order i and all R orders of the run:
@@ -218,11 +219,18 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
 // column moves up one order, so a step loads only one new column; the
 // window is circular (slot (q - u) mod R at step u of an R-step block), so
 // it needs no register moves.  Right columns below order 1 read as zero,
-// which pads a run's first R-1 steps and the lo run's last step with exact
-// zero terms; the hi run's last R-1 steps (common to all lanes) skip them.
-// The sum over i runs in the same (ascending) order as in product(), so
-// both forms give the same values.  Every lane finishes reading before any
-// writes, so the result may overwrite either operand.
+// which pads the hi run's last steps with exact zero terms; the last R-1
+// steps of the walk (common to all lanes) skip them.  The sum over i runs
+// in the same (ascending) order as in product(), so both forms give the
+// same values.
+//
+// In place (the result overwriting A or B): a lane writes its hi run when
+// it moves on to its lo run, at the start of block rhi.  Every lane has then
+// finished the steps before that block (a __syncwarp opens each block), and
+// from there on it reads only left orders above rhi R (A_i, i > rhi R >= the
+// hi run's orders) and right orders below (rhi' - rhi) R + 1 <= (rhi - 1) R
+// (rhi' <= 2 rhi - 1 for the runs here), below the hi run's first order; the
+// lo runs read orders up to 3R and are written after a final __syncwarp.
 template <int R, bool DA, class Left>
 __device__ __forceinline__ void pr_step(const Left &A, int i, int u, int qlo,
                                         double2 (&acc)[R][3], const double2 (&w)[R][3]) {
@@ -275,44 +283,9 @@ __device__ __forceinline__ void product_pr(const Left &A, double2 a0, const doub
   const int rhi = NR - s;
   const int alo = (rlo - 1) * R + 1;
   const int ahi = (rhi - 1) * R + 1;
-  const int nblk = rlo + rhi - 1;  // R-step blocks; then the hi run's last R-1 steps
-  double2 acc[R][3], lo[R][3], w[R][3];
-#pragma unroll
-  for (int q = 0; q < R; q++)
-#pragma unroll
-    for (int r = 0; r < 3; r++) acc[q][r] = lo[q][r] = cz();
-  int a = rlo > 0 ? alo : ahi;
-#pragma unroll
-  for (int q = 1; q < R; q++) pr_col(B, a + q - 1, c, w[q]);
-  int i = 0;
-  for (int b = 0; b < nblk; b++) {
-    if (b == rlo) {  // the lo run (rlo blocks) is done: on to the hi run
-#pragma unroll
-      for (int q = 0; q < R; q++)
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-          lo[q][r] = acc[q][r];
-          acc[q][r] = cz();
-        }
-      a = ahi;
-      i = 0;
-#pragma unroll
-      for (int q = 1; q < R; q++) pr_col(B, a + q - 1, c, w[q]);
-    }
-#pragma unroll
-    for (int u = 0; u < R; u++) {
-      ++i;
-      pr_col(B, a - i, c, w[(R - u) % R]);
-      pr_step<R, DA>(A, i, u, 0, acc, w);
-    }
-  }
-#pragma unroll
-  for (int u = 0; u < R - 1; u++) {  // order q of the hi run is active while q > u
-    ++i;
-    pr_step<R, DA>(A, i, u, u + 1, acc, w);
-  }
-  __syncwarp(L.mask);
+  const int nblk = rlo + rhi - 1;  // R-step blocks; then the walk's last R-1 steps
   const bool fa = !cis0(a0), fb = !cis0(b0);
+  // the orders of one run, with the flag terms b0 A_k + a0 B_k
   auto out = [&](int k, const double2(&v3)[3]) {
     double2 ak[3];
     if (fb) A.template col<DA>(k, c, ak);
@@ -332,12 +305,44 @@ __device__ __forceinline__ void product_pr(const Left &A, double2 a0, const doub
       emit(k, r, v);
     }
   };
-  if (rlo > 0) {
+  double2 acc[R][3], w[R][3];
 #pragma unroll
-    for (int q = 0; q < R; q++) out(alo + q, lo[q]);
+  for (int q = 0; q < R; q++)
+#pragma unroll
+    for (int r = 0; r < 3; r++) acc[q][r] = cz();
+  int a = ahi;
+#pragma unroll
+  for (int q = 1; q < R; q++) pr_col(B, a + q - 1, c, w[q]);
+  int i = 0;
+  for (int b = 0; b < nblk; b++) {
+    __syncwarp(L.mask);
+    if (rlo > 0 && b == rhi) {  // hi run done (padded to rhi blocks): write it, on to lo
+#pragma unroll
+      for (int q = 0; q < R; q++) {
+        out(ahi + q, acc[q]);
+#pragma unroll
+        for (int r = 0; r < 3; r++) acc[q][r] = cz();
+      }
+      a = alo;
+      i = 0;
+#pragma unroll
+      for (int q = 1; q < R; q++) pr_col(B, a + q - 1, c, w[q]);
+    }
+#pragma unroll
+    for (int u = 0; u < R; u++) {
+      ++i;
+      pr_col(B, a - i, c, w[(R - u) % R]);
+      pr_step<R, DA>(A, i, u, 0, acc, w);
+    }
   }
 #pragma unroll
-  for (int q = 0; q < R; q++) out(ahi + q, acc[q]);
+  for (int u = 0; u < R - 1; u++) {  // order q of the last run is active while q > u
+    ++i;
+    pr_step<R, DA>(A, i, u, u + 1, acc, w);
+  }
+  __syncwarp(L.mask);
+#pragma unroll
+  for (int q = 0; q < R; q++) out(a + q, acc[q]);
   __syncwarp(L.mask);
 }
 
@@ -365,8 +370,13 @@ template <int MO>
 __device__ __noinline__ void slot_mul_to(double2 *out, const double2 *A, double2 a0,
                                          const double2 *B, double2 b0, int M, const Lane &L) {
   const int c = L.c;
+#ifdef NSPT_PR_STAPLES_ONLY
+  product<MO, false>(LeftS{A}, a0, B, b0, M, L,
+                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
+#else
   product_any<MO, false>(LeftS{A}, a0, B, b0, M, L,
                          [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
+#endif
   __syncwarp(L.mask);
 }
 
@@ -376,10 +386,12 @@ template <int MO>
 __device__ __noinline__ void slot_horner(double2 *S, const double2 *Y, double2 sf, const double2 *X,
                                          double cx, int M, const Lane &L) {
   const int c = L.c;
-  product_any<MO, false>(
-      LeftS{Y}, cz(), S, sf, M, L,
-      [&](int k, int r, double2 v) { S[sidx(k, r, c)] = cadd(v, cscale(X[sidx(k, r, c)], cx)); },
-      2);
+  auto em = [&](int k, int r, double2 v) { S[sidx(k, r, c)] = cadd(v, cscale(X[sidx(k, r, c)], cx)); };
+#ifdef NSPT_PR_STAPLES_ONLY
+  product<MO, false>(LeftS{Y}, cz(), S, sf, M, L, em, 2);
+#else
+  product_any<MO, false>(LeftS{Y}, cz(), S, sf, M, L, em, 2);
+#endif
   __syncwarp(L.mask);
 }
 

@@ -96,3 +96,22 @@ def test_batch_captures_again_after_a_replica_is_reseeded(engine_mod):
                 e.seed(999, 2)
             e.NsptEvolve(dt, 2, 1)
             assert np.array_equal(got[r], e.download()), r
+
+
+def test_batch_shape_tuner_covers_orders_per_lane_and_warps(engine_mod):
+    """nspt_batch_tune_shape times both kernel shapes (8 and 4 orders per
+    lane and pass; N = 6 allows both) at every warp count and keeps the
+    fastest; the start is restored, and whatever shape it picks, the batch
+    equals single contexts bit for bit (the shapes sum in the same order)."""
+    P = engine_mod
+    N, kw = 6, dict(zero_modes=True, fa=True, alpha=-0.05)
+    want = singles(P, N, [(2, 1)], **kw)
+    with P.NsptBatch(CASES["L"], N, CASES["dt"], CASES["seeds"], **kw) as b:
+        w, mo, table = b.tune_shape(1)
+        assert mo in (4, 8)
+        assert np.all(table[0, :8] > 0) and np.all(table[1, :6] > 0) and np.all(table[1, 6:] == 0)
+        row = 0 if mo == 8 else 1
+        assert table[row, w - 1] == table[table > 0].min()
+        b.step(2, 1)
+        for r, (links, _) in enumerate(want):
+            assert np.array_equal(b.replicas[r].download(), links), r
