@@ -19,6 +19,7 @@
 
 #include "../../include/nspt_b200.h"
 #include "kernels.cuh"
+#include "fft.cuh"
 #include "loops.cuh"
 
 using namespace nspt;
@@ -54,6 +55,7 @@ struct nspt_ctx {
   double2 *red2;  // [(N+1) + 4N + 4*9N] reduced sums
   double *red1;   // [N]
   double *p2;     // lattice momenta p2hat[4][128] of this context's extents
+  double2 *ftw;   // FFT twiddles exp(-2 pi i t / L_d), [4][128] (FA only)
   int gf_grid[4]; // local gauge fixing: the reference's thread grid (ntt, ntx, nty, ntz)
   unsigned long long *dcounter;  // Philox step counter on the device (advanced by k_inc)
   int sweep_warps;               // warps per CTA of the sweep, 0 = as many as fit
@@ -332,6 +334,83 @@ static int fft4d(nspt_ctx *ctx, double2 *data, int sign) {
   return NSPT_OK;
 }
 
+// Extents with a compile-time FFT plan (fft.cuh); others use fft4d.
+#define NSPT_FFT_SIZES(X) X(2) X(3) X(4) X(5) X(6) X(8) X(10) X(12) X(16) X(20) X(24) X(32)
+
+static bool fft_planned(int n) {
+#define NSPT_FFT_CASE(n_) if (n == n_) return true;
+  NSPT_FFT_SIZES(NSPT_FFT_CASE)
+#undef NSPT_FFT_CASE
+  return false;
+}
+
+template <int n>
+static void fft_t_launch(nspt_ctx *ctx, double2 *data, const double2 *Lg, bool div, int inv) {
+  const long nlines = (long)9 * ctx->N * (ctx->V / n);
+  const unsigned grid = (unsigned)((nlines + 127) / 128);
+  const size_t smem = (size_t)128 * (n | 1) * sizeof(double2);
+  if (div) {
+    cudaFuncSetAttribute(k_fft_t<n, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fft_t<n, true><<<grid, 128, smem, ctx->st>>>(data, Lg, nlines, 9 * ctx->N, ctx->geo,
+                                                   ctx->ftw + 3 * 128, inv);
+  } else {
+    cudaFuncSetAttribute(k_fft_t<n, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_fft_t<n, false><<<grid, 128, smem, ctx->st>>>(data, Lg, nlines, 9 * ctx->N, ctx->geo,
+                                                    ctx->ftw + 3 * 128, inv);
+  }
+}
+
+template <int n>
+static void fft_strided_launch(nspt_ctx *ctx, double2 *data, int d, int inv) {
+  const long nlines = (long)9 * ctx->N * (ctx->V / n);
+  const int st = d == 0 ? ctx->geo.s0 : d == 1 ? ctx->geo.s1 : ctx->geo.s2;
+  k_fft_strided<n><<<(unsigned)((nlines + 127) / 128), 128, 0, ctx->st>>>(
+      data, nlines, st, (size_t)ctx->V, ctx->ftw + d * 128, inv);
+}
+
+template <int n>
+static void fft_x_launch(nspt_ctx *ctx, double2 *data, double alpha) {
+  const long nlines = (long)9 * ctx->N * (ctx->V / n);
+  k_fft_x_scale<n><<<(unsigned)((nlines + 127) / 128), 128, 0, ctx->st>>>(
+      data, nlines, ctx->geo, ctx->ftw, alpha, ctx->p2);
+}
+
+// Wg = iFFT(-alpha / p^2 FFT(div log U)) in seven passes (fft.cuh), or
+// NSPT_ERR_ARG when an extent has no compile-time plan.
+static int fa_fft_fused(nspt_ctx *ctx, double alpha) {
+  for (int d = 0; d < 4; d++)
+    if (!fft_planned(ctx->L[d])) return NSPT_ERR_ARG;
+  double2 *Wg = ctx->Wg;
+  const double2 *Lg = ctx->Lg;
+  auto t_pass = [&](bool div, int inv) {
+    switch (ctx->L[3]) {
+#define NSPT_FFT_CASE(n_) case n_: fft_t_launch<n_>(ctx, Wg, Lg, div, inv); break;
+      NSPT_FFT_SIZES(NSPT_FFT_CASE)
+#undef NSPT_FFT_CASE
+    }
+  };
+  auto s_pass = [&](int d, int inv) {
+    switch (ctx->L[d]) {
+#define NSPT_FFT_CASE(n_) case n_: fft_strided_launch<n_>(ctx, Wg, d, inv); break;
+      NSPT_FFT_SIZES(NSPT_FFT_CASE)
+#undef NSPT_FFT_CASE
+    }
+  };
+  t_pass(true, 0);  // divergence + forward t
+  s_pass(2, 0);
+  s_pass(1, 0);
+  switch (ctx->L[0]) {  // forward x, -alpha / p^2, backward x
+#define NSPT_FFT_CASE(n_) case n_: fft_x_launch<n_>(ctx, Wg, alpha); break;
+    NSPT_FFT_SIZES(NSPT_FFT_CASE)
+#undef NSPT_FFT_CASE
+  }
+  s_pass(1, 1);
+  s_pass(2, 1);
+  t_pass(false, 1);
+  CK(cudaGetLastError());
+  return NSPT_OK;
+}
+
 static int do_fa(nspt_ctx *ctx, double alpha) {
   const int N = ctx->N, SS = ctx->SS;
   const long nl = 4 * ctx->V;
@@ -350,14 +429,19 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
       },
       "FA logs", 0, low);
   if (rc) return rc;
-  const size_t tot = (size_t)9 * N * ctx->V;
-  const unsigned eg = (unsigned)std::min<size_t>((tot + 255) / 256, (size_t)ctx->nsm * 32);
-  k_fa_div<<<eg, 256, 0, st>>>(Lg, Wg, N, geo);
-  CK(cudaGetLastError());
-  if ((rc = fft4d(ctx, Wg, -1))) return rc;
-  k_fa_scale<<<eg, 256, 0, st>>>(Wg, N, geo, alpha, ctx->p2);
-  CK(cudaGetLastError());
-  if ((rc = fft4d(ctx, Wg, +1))) return rc;
+  rc = fa_fft_fused(ctx, alpha);
+  if (rc == NSPT_ERR_ARG) {  // an extent without a compile-time FFT plan
+    const size_t tot = (size_t)9 * N * ctx->V;
+    const unsigned eg = (unsigned)std::min<size_t>((tot + 255) / 256, (size_t)ctx->nsm * 32);
+    k_fa_div<<<eg, 256, 0, st>>>(Lg, Wg, N, geo);
+    CK(cudaGetLastError());
+    if ((rc = fft4d(ctx, Wg, -1))) return rc;
+    k_fa_scale<<<eg, 256, 0, st>>>(Wg, N, geo, alpha, ctx->p2);
+    CK(cudaGetLastError());
+    if ((rc = fft4d(ctx, Wg, +1))) return rc;
+  } else if (rc) {
+    return rc;
+  }
   rc = launch_groups(
       ctx, low ? (const void *)k_fa_gt<true> : (const void *)k_fa_gt<false>, 3, ctx->V,
       [&](unsigned g, dim3 b, size_t sm) {
@@ -467,11 +551,21 @@ static int upload_constants(nspt_ctx *ctx) {
     tw[k] = make_double2(cos(ang), sin(ang));
   }
   CK(cudaMemcpyToSymbol(c_tw64, tw, sizeof(tw)));
+  if (ctx->ftw) {
+    std::vector<double2> ftw(4 * 128, make_double2(0.0, 0.0));
+    for (int d = 0; d < 4; d++)
+      for (int t = 0; t < ctx->L[d]; t++) {
+        const double ang = -2.0 * M_PI * (double)t / (double)ctx->L[d];
+        ftw[d * 128 + t] = make_double2(cos(ang), sin(ang));
+      }
+    CK(cudaMemcpy(ctx->ftw, ftw.data(), ftw.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  }
   return NSPT_OK;
 }
 
 static void free_all(nspt_ctx *ctx) {
-  void *ptrs[] = {ctx->U, ctx->Uf, ctx->F, ctx->Ff, ctx->Lg, ctx->Wg, ctx->Gx, ctx->p2, ctx->dcounter,
+  void *ptrs[] = {ctx->U, ctx->Uf, ctx->F, ctx->Ff, ctx->Lg, ctx->Wg, ctx->Gx, ctx->p2, ctx->ftw,
+                  ctx->dcounter,
                   ctx->loop_part, ctx->obs_tr2, ctx->ff_e, ctx->ff_mx,
                   ctx->obs_tr, ctx->obs_tru, ctx->obs_norm, ctx->red2, ctx->red1, ctx->noise};
   for (void *p : ptrs)
@@ -514,6 +608,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->V = V;
   ctx->U = ctx->Uf = ctx->F = ctx->Ff = ctx->Lg = ctx->Wg = ctx->Gx = nullptr;
   ctx->p2 = nullptr;
+  ctx->ftw = nullptr;
   ctx->dcounter = nullptr;
   ctx->sweep_warps = 0;
   ctx->shape_mo = 0;
@@ -597,7 +692,8 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
     ok = alloc((void **)&ctx->ff_e, sizeof(int)) &&
          alloc((void **)&ctx->ff_mx, N * sizeof(unsigned long long));
   if (ok && (flags & NSPT_GF_FA))
-    ok = alloc((void **)&ctx->Wg, field / 4) && alloc((void **)&ctx->Gx, field / 4);
+    ok = alloc((void **)&ctx->Wg, field / 4) && alloc((void **)&ctx->Gx, field / 4) &&
+         alloc((void **)&ctx->ftw, 4 * 128 * sizeof(double2));
   if (!ok) {
     cudaGetLastError();
     cudaStreamDestroy(ctx->st);

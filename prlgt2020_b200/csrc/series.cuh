@@ -314,7 +314,9 @@ __device__ __forceinline__ void product_pr(const Left &A, double2 a0, const doub
 #pragma unroll
   for (int q = 1; q < R; q++) pr_col(B, a + q - 1, c, w[q]);
   int i = 0;
-  for (int b = 0; b < nblk; b++) {
+  // b == nblk only checks the switch: with rlo == 1 the lo run is just the
+  // final R-1 steps, and the hi run fills every block
+  for (int b = 0; b <= nblk; b++) {
     __syncwarp(L.mask);
     if (rlo > 0 && b == rhi) {  // hi run done (padded to rhi blocks): write it, on to lo
 #pragma unroll
@@ -328,6 +330,7 @@ __device__ __forceinline__ void product_pr(const Left &A, double2 a0, const doub
 #pragma unroll
       for (int q = 1; q < R; q++) pr_col(B, a + q - 1, c, w[q]);
     }
+    if (b == nblk) break;
 #pragma unroll
     for (int u = 0; u < R; u++) {
       ++i;

@@ -107,8 +107,14 @@ def test_cold_start_one_sweep_no_zero_modes(engine_mod, oracle_mod):
 
 
 @pytest.mark.parametrize("L,N,alpha", [((4, 4, 4, 4), 6, -0.05), ((4, 2, 3, 6), 4, -0.1),
-                                       ((8, 4, 4, 4), 12, -0.05)])
+                                       ((8, 4, 4, 4), 12, -0.05), ((10, 5, 4, 2), 4, -0.05),
+                                       ((2, 12, 4, 6), 4, -0.05), ((16, 2, 2, 8), 3, -0.05),
+                                       ((7, 4, 2, 4), 4, -0.05)])
 def test_zero_modes_and_fa_gauge_fixing(engine_mod, oracle_mod, L, N, alpha):
+    """Sweep + zero modes + FA gauge fixing, three steps.  The extents cover
+    the FFT's radix-2, 3, 4 and 5 plans on every axis (10 and 5 on x, y; 12
+    and 6 on y, t; 16 and 8 on x, t) and, with 7, the direct transform used
+    for extents without a plan."""
     e, o = make_pair(engine_mod, oracle_mod, L, N, zm=True, fa=True, alpha=alpha, start=77)
     rng = oracle_mod.Rand55(3)
     for s in range(3):
