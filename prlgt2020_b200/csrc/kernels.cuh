@@ -323,31 +323,23 @@ __device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, doub
 constexpr int SWEEP_THREADS = NSPT_SWEEP_THREADS;
 constexpr int SWEEP_SLOTS = 3;
 
-// Slot products shared by the sweeps' staple chains (one copy of the
-// product code each, not one per call site), in the paired-run form where
-// the order count fits it (series.cuh).
+// Slot products of the sweeps' staple chains, through the kernel's one
+// out-of-line product (slot_product, series.cuh).
 // T <- T Y, in place
 template <int MOx = MO>
-__device__ __noinline__ void slot_mul(double2 *T, const double2 *Y, int N, const Lane &L) {
+__device__ __forceinline__ void slot_mul(double2 *T, const double2 *Y, int N, const Lane &L) {
   const double2 a0 = T[0], b0 = Y[0];
-  const int c = L.c;
-  product_any<MOx, false>(LeftS{T}, a0, Y, b0, N, L,
-                          [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+  slot_product<MOx>(T, T, a0, Y, b0, N, L, SLOT_SET, nullptr, 0.0, 1);
   if (L.j == 0) T[0] = flag_mul(a0, b0);
   __syncwarp(L.mask);
 }
 
 // Wacc (+)= T Y; first: Wacc = T Y.  Returns the product's flag.
 template <int MOx = MO>
-__device__ __noinline__ double2 slot_acc(double2 *Wacc, const double2 *T, const double2 *Y,
-                                        bool first, int N, const Lane &L) {
+__device__ __forceinline__ double2 slot_acc(double2 *Wacc, const double2 *T, const double2 *Y,
+                                           bool first, int N, const Lane &L) {
   const double2 a0 = T[0], b0 = Y[0];
-  const int c = L.c;
-  product_any<MOx, false>(LeftS{T}, a0, Y, b0, N, L, [&](int k, int r, double2 v) {
-    double2 &w = Wacc[sidx(k, r, c)];
-    w = first ? v : cadd(w, v);
-  });
-  __syncwarp(L.mask);
+  slot_product<MOx>(Wacc, T, a0, Y, b0, N, L, first ? SLOT_SET : SLOT_ADD, nullptr, 0.0, 1);
   return flag_mul(a0, b0);
 }
 

@@ -349,8 +349,7 @@ __device__ __forceinline__ void product_pr(const Left &A, double2 a0, const doub
   __syncwarp(L.mask);
 }
 
-// product() or, where M fits, product_pr(): for the out-of-line slot
-// helpers, which hold one copy of each.
+// product() or, where M fits, product_pr()
 template <int MO, bool DA, class Left, class Emit>
 __device__ __forceinline__ void product_any(const Left &A, double2 a0, const double2 *B, double2 b0,
                                             int M, const Lane &L, Emit emit, int i0 = 1) {
@@ -366,36 +365,52 @@ __device__ __forceinline__ void product_any(const Left &A, double2 a0, const dou
   product<MO, DA>(A, a0, B, b0, M, L, emit, i0);
 }
 
-// out <- A B, orders 1..M, with a0 and b0 taken as the operands' flags
-// (out may be A or B: the products work in place); the result's flag is
-// the caller's
+// What slot_product does with each result coefficient v of (k, r, c).
+enum SlotMode {
+  SLOT_SET = 0,    // out = v
+  SLOT_ADD = 1,    // out += v
+  SLOT_HORNER = 2  // out = v + cx X  (a Horner step of ser_poly2)
+};
+
+// The one out-of-line copy of the series product that every slot product
+// of a kernel goes through (staple chains, U W, exp U, the exp/log Horner
+// steps): out <op>= A B, orders 1..M, with a0 and b0 taken as the
+// operands' flags; out may be A or B (the products work in place).  One
+// copy of each form keeps the kernels' hot code small: warps of an SM run
+// different products at the same time, and a product is a few thousand
+// instructions long.  i0: as product()'s.  The result's flag is the
+// caller's.
 template <int MO>
-__device__ __noinline__ void slot_mul_to(double2 *out, const double2 *A, double2 a0,
-                                         const double2 *B, double2 b0, int M, const Lane &L) {
+__device__ __noinline__ void slot_product(double2 *out, const double2 *A, double2 a0,
+                                          const double2 *B, double2 b0, int M, const Lane &L,
+                                          int mode, const double2 *X, double cx, int i0) {
   const int c = L.c;
-#ifdef NSPT_PR_STAPLES_ONLY
-  product<MO, false>(LeftS{A}, a0, B, b0, M, L,
-                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
-#else
   product_any<MO, false>(LeftS{A}, a0, B, b0, M, L,
-                         [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
-#endif
+                         [&](int k, int r, double2 v) {
+                           double2 &o = out[sidx(k, r, c)];
+                           if (mode == SLOT_ADD)
+                             v = cadd(o, v);
+                           else if (mode == SLOT_HORNER)
+                             v = cadd(v, cscale(X[sidx(k, r, c)], cx));
+                           o = v;
+                         },
+                         i0);
   __syncwarp(L.mask);
+}
+
+// out <- A B, orders 1..M, flags a0 and b0 (the result's flag is the caller's)
+template <int MO>
+__device__ __forceinline__ void slot_mul_to(double2 *out, const double2 *A, double2 a0,
+                                            const double2 *B, double2 b0, int M, const Lane &L) {
+  slot_product<MO>(out, A, a0, B, b0, M, L, SLOT_SET, nullptr, 0.0, 1);
 }
 
 // One Horner step of ser_poly2: S <- Y S + cx X, orders 1..M, in place (Y
 // has flag 0 and no order 1; S's flag is sf).  The flag is the caller's.
 template <int MO>
-__device__ __noinline__ void slot_horner(double2 *S, const double2 *Y, double2 sf, const double2 *X,
-                                         double cx, int M, const Lane &L) {
-  const int c = L.c;
-  auto em = [&](int k, int r, double2 v) { S[sidx(k, r, c)] = cadd(v, cscale(X[sidx(k, r, c)], cx)); };
-#ifdef NSPT_PR_STAPLES_ONLY
-  product<MO, false>(LeftS{Y}, cz(), S, sf, M, L, em, 2);
-#else
-  product_any<MO, false>(LeftS{Y}, cz(), S, sf, M, L, em, 2);
-#endif
-  __syncwarp(L.mask);
+__device__ __forceinline__ void slot_horner(double2 *S, const double2 *Y, double2 sf,
+                                            const double2 *X, double cx, int M, const Lane &L) {
+  slot_product<MO>(S, Y, cz(), S, sf, M, L, SLOT_HORNER, X, cx, 2);
 }
 
 // ---------------- compensated float-float Cauchy product ----------------
