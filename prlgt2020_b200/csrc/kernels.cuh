@@ -289,24 +289,22 @@ __device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, doub
     __syncwarp(L.mask);
   }
   // ---- F = exp(W1) * U  (nspt.cc:429): exp into Y (W holds the square of
-  // W1), U_mu(x) restaged into W, the product into T (W1 is spent)
+  // W1), U_mu(x) restaged into W
   ser_exp<MOx>(T, W, Y, N, L);
   stage(W, a.U, a.Uf, mu, self, a.g, N, L);
   const bool zm = a.Lg != nullptr;
-  const double2 fflag = W[0];  // exp(W1) has flag 1
-  slot_mul_to<MOx>(T, Y, make_double2(1.0, 0.0), W, fflag, N, L);
   double2 *Fc = a.F + (size_t)mu * plane_mu + site;
-  for (int k = L.s + 1; k <= N; k += 3) {
-#pragma unroll
-    for (int r = 0; r < 3; r++) Fc[(size_t)(9 * (k - 1) + 3 * r + c) * V] = T[sidx(k, r, c)];
-  }
-  if (L.j == 0) a.Ff[(size_t)mu * V + site] = fflag;
+  product<MOx, false>(LeftS{Y}, make_double2(1.0, 0.0), W, W[0], N, L,
+                     [&](int k, int r, double2 v) {
+                       Fc[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
+                       if (zm) W[sidx(k, r, c)] = v;
+                     });
+  if (L.j == 0) a.Ff[(size_t)mu * V + site] = W[0];
   if (!zm) return;
-  if (L.j == 0) T[0] = fflag;
   __syncwarp(L.mask);
   // ---- MM[mu] += log(F[link])  (nspt.cc:432-439): logs stored per link
   double2 *Lo = a.Lg + (size_t)mu * plane_mu + site;
-  ser_log<MOx>(T, Y, W, N, L, [&](int k, int r, double2 v) {
+  ser_log<MOx>(W, T, Y, N, L, [&](int k, int r, double2 v) {
     Lo[(size_t)(9 * (k - 1) + 3 * r + c) * V] = v;
   });
 }
@@ -323,14 +321,66 @@ __device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, doub
 constexpr int SWEEP_THREADS = NSPT_SWEEP_THREADS;
 constexpr int SWEEP_SLOTS = 3;
 
-// Slot products of the sweeps' staple chains, through the kernel's one
-// out-of-line product (slot_product, series.cuh).
+// Slot products shared by the sweeps' staple chains (one copy of the
+// product code each, not one per call site).  Each exists in two out-of-line
+// forms, product() and, where the order count fits it, product_pr()
+// (series.cuh), so that each form gets its own register allocation; a
+// kernel at a fitting N runs only the second.
+template <int MOx, bool PR>
+__device__ __noinline__ void slot_mul_f(double2 *T, const double2 *Y, int N, const Lane &L) {
+  const double2 a0 = T[0], b0 = Y[0];
+  const int c = L.c;
+  auto emit = [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; };
+  if constexpr (PR)
+    product_pr<PrRun<MOx>::R, false>(LeftS{T}, a0, Y, b0, N, L, emit);
+  else
+    product<MOx, false>(LeftS{T}, a0, Y, b0, N, L, emit);
+  if (L.j == 0) T[0] = flag_mul(a0, b0);
+  __syncwarp(L.mask);
+}
+
+template <int MOx, bool PR, bool FIRST>
+__device__ __noinline__ double2 slot_acc_f(double2 *Wacc, const double2 *T, const double2 *Y,
+                                          int N, const Lane &L) {
+  const double2 a0 = T[0], b0 = Y[0];
+  const int c = L.c;
+  auto emit = [&](int k, int r, double2 v) {
+    double2 &w = Wacc[sidx(k, r, c)];
+    w = FIRST ? v : cadd(w, v);
+  };
+  if constexpr (PR)
+    product_pr<PrRun<MOx>::R, false>(LeftS{T}, a0, Y, b0, N, L, emit);
+  else
+    product<MOx, false>(LeftS{T}, a0, Y, b0, N, L, emit);
+  __syncwarp(L.mask);
+  return flag_mul(a0, b0);
+}
+
+__device__ __forceinline__ bool use_pr(int R, int N) {
+#ifdef NSPT_NO_PAIRED_RUNS
+  return false;
+#else
+  return pr_fits(R, N);
+#endif
+}
+
 // T <- T Y, in place
 template <int MOx = MO>
 __device__ __forceinline__ void slot_mul(double2 *T, const double2 *Y, int N, const Lane &L) {
-  const double2 a0 = T[0], b0 = Y[0];
-  slot_product<MOx>(T, T, a0, Y, b0, N, L, SLOT_SET, nullptr, 0.0, 1);
-  if (L.j == 0) T[0] = flag_mul(a0, b0);
+  if (use_pr(PrRun<MOx>::R, N))
+    slot_mul_f<MOx, true>(T, Y, N, L);
+  else
+    slot_mul_f<MOx, false>(T, Y, N, L);
+}
+
+// out <- A B, orders 1..N (out may be B: the product works in place); the
+// flag is the caller's
+template <int MOx = MO>
+__device__ __noinline__ void slot_mul_to(double2 *out, const double2 *A, const double2 *B, int N,
+                                         const Lane &L) {
+  const int c = L.c;
+  product<MOx, false>(LeftS{A}, A[0], B, B[0], N, L,
+                     [&](int k, int r, double2 v) { out[sidx(k, r, c)] = v; });
   __syncwarp(L.mask);
 }
 
@@ -338,9 +388,13 @@ __device__ __forceinline__ void slot_mul(double2 *T, const double2 *Y, int N, co
 template <int MOx = MO>
 __device__ __forceinline__ double2 slot_acc(double2 *Wacc, const double2 *T, const double2 *Y,
                                            bool first, int N, const Lane &L) {
-  const double2 a0 = T[0], b0 = Y[0];
-  slot_product<MOx>(Wacc, T, a0, Y, b0, N, L, first ? SLOT_SET : SLOT_ADD, nullptr, 0.0, 1);
-  return flag_mul(a0, b0);
+  // the first staple sets the sum, the others add to it: slot_mul_f's
+  // in-place write form and an accumulating one
+  if (use_pr(PrRun<MOx>::R, N))
+    return first ? slot_acc_f<MOx, true, true>(Wacc, T, Y, N, L)
+                 : slot_acc_f<MOx, true, false>(Wacc, T, Y, N, L);
+  return first ? slot_acc_f<MOx, false, true>(Wacc, T, Y, N, L)
+               : slot_acc_f<MOx, false, false>(Wacc, T, Y, N, L);
 }
 
 // LOW: the variant for N <= 3 * MO_LOW: products with MO_LOW orders per lane
@@ -371,6 +425,7 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ?
   const int site = (int)(link - (long)mu * a.g.V);
   int x[4];
   coords(a.g, site, x);
+  const size_t plane_mu = (size_t)9 * N * V;
 
   double2 wflag = cz();
   bool first = true;
@@ -439,11 +494,8 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ?
   // ---- P = U_mu(x) * staples (nspt.cc:392) into T; U_mu(x) in Y
   stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
   const double2 pflag = flag_mul(Y[0], wflag);
-  if constexpr (FF)
-    cprod<FF, MOK, false>(LeftS{Y}, Y[0], W, wflag, N, L, ffe,
-                          [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
-  else
-    slot_mul_to<MOK>(T, Y, Y[0], W, wflag, N, L);
+  cprod<FF, MOK, false>(LeftS{Y}, Y[0], W, wflag, N, L, ffe,
+                     [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
   if (L.j == 0) T[0] = pflag;
   __syncwarp(L.mask);
   // ---- traces (ptSU3::Tr, QCDpt.cc:115-122), norm and Tr U_k (nspt.cc:393-402)
@@ -634,8 +686,8 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
   self.fwd = self.bwd = 0;
   stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
   const double2 pflag = flag_mul(Y[0], wflag), p2flag = flag_mul(Y[0], w2flag);
-  slot_mul_to<MOK>(T, Y, Y[0], W, W[0], N, L);
-  slot_mul_to<MOK>(W2, Y, Y[0], W2, W2[0], N, L);
+  slot_mul_to<MOK>(T, Y, W, N, L);
+  slot_mul_to<MOK>(W2, Y, W2, N, L);
   if (L.j == 0) {
     T[0] = pflag;
     W2[0] = p2flag;
@@ -742,12 +794,14 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
   n.site = site;
   n.fwd = n.bwd = 0;
   stage(X, U, Uf, mu, n, geo, N, L);
-  ser_log<(LOW ? MO_LOW : MO)>(X, Y2, Sc, N, L, [](int, int, double2) {});
+  const int c = L.c;
+  ser_log<(LOW ? MO_LOW : MO)>(X, Y2, Sc, N, L,
+                               [&](int k, int r, double2 v) { Sc[sidx(k, r, c)] = v; });
+  __syncwarp(L.mask);
   ser_reH(Sc, N, L);
   __syncwarp(L.mask);
   ser_exp<(LOW ? MO_LOW : MO)>(Sc, Y2, X, N, L);
   double2 *dst = U + (size_t)mu * 9 * N * V + site;
-  const int c = L.c;
   for (int k = L.s + 1; k <= N; k += 3) {
 #pragma unroll
     for (int r = 0; r < 3; r++) dst[(size_t)(9 * (k - 1) + 3 * r + c) * V] = X[sidx(k, r, c)];
@@ -960,9 +1014,11 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
     __syncwarp(L.mask);
     // E1 = exp(alpha W), E2 = exp(-alpha W), sharing (alpha W)^2
     ser_square<(LOW ? MO_LOW : MO)>(A, Y2, N, L);
-    ser_horner2<(LOW ? MO_LOW : MO)>(A, Y2, E1, N, L, [](int n) { return inv_factorial(n); });
+    ser_horner2<(LOW ? MO_LOW : MO)>(A, Y2, E1, N, L, [](int n) { return inv_factorial(n); },
+                    [&](int k, int rr, double2 v) { E1[sidx(k, rr, c)] = v; });
     ser_horner2<(LOW ? MO_LOW : MO)>(A, Y2, E2, N, L,
-                    [](int n) { return (n & 1) ? -inv_factorial(n) : inv_factorial(n); });
+                    [](int n) { return (n & 1) ? -inv_factorial(n) : inv_factorial(n); },
+                    [&](int k, int rr, double2 v) { E2[sidx(k, rr, c)] = v; });
     if (L.j == 0) E1[0] = E2[0] = one;
     __syncwarp(L.mask);
     for (int mu = 0; mu < 4; mu++) {

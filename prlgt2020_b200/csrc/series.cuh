@@ -209,45 +209,28 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
 // owns column c of two runs: hi = NR - s and lo = s + 1 (NR = 6) or lo = s
 // (NR = 5; none for s = 0).  A run ending at order b takes b - 1 steps
 // (left orders i = 1 .. b-1).  The hi run goes first, padded to rhi R steps
-// (a whole number of R-step blocks) when a lo run follows it; the lo run
-// ends the lane's walk.  A lane's two runs then take (NR + 1) R - 1 or
-// NR R - 1 steps whatever s is: every lane walks the same number of steps
-// and the same straight-line code, without the per-order branches of
-// product().  A step is one left order i and all R orders of the run:
-// acc[q] += A_i w[q], 9 R complex FMAs per lane, where w holds the R right
-// columns B_{a+q-i}[:, c] in registers.  From one step to the next every
-// column moves up one order, so a step loads only one new column; the
-// window is circular (slot (q - u) mod R at step u of an R-step block), so
-// it needs no register moves.  Right columns below order 1 read as zero,
-// which pads the hi run's last steps with exact zero terms; the last R-1
-// steps of the walk (common to all lanes) skip them.  The sum over i runs
-// in the same (ascending) order as in product(), so both forms give the
-// same values.
+// when a lo run follows it; the lo run ends the lane's walk.  A lane's two
+// runs then take (NR + 1) R - 1 or NR R - 1 steps whatever s is: every lane
+// walks the same number of steps through the same code, without the
+// per-order branches of product().  A step is one left order i and all R
+// orders of the run, acc[q] += A_i w[q] (9 R complex FMAs per lane), where w
+// holds the R right columns B_{a+q-i}[:, c] in registers.  From one step to
+// the next every column moves up one order, so a step loads one new column
+// and shifts the others (register moves, issued in the FP64 pipe's idle
+// slots).  The loop is rolled: the product is a few hundred instructions,
+// small enough to share the instruction cache with the rest of a sweep.
+// Right columns below order 1 read as zero, which pads the hi run's last
+// steps with exact zero terms; the last R-1 steps of the walk (common to all
+// lanes) skip them.  The sum over i runs in the same (ascending) order as in
+// product(), so both forms give the same values.
 //
 // In place (the result overwriting A or B): a lane writes its hi run when
-// it moves on to its lo run, at the start of block rhi.  Every lane has then
-// finished the steps before that block (a __syncwarp opens each block), and
-// from there on it reads only left orders above rhi R (A_i, i > rhi R >= the
-// hi run's orders) and right orders below (rhi' - rhi) R + 1 <= (rhi - 1) R
-// (rhi' <= 2 rhi - 1 for the runs here), below the hi run's first order; the
-// lo runs read orders up to 3R and are written after a final __syncwarp.
-template <int R, bool DA, class Left>
-__device__ __forceinline__ void pr_step(const Left &A, int i, int u, int qlo,
-                                        double2 (&acc)[R][3], const double2 (&w)[R][3]) {
-#pragma unroll
-  for (int r = 0; r < 3; r++) {
-    double2 a[3];  // row r of op(A_i): one row at a time keeps registers low
-    A.template row<DA>(i, r, a);
-#pragma unroll
-    for (int q = 0; q < R; q++) {
-      if (q < qlo) continue;
-      const int sl = (q - u + R) % R;
-      cfma(acc[q][r], a[0], w[sl][0]);
-      cfma(acc[q][r], a[1], w[sl][1]);
-      cfma(acc[q][r], a[2], w[sl][2]);
-    }
-  }
-}
+// it moves on to its lo run, at step rhi R.  A __syncwarp every R steps
+// makes every lane finish the steps before it first, and from there on
+// every lane reads only left orders above rhi R and right orders at most
+// (rhi' - rhi) R <= (rhi - 1) R (rhi' <= 2 rhi - 1 for these runs), below
+// the hi run's first order; the lo runs read orders up to 3R and are written
+// after a final __syncwarp.
 
 // column c of order j of a slot; zero below order 1
 __device__ __forceinline__ void pr_col(const double2 *B, int j, int c, double2 (&o)[3]) {
@@ -283,7 +266,8 @@ __device__ __forceinline__ void product_pr(const Left &A, double2 a0, const doub
   const int rhi = NR - s;
   const int alo = (rlo - 1) * R + 1;
   const int ahi = (rhi - 1) * R + 1;
-  const int nblk = rlo + rhi - 1;  // R-step blocks; then the walk's last R-1 steps
+  const int nsteps = (rlo + rhi) * R - 1;      // the same for every lane
+  const int sw = rlo > 0 ? rhi * R : -1;       // step at which the lane moves to its lo run
   const bool fa = !cis0(a0), fb = !cis0(b0);
   // the orders of one run, with the flag terms b0 A_k + a0 B_k
   auto out = [&](int k, const double2(&v3)[3]) {
@@ -312,13 +296,35 @@ __device__ __forceinline__ void product_pr(const Left &A, double2 a0, const doub
     for (int r = 0; r < 3; r++) acc[q][r] = cz();
   int a = ahi;
 #pragma unroll
-  for (int q = 1; q < R; q++) pr_col(B, a + q - 1, c, w[q]);
+  for (int q = 0; q < R - 1; q++) pr_col(B, a + q, c, w[q]);  // shifted up by the first step
   int i = 0;
-  // b == nblk only checks the switch: with rlo == 1 the lo run is just the
-  // final R-1 steps, and the hi run fills every block
-  for (int b = 0; b <= nblk; b++) {
-    __syncwarp(L.mask);
-    if (rlo > 0 && b == rhi) {  // hi run done (padded to rhi blocks): write it, on to lo
+  // acc[q] += A_i w[q] for q >= qlo
+  auto step = [&](int qlo) {
+#pragma unroll
+    for (int r = 0; r < 3; r++) {
+      double2 ar[3];  // row r of op(A_i)
+      A.template row<DA>(i, r, ar);
+#pragma unroll
+      for (int q = 0; q < R; q++) {
+        if (q < qlo) continue;
+        cfma(acc[q][r], ar[0], w[q][0]);
+        cfma(acc[q][r], ar[1], w[q][1]);
+        cfma(acc[q][r], ar[2], w[q][2]);
+      }
+    }
+  };
+  auto shift = [&]() {  // every column up one order, the new one at q = 0
+#pragma unroll
+    for (int q = R - 1; q > 0; q--)
+#pragma unroll
+      for (int r = 0; r < 3; r++) w[q][r] = w[q - 1][r];
+    pr_col(B, a - i, c, w[0]);
+  };
+  const int nfull = nsteps - (R - 1);
+#pragma unroll 1
+  for (int t = 0; t < nfull; t++) {
+    if (t % R == 0) __syncwarp(L.mask);
+    if (t == sw) {  // hi run done (padded to rhi R steps): write it, on to lo
 #pragma unroll
       for (int q = 0; q < R; q++) {
         out(ahi + q, acc[q]);
@@ -328,89 +334,39 @@ __device__ __forceinline__ void product_pr(const Left &A, double2 a0, const doub
       a = alo;
       i = 0;
 #pragma unroll
-      for (int q = 1; q < R; q++) pr_col(B, a + q - 1, c, w[q]);
+      for (int q = 0; q < R - 1; q++) pr_col(B, a + q, c, w[q]);  // shifted up by the first step
     }
-    if (b == nblk) break;
-#pragma unroll
-    for (int u = 0; u < R; u++) {
-      ++i;
-      pr_col(B, a - i, c, w[(R - u) % R]);
-      pr_step<R, DA>(A, i, u, 0, acc, w);
-    }
+    ++i;
+    shift();
+    step(0);
   }
+  // with rlo == 1 the lo run is only these last steps
+  __syncwarp(L.mask);
+  if (nfull == sw) {
 #pragma unroll
+    for (int q = 0; q < R; q++) {
+      out(ahi + q, acc[q]);
+#pragma unroll
+      for (int r = 0; r < 3; r++) acc[q][r] = cz();
+    }
+    a = alo;
+    i = 0;
+#pragma unroll
+    for (int q = 0; q < R - 1; q++) pr_col(B, a + q, c, w[q]);  // shifted up by the first step
+  }
+#pragma unroll 1
   for (int u = 0; u < R - 1; u++) {  // order q of the last run is active while q > u
     ++i;
-    pr_step<R, DA>(A, i, u, u + 1, acc, w);
+#pragma unroll
+    for (int q = R - 1; q > 0; q--)
+#pragma unroll
+      for (int r = 0; r < 3; r++) w[q][r] = w[q - 1][r];
+    step(u + 1);
   }
   __syncwarp(L.mask);
 #pragma unroll
   for (int q = 0; q < R; q++) out(a + q, acc[q]);
   __syncwarp(L.mask);
-}
-
-// product() or, where M fits, product_pr()
-template <int MO, bool DA, class Left, class Emit>
-__device__ __forceinline__ void product_any(const Left &A, double2 a0, const double2 *B, double2 b0,
-                                            int M, const Lane &L, Emit emit, int i0 = 1) {
-  constexpr int R = PrRun<MO>::R;
-#ifndef NSPT_NO_PAIRED_RUNS
-  if constexpr (R > 0) {
-    if (pr_fits(R, M)) {
-      product_pr<R, DA>(A, a0, B, b0, M, L, emit);
-      return;
-    }
-  }
-#endif
-  product<MO, DA>(A, a0, B, b0, M, L, emit, i0);
-}
-
-// What slot_product does with each result coefficient v of (k, r, c).
-enum SlotMode {
-  SLOT_SET = 0,    // out = v
-  SLOT_ADD = 1,    // out += v
-  SLOT_HORNER = 2  // out = v + cx X  (a Horner step of ser_poly2)
-};
-
-// The one out-of-line copy of the series product that every slot product
-// of a kernel goes through (staple chains, U W, exp U, the exp/log Horner
-// steps): out <op>= A B, orders 1..M, with a0 and b0 taken as the
-// operands' flags; out may be A or B (the products work in place).  One
-// copy of each form keeps the kernels' hot code small: warps of an SM run
-// different products at the same time, and a product is a few thousand
-// instructions long.  i0: as product()'s.  The result's flag is the
-// caller's.
-template <int MO>
-__device__ __noinline__ void slot_product(double2 *out, const double2 *A, double2 a0,
-                                          const double2 *B, double2 b0, int M, const Lane &L,
-                                          int mode, const double2 *X, double cx, int i0) {
-  const int c = L.c;
-  product_any<MO, false>(LeftS{A}, a0, B, b0, M, L,
-                         [&](int k, int r, double2 v) {
-                           double2 &o = out[sidx(k, r, c)];
-                           if (mode == SLOT_ADD)
-                             v = cadd(o, v);
-                           else if (mode == SLOT_HORNER)
-                             v = cadd(v, cscale(X[sidx(k, r, c)], cx));
-                           o = v;
-                         },
-                         i0);
-  __syncwarp(L.mask);
-}
-
-// out <- A B, orders 1..M, flags a0 and b0 (the result's flag is the caller's)
-template <int MO>
-__device__ __forceinline__ void slot_mul_to(double2 *out, const double2 *A, double2 a0,
-                                            const double2 *B, double2 b0, int M, const Lane &L) {
-  slot_product<MO>(out, A, a0, B, b0, M, L, SLOT_SET, nullptr, 0.0, 1);
-}
-
-// One Horner step of ser_poly2: S <- Y S + cx X, orders 1..M, in place (Y
-// has flag 0 and no order 1; S's flag is sf).  The flag is the caller's.
-template <int MO>
-__device__ __forceinline__ void slot_horner(double2 *S, const double2 *Y, double2 sf,
-                                            const double2 *X, double cx, int M, const Lane &L) {
-  slot_product<MO>(S, Y, cz(), S, sf, M, L, SLOT_HORNER, X, cx, 2);
 }
 
 // ---------------- compensated float-float Cauchy product ----------------
@@ -552,20 +508,20 @@ __device__ __forceinline__ void cprod(const Left &A, double2 a0, const double2 *
 // with S_j needed only to order N - 2j (Y^j starts at order 2j).  X^n starts
 // at order n, so this is the same truncated sum as Horner in X, with
 // 1 + N/2 series products of sizes 2, 4, ..., N instead of N products of
-// sizes 1..N (1354 instead of 2300 3x3 products at N = 24).  The result
-// (S_0, flag coef(0)) is left in S.  X, Y and S are slots.
+// sizes 1..N (1354 instead of 2300 3x3 products at N = 24).  The last step
+// goes to last(k, r, v) instead of S.  X, Y and S are slots.
 template <int MO>
 __device__ __forceinline__ void ser_square(const double2 *X, double2 *Y, int N, const Lane &L) {
-  // Y = X X (order 1 comes out as an exact zero); X's flag is not used (the
-  // log passes U, whose flag 1 is the X = U - 1 it leaves out)
-  slot_mul_to<MO>(Y, X, cz(), X, cz(), N, L);
+  const int c = L.c;
+  // Y = X X (order 1 comes out as an exact zero)
+  product<MO, false>(LeftS{X}, cz(), X, cz(), N, L,
+                     [&](int k, int r, double2 v) { Y[sidx(k, r, c)] = v; });
 }
 
-// The Horner part of ser_poly2, for a Y = X^2 already formed: S <- p(X),
-// orders 1..N and flag coef(0).
-template <int MO, class Coef>
+// The Horner part of ser_poly2, for a Y = X^2 already formed.
+template <int MO, class Coef, class Last>
 __device__ __forceinline__ void ser_horner2(const double2 *X, const double2 *Y, double2 *S, int N,
-                                            const Lane &L, Coef coef) {
+                                            const Lane &L, Coef coef, Last last) {
   const int c = L.c;
   const int J = N / 2;
   // S_J = coef(2J) + coef(2J+1) X to order N - 2J; higher orders zero (they
@@ -580,20 +536,40 @@ __device__ __forceinline__ void ser_horner2(const double2 *X, const double2 *Y, 
     if (L.j == 0) S[0] = make_double2(coef(2 * J), 0.0);
     __syncwarp(L.mask);
   }
-  // Y = X^2 has no order 1 (X has flag 0): the products start at Y's order 2
-  for (int j = J - 1; j >= 0; --j) {
-    const double2 sf = S[0];
-    slot_horner<MO>(S, Y, sf, X, coef(2 * j + 1), N - 2 * j, L);
-    if (L.j == 0) S[0] = make_double2(coef(2 * j), 0.0);
+  if (J == 0) {  // N = 1: S_0 is the result
+    for (int k = L.s + 1; k <= N; k += 3) {
+#pragma unroll
+      for (int r = 0; r < 3; r++) last(k, r, S[sidx(k, r, c)]);
+    }
     __syncwarp(L.mask);
+    return;
+  }
+  // Y = X^2 has no order 1 (X has flag 0): the products start at Y's order 2
+  const LeftS Yl{Y};
+  for (int j = J - 1; j >= 0; --j) {
+    const int M = N - 2 * j;
+    const double2 sf = S[0];
+    const double cx = coef(2 * j + 1);
+    if (j > 0) {
+      product<MO, false>(
+          Yl, cz(), S, sf, M, L,
+          [&](int k, int r, double2 v) { S[sidx(k, r, c)] = cadd(v, cscale(X[sidx(k, r, c)], cx)); },
+          2);
+      if (L.j == 0) S[0] = make_double2(coef(2 * j), 0.0);
+      __syncwarp(L.mask);
+    } else {
+      product<MO, false>(
+          Yl, cz(), S, sf, M, L,
+          [&](int k, int r, double2 v) { last(k, r, cadd(v, cscale(X[sidx(k, r, c)], cx))); }, 2);
+    }
   }
 }
 
-template <int MO, class Coef>
+template <int MO, class Coef, class Last>
 __device__ __forceinline__ void ser_poly2(const double2 *X, double2 *Y, double2 *S, int N,
-                                          const Lane &L, Coef coef) {
+                                          const Lane &L, Coef coef, Last last) {
   ser_square<MO>(X, Y, N, L);
-  ser_horner2<MO>(X, Y, S, N, L, coef);
+  ser_horner2<MO>(X, Y, S, N, L, coef, last);
 }
 
 __device__ __forceinline__ double inv_factorial(int n) {
@@ -607,24 +583,21 @@ __device__ __forceinline__ double inv_factorial(int n) {
 template <int MO>
 __device__ __forceinline__ void ser_exp(const double2 *P, double2 *Y, double2 *R, int N,
                                         const Lane &L) {
-  ser_poly2<MO>(P, Y, R, N, L, [](int n) { return inv_factorial(n); });
+  const int c = L.c;
+  ser_poly2<MO>(P, Y, R, N, L, [](int n) { return inv_factorial(n); },
+                [&](int k, int r, double2 v) { R[sidx(k, r, c)] = v; });
+  if (L.j == 0) R[0] = make_double2(1.0, 0.0);
+  __syncwarp(L.mask);
 }
 
 // log(U) for U with flag 1 (log(const ptSU3&), QCDpt.h:176-198): with
 // X = U - 1, sum_{n<=N} (-1)^{n+1} X^n / n, flag 0.  U, Y and Sc are slots
-// (Y scratch); the result is left in Sc, and emit(k, r, v) receives
-// log_k[r][c] from it.
+// (Y, Sc scratch); emit(k, r, v) receives log_k[r][c].
 template <int MO, class Emit>
 __device__ __forceinline__ void ser_log(const double2 *U, double2 *Y, double2 *Sc, int N,
                                         const Lane &L, Emit emit) {
   ser_poly2<MO>(U, Y, Sc, N, L,
-                [](int n) { return n == 0 ? 0.0 : ((n & 1) ? 1.0 : -1.0) / (double)n; });
-  const int c = L.c;
-  for (int k = L.s + 1; k <= N; k += 3) {
-#pragma unroll
-    for (int r = 0; r < 3; r++) emit(k, r, Sc[sidx(k, r, c)]);
-  }
-  __syncwarp(L.mask);
+                [](int n) { return n == 0 ? 0.0 : ((n & 1) ? 1.0 : -1.0) / (double)n; }, emit);
 }
 
 // reH on a slot (ptSU3::reH, QCDpt.cc:197-209): per order (M - M^dag)/2
