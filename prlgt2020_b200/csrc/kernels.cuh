@@ -30,6 +30,7 @@ struct Geo {
   int V;
   int s0, s1, s2;  // site strides of directions 0, 1, 2 (direction 3: 1)
   unsigned twist;  // bit d: direction d twisted
+  int t0, t1;      // the sweep's site tiles: t0 x t1 sites in directions 0, 1 (sweep_link)
 };
 
 
@@ -249,6 +250,32 @@ __device__ __forceinline__ long group_unit(int g, long nunits, bool &valid) {
   return valid ? u : nunits - 1;
 }
 
+// Link (mu, site) of the sweep's unit u.  Units run tile by tile, a tile
+// being t0 x t1 sites in directions 0 and 1 times the whole planes of
+// directions 2 and 3; inside a tile, all its sites for mu = 0, then mu = 1,
+// ... .  A link's staples read links at +-1 in every direction, and in a
+// plain (mu, site) order the neighbours one step away in direction 0 were
+// last read V / L0 sites earlier, far outside the 126 MB L2 at large
+// volumes; inside a tile they were read t1 L2 L3 sites earlier, and the
+// other mu of the tile within 4 t0 t1 L2 L3 links.  (t0 = t1 = 4: 16K sites
+// per tile at 32^4, about 57 MB of 24-order links per mu pass.)  The link
+// index mu V + site, which the observables and the noise counter use, does
+// not depend on the order.
+__device__ __forceinline__ void sweep_link(const Geo &g, long u, int &mu, int &site) {
+  const long P = (long)g.t0 * g.t1 * g.s1;  // sites per tile
+  const long tile = u / (4 * P);
+  long r = u - tile * 4 * P;
+  mu = (int)(r / P);
+  r -= (long)mu * P;
+  const int nt1 = g.L[1] / g.t1;
+  const int tt0 = (int)(tile / nt1), tt1 = (int)(tile - (long)tt0 * nt1);
+  const int i0 = (int)(r / ((long)g.t1 * g.s1));
+  r -= (long)i0 * g.t1 * g.s1;
+  const int i1 = (int)(r / g.s1);
+  r -= (long)i1 * g.s1;
+  site = (tt0 * g.t0 + i0) * g.s0 + (tt1 * g.t1 + i1) * g.s1 + (int)r;
+}
+
 // The rest of a link update once the force (nspt.cc:392-416) is in slot T and
 // U_mu(x) in slot Y, observables written: W1 = reH(W1) tau_g - stau eta,
 // F = exp(W1) U_mu(x), and the per-link log for the zero modes.  W is a
@@ -322,55 +349,16 @@ constexpr int SWEEP_THREADS = NSPT_SWEEP_THREADS;
 constexpr int SWEEP_SLOTS = 3;
 
 // Slot products shared by the sweeps' staple chains (one copy of the
-// product code each, not one per call site).  Each exists in two out-of-line
-// forms, product() and, where the order count fits it, product_pr()
-// (series.cuh), so that each form gets its own register allocation; a
-// kernel at a fitting N runs only the second.
-template <int MOx, bool PR>
-__device__ __noinline__ void slot_mul_f(double2 *T, const double2 *Y, int N, const Lane &L) {
-  const double2 a0 = T[0], b0 = Y[0];
-  const int c = L.c;
-  auto emit = [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; };
-  if constexpr (PR)
-    product_pr<PrRun<MOx>::R, false>(LeftS{T}, a0, Y, b0, N, L, emit);
-  else
-    product<MOx, false>(LeftS{T}, a0, Y, b0, N, L, emit);
-  if (L.j == 0) T[0] = flag_mul(a0, b0);
-  __syncwarp(L.mask);
-}
-
-template <int MOx, bool PR, bool FIRST>
-__device__ __noinline__ double2 slot_acc_f(double2 *Wacc, const double2 *T, const double2 *Y,
-                                          int N, const Lane &L) {
-  const double2 a0 = T[0], b0 = Y[0];
-  const int c = L.c;
-  auto emit = [&](int k, int r, double2 v) {
-    double2 &w = Wacc[sidx(k, r, c)];
-    w = FIRST ? v : cadd(w, v);
-  };
-  if constexpr (PR)
-    product_pr<PrRun<MOx>::R, false>(LeftS{T}, a0, Y, b0, N, L, emit);
-  else
-    product<MOx, false>(LeftS{T}, a0, Y, b0, N, L, emit);
-  __syncwarp(L.mask);
-  return flag_mul(a0, b0);
-}
-
-__device__ __forceinline__ bool use_pr(int R, int N) {
-#ifdef NSPT_NO_PAIRED_RUNS
-  return false;
-#else
-  return pr_fits(R, N);
-#endif
-}
-
+// product code each, not one per call site).
 // T <- T Y, in place
 template <int MOx = MO>
-__device__ __forceinline__ void slot_mul(double2 *T, const double2 *Y, int N, const Lane &L) {
-  if (use_pr(PrRun<MOx>::R, N))
-    slot_mul_f<MOx, true>(T, Y, N, L);
-  else
-    slot_mul_f<MOx, false>(T, Y, N, L);
+__device__ __noinline__ void slot_mul(double2 *T, const double2 *Y, int N, const Lane &L) {
+  const double2 a0 = T[0], b0 = Y[0];
+  const int c = L.c;
+  product<MOx, false>(LeftS{T}, a0, Y, b0, N, L,
+                     [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+  if (L.j == 0) T[0] = flag_mul(a0, b0);
+  __syncwarp(L.mask);
 }
 
 // out <- A B, orders 1..N (out may be B: the product works in place); the
@@ -386,15 +374,16 @@ __device__ __noinline__ void slot_mul_to(double2 *out, const double2 *A, const d
 
 // Wacc (+)= T Y; first: Wacc = T Y.  Returns the product's flag.
 template <int MOx = MO>
-__device__ __forceinline__ double2 slot_acc(double2 *Wacc, const double2 *T, const double2 *Y,
-                                           bool first, int N, const Lane &L) {
-  // the first staple sets the sum, the others add to it: slot_mul_f's
-  // in-place write form and an accumulating one
-  if (use_pr(PrRun<MOx>::R, N))
-    return first ? slot_acc_f<MOx, true, true>(Wacc, T, Y, N, L)
-                 : slot_acc_f<MOx, true, false>(Wacc, T, Y, N, L);
-  return first ? slot_acc_f<MOx, false, true>(Wacc, T, Y, N, L)
-               : slot_acc_f<MOx, false, false>(Wacc, T, Y, N, L);
+__device__ __noinline__ double2 slot_acc(double2 *Wacc, const double2 *T, const double2 *Y,
+                                        bool first, int N, const Lane &L) {
+  const double2 a0 = T[0], b0 = Y[0];
+  const int c = L.c;
+  product<MOx, false>(LeftS{T}, a0, Y, b0, N, L, [&](int k, int r, double2 v) {
+    double2 &w = Wacc[sidx(k, r, c)];
+    w = first ? v : cadd(w, v);
+  });
+  __syncwarp(L.mask);
+  return flag_mul(a0, b0);
 }
 
 // LOW: the variant for N <= 3 * MO_LOW: products with MO_LOW orders per lane
@@ -419,10 +408,11 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ?
   double2 *T = sm + (size_t)(warp * LPW + g) * (SWEEP_SLOTS * SS), *Y = T + SS;
   double2 *W = Y + SS;
   bool valid;
-  const long link = group_unit(g, 4L * a.g.V, valid);
+  const long unit = group_unit(g, 4L * a.g.V, valid);
   if (!valid) return;  // groups are independent: a group past the end has no work
-  const int mu = (int)(link / a.g.V);
-  const int site = (int)(link - (long)mu * a.g.V);
+  int mu, site;
+  sweep_link(a.g, unit, mu, site);
+  const long link = (long)mu * a.g.V + site;
   int x[4];
   coords(a.g, site, x);
   const size_t plane_mu = (size_t)9 * N * V;

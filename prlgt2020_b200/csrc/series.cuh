@@ -124,12 +124,6 @@ struct LeftS {
 #pragma unroll
     for (int r = 0; r < 3; r++) o[r] = DAG ? cconj(s[sidx(k, c, r)]) : s[sidx(k, r, c)];
   }
-  // row r of order k
-  template <bool DAG>
-  __device__ __forceinline__ void row(int k, int r, double2 *o) const {
-#pragma unroll
-    for (int l = 0; l < 3; l++) o[l] = DAG ? cconj(s[sidx(k, l, r)]) : s[sidx(k, r, l)];
-  }
 };
 
 // C = op(A) * B, orders 1..M (truncated Cauchy product, ptSU3::operator*,
@@ -199,174 +193,6 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
     }
     __syncwarp(L.mask);
   }
-}
-
-// ---------------- paired-run form of the same product ----------------
-//
-// For M = NR * R result orders with NR in {5, 6} (R set by the caller's
-// orders-per-lane budget), the triangle is cut into NR runs of R consecutive
-// orders, run r holding orders (r-1)R+1 .. rR.  Lane (c, s) of the group
-// owns column c of two runs: hi = NR - s and lo = s + 1 (NR = 6) or lo = s
-// (NR = 5; none for s = 0).  A run ending at order b takes b - 1 steps
-// (left orders i = 1 .. b-1).  The hi run goes first, padded to rhi R steps
-// when a lo run follows it; the lo run ends the lane's walk.  A lane's two
-// runs then take (NR + 1) R - 1 or NR R - 1 steps whatever s is: every lane
-// walks the same number of steps through the same code, without the
-// per-order branches of product().  A step is one left order i and all R
-// orders of the run, acc[q] += A_i w[q] (9 R complex FMAs per lane), where w
-// holds the R right columns B_{a+q-i}[:, c] in registers.  From one step to
-// the next every column moves up one order, so a step loads one new column
-// and shifts the others (register moves, issued in the FP64 pipe's idle
-// slots).  The loop is rolled: the product is a few hundred instructions,
-// small enough to share the instruction cache with the rest of a sweep.
-// Right columns below order 1 read as zero, which pads the hi run's last
-// steps with exact zero terms; the last R-1 steps of the walk (common to all
-// lanes) skip them.  The sum over i runs in the same (ascending) order as in
-// product(), so both forms give the same values.
-//
-// In place (the result overwriting A or B): a lane writes its hi run when
-// it moves on to its lo run, at step rhi R.  A __syncwarp every R steps
-// makes every lane finish the steps before it first, and from there on
-// every lane reads only left orders above rhi R and right orders at most
-// (rhi' - rhi) R <= (rhi - 1) R (rhi' <= 2 rhi - 1 for these runs), below
-// the hi run's first order; the lo runs read orders up to 3R and are written
-// after a final __syncwarp.
-
-// column c of order j of a slot; zero below order 1
-__device__ __forceinline__ void pr_col(const double2 *B, int j, int c, double2 (&o)[3]) {
-  if (j >= 1) {
-    const double2 *bj = B + 1 + 9 * (j - 1) + 3 * c;
-    o[0] = bj[0];
-    o[1] = bj[1];
-    o[2] = bj[2];
-  } else {
-    o[0] = o[1] = o[2] = cz();
-  }
-}
-
-__device__ __forceinline__ bool pr_fits(int R, int M) {
-  return R > 0 && (M == 5 * R || M == 6 * R);
-}
-
-// Run length of the paired-run form for a kernel built for MO orders per
-// lane and pass (0: not used).
-template <int MO>
-struct PrRun {
-  static constexpr int R = MO >= 8 ? 4 : (MO >= 4 ? 2 : 0);
-};
-
-// C = op(A) * B, orders 1..M, M = NR R with NR in {5, 6}: product()'s
-// result and interface (no i0: a zero left order adds exact zeros).
-template <int R, bool DA, class Left, class Emit>
-__device__ __forceinline__ void product_pr(const Left &A, double2 a0, const double2 *B, double2 b0,
-                                           int M, const Lane &L, Emit emit) {
-  const int c = L.c, s = L.s;
-  const int NR = M / R;
-  const int rlo = (NR == 6) ? s + 1 : s;  // 0: no lo run
-  const int rhi = NR - s;
-  const int alo = (rlo - 1) * R + 1;
-  const int ahi = (rhi - 1) * R + 1;
-  const int nsteps = (rlo + rhi) * R - 1;      // the same for every lane
-  const int sw = rlo > 0 ? rhi * R : -1;       // step at which the lane moves to its lo run
-  const bool fa = !cis0(a0), fb = !cis0(b0);
-  // the orders of one run, with the flag terms b0 A_k + a0 B_k
-  auto out = [&](int k, const double2(&v3)[3]) {
-    double2 ak[3];
-    if (fb) A.template col<DA>(k, c, ak);
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-      double2 v = v3[r];
-      if (fa || fb) {
-        double2 t;
-        if (!fa)
-          t = cmul(b0, ak[r]);
-        else if (!fb)
-          t = cmul(a0, B[sidx(k, r, c)]);
-        else
-          t = cadd(cmul(b0, ak[r]), cmul(a0, B[sidx(k, r, c)]));
-        v = cadd(v, t);
-      }
-      emit(k, r, v);
-    }
-  };
-  double2 acc[R][3], w[R][3];
-#pragma unroll
-  for (int q = 0; q < R; q++)
-#pragma unroll
-    for (int r = 0; r < 3; r++) acc[q][r] = cz();
-  int a = ahi;
-#pragma unroll
-  for (int q = 0; q < R - 1; q++) pr_col(B, a + q, c, w[q]);  // shifted up by the first step
-  int i = 0;
-  // acc[q] += A_i w[q] for q >= qlo
-  auto step = [&](int qlo) {
-#pragma unroll
-    for (int r = 0; r < 3; r++) {
-      double2 ar[3];  // row r of op(A_i)
-      A.template row<DA>(i, r, ar);
-#pragma unroll
-      for (int q = 0; q < R; q++) {
-        if (q < qlo) continue;
-        cfma(acc[q][r], ar[0], w[q][0]);
-        cfma(acc[q][r], ar[1], w[q][1]);
-        cfma(acc[q][r], ar[2], w[q][2]);
-      }
-    }
-  };
-  auto shift = [&]() {  // every column up one order, the new one at q = 0
-#pragma unroll
-    for (int q = R - 1; q > 0; q--)
-#pragma unroll
-      for (int r = 0; r < 3; r++) w[q][r] = w[q - 1][r];
-    pr_col(B, a - i, c, w[0]);
-  };
-  const int nfull = nsteps - (R - 1);
-#pragma unroll 1
-  for (int t = 0; t < nfull; t++) {
-    if (t % R == 0) __syncwarp(L.mask);
-    if (t == sw) {  // hi run done (padded to rhi R steps): write it, on to lo
-#pragma unroll
-      for (int q = 0; q < R; q++) {
-        out(ahi + q, acc[q]);
-#pragma unroll
-        for (int r = 0; r < 3; r++) acc[q][r] = cz();
-      }
-      a = alo;
-      i = 0;
-#pragma unroll
-      for (int q = 0; q < R - 1; q++) pr_col(B, a + q, c, w[q]);  // shifted up by the first step
-    }
-    ++i;
-    shift();
-    step(0);
-  }
-  // with rlo == 1 the lo run is only these last steps
-  __syncwarp(L.mask);
-  if (nfull == sw) {
-#pragma unroll
-    for (int q = 0; q < R; q++) {
-      out(ahi + q, acc[q]);
-#pragma unroll
-      for (int r = 0; r < 3; r++) acc[q][r] = cz();
-    }
-    a = alo;
-    i = 0;
-#pragma unroll
-    for (int q = 0; q < R - 1; q++) pr_col(B, a + q, c, w[q]);  // shifted up by the first step
-  }
-#pragma unroll 1
-  for (int u = 0; u < R - 1; u++) {  // order q of the last run is active while q > u
-    ++i;
-#pragma unroll
-    for (int q = R - 1; q > 0; q--)
-#pragma unroll
-      for (int r = 0; r < 3; r++) w[q][r] = w[q - 1][r];
-    step(u + 1);
-  }
-  __syncwarp(L.mask);
-#pragma unroll
-  for (int q = 0; q < R; q++) out(a + q, acc[q]);
-  __syncwarp(L.mask);
 }
 
 // ---------------- compensated float-float Cauchy product ----------------
