@@ -119,16 +119,39 @@ def dist_setup():
     return world_info()
 
 
-def read_profile_traffic():
-    """Per-launch DRAM bytes of the sweep kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "sweep_32x4_n24_traffic.txt")
+def read_profile_value(key: str, path: str = "profiles/sweep_32x4_n24_traffic.txt"):
+    """A per-launch figure of the sweep kernel from a committed ncu summary
+    (`key: value` lines)."""
     try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
+        for line in open(os.path.join(ROOT, path)):
+            if line.startswith(key + ":"):
                 return float(line.split(":", 1)[1])
     except OSError:
         pass
     return None
+
+
+def read_profile_traffic():
+    """DRAM bytes (read + write) of one 32^4 x 24 sweep-kernel launch, from
+    the committed ncu summary (a 16^4 capture scaled by the link count)."""
+    return read_profile_value("traffic_bytes_per_launch")
+
+
+def executed_fraction(N: int, V: int, kernel_ms: float, peak: float):
+    """The FP64 rate the sweep kernel executes (not the canonical count):
+    DFMA thread instructions per link from the committed ncu summary of the
+    benchmark kernel (profiles/k_sweep_16x16x16x8_n24_full.md, key
+    dfma_thread_inst_per_link) x 2 flops x the 4V links of this sweep, over
+    the kernel time measured here.  Only for the 24-order benchmark shape."""
+    per_link = read_profile_value("dfma_thread_inst_per_link",
+                                  "profiles/k_sweep_16x16x16x8_n24_full.md")
+    if per_link is None or N != 24:
+        return None
+    tflops = per_link * 2.0 * 4 * V / (kernel_ms * 1e-3) / 1e12
+    return {"achieved": tflops, "frac": tflops / peak, "unit": "TFLOP/s",
+            "source": "DFMA thread instructions per link: ncu smsp__sass_thread_inst_executed_"
+                      "op_dfma_pred_on.sum of one launch at 16x16x16x8 x 24 orders "
+                      "(profiles/k_sweep_16x16x16x8_n24_full.md)"}
 
 
 def host_cpu() -> dict:
@@ -359,10 +382,14 @@ def run_ours(args, world, rank, local):
                        "parallelism": "replicas" if world > 1 else "single"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": read_profile_traffic(),
+                         "traffic_source": "profiles/sweep_32x4_n24_traffic.txt: ncu dram__bytes_read.sum "
+                                           "+ dram__bytes_write.sum of one k_sweep launch at 16^4 x 24, "
+                                           "scaled x16 (links) to 32^4; not measured in this run",
                          "kernel": "k_sweep", "kernel_ms": kernel_ms,
                          "peak_source": "FP64 FMA microbenchmark on this GPU "
                                         "(nspt_measure_fp64_peak); MEASURED_PEAKS.json has no FP64 entry",
                          "flops_per_sweep": flops,
+                         "executed": executed_fraction(N, V, kernel_ms, peak),
                          "algorithmic_bytes_per_sweep": algorithmic_bytes_per_sweep(V, N),
                          "hbm_gbs_equiv": algorithmic_bytes_per_sweep(V, N) / (ms_step * 1e-3) / 1e9},
             "clocks": clocks,
