@@ -850,6 +850,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-gf", action="store_true", help="skip the gauge-fixing figure")
+    ap.add_argument("--c4-therm", type=int, default=600,
+                    help="c4: thermalisation steps before the dt -> 0 measurement")
+    ap.add_argument("--c4-meas", type=int, default=600,
+                    help="c4: measured steps (plaquette read every 2nd) for dt -> 0")
     ap.add_argument("--workload", default="sweep", choices=["sweep", "c2", "c4", "c5", "imp", "loops", "qcfg"],
                     help="sweep: 32^4 x 24 twisted (the headline); c2: 16^4 x 20 periodic "
                          "with zero modes and FA gauge fixing every step, per pass; c4: 64 "

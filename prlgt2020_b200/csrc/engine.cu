@@ -49,6 +49,8 @@ struct nspt_ctx {
   int SS;  // slot stride (double2)
   double2 *U, *Uf, *F, *Ff;
   double2 *Lg;       // per-link logs (zero modes, FA)
+  bool lg_current;   // Lg holds log U of the current field (after a sweep with
+                     // zero modes and after the zero-mode subtraction)
   double2 *Wg, *Gx;  // FA work planes
   double2 *obs_tr, *obs_tru;
   double *obs_norm;
@@ -284,6 +286,7 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   std::swap(ctx->Uf, ctx->Ff);
   ctx->counter++;
   ctx->have_obs = true;
+  ctx->lg_current = a.Lg != nullptr;  // the sweep stored log U' per link
   return NSPT_OK;
 }
 
@@ -295,12 +298,12 @@ static int do_zero_modes(nspt_ctx *ctx) {
   CK(cudaGetLastError());
   const long nl = 4 * ctx->V;
   double2 *U = ctx->U, *Uf = ctx->Uf;
-  const double2 *Lg = ctx->Lg;
+  double2 *Lg = ctx->Lg;
   const int SS = ctx->SS;
   const Geo geo = ctx->geo;
   cudaStream_t st = ctx->st;
   const bool low = use_low(ctx);
-  return launch_groups(
+  const int rc = launch_groups(
       ctx, low ? (const void *)k_zero_modes<true> : (const void *)k_zero_modes<false>, 3, nl,
       [&](unsigned g, dim3 b, size_t sm) {
         if (low)
@@ -309,6 +312,8 @@ static int do_zero_modes(nspt_ctx *ctx) {
           k_zero_modes<false><<<g, b, sm, st>>>(U, Uf, Lg, MM, N, SS, geo);
       },
       "zero modes", 0, low);
+  if (rc == NSPT_OK) ctx->lg_current = true;  // Lg = the new field's log
+  return rc;
 }
 
 static int fft4d(nspt_ctx *ctx, double2 *data, int sign) {
@@ -419,7 +424,11 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
   double2 *U = ctx->U, *Uf = ctx->Uf, *F = ctx->F, *Ff = ctx->Ff, *Lg = ctx->Lg, *Wg = ctx->Wg,
           *Gx = ctx->Gx;
   const bool low = use_low(ctx);
-  int rc = launch_groups(
+  // log U per link (nspt.cc:874-875); after the zero-mode subtraction Lg
+  // already holds it (k_zero_modes)
+  int rc = NSPT_OK;
+  if (!ctx->lg_current) {
+    rc = launch_groups(
       ctx, low ? (const void *)k_log_links<true> : (const void *)k_log_links<false>, 3, nl,
       [&](unsigned g, dim3 b, size_t sm) {
         if (low)
@@ -428,7 +437,8 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
           k_log_links<false><<<g, b, sm, st>>>(U, Uf, Lg, N, SS, geo);
       },
       "FA logs", 0, low);
-  if (rc) return rc;
+    if (rc) return rc;
+  }
   rc = fa_fft_fused(ctx, alpha);
   if (rc == NSPT_ERR_ARG) {  // an extent without a compile-time FFT plan
     const size_t tot = (size_t)9 * N * ctx->V;
@@ -464,6 +474,7 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
   if (rc) return rc;
   std::swap(ctx->U, ctx->F);
   std::swap(ctx->Uf, ctx->Ff);
+  ctx->lg_current = false;
   return NSPT_OK;
 }
 
@@ -492,6 +503,7 @@ static int do_local_gf(nspt_ctx *ctx, double alpha) {
   cudaStream_t st = ctx->st;
   double2 *U = ctx->U, *Uf = ctx->Uf;
   const bool low = use_low(ctx);
+  ctx->lg_current = false;
   for (long p = 0; p < steps; p++) {
     int rc = launch_groups(
         ctx, low ? (const void *)k_local_gf<true> : (const void *)k_local_gf<false>, 4, gr.nthr,
@@ -612,6 +624,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->dcounter = nullptr;
   ctx->sweep_warps = 0;
   ctx->shape_mo = 0;
+  ctx->lg_current = false;
   ctx->launch_gen = 0;
   ctx->loop_part = nullptr;
   ctx->loop_part_n = 0;
@@ -728,6 +741,7 @@ extern "C" size_t nspt_device_bytes(const nspt_ctx *ctx) { return ctx ? ctx->byt
 
 extern "C" int nspt_cold_start(nspt_ctx *ctx) {
   if (!ctx) return NSPT_ERR_ARG;
+  ctx->lg_current = false;
   const size_t nU = (size_t)4 * 9 * ctx->N * ctx->V, nF = (size_t)4 * ctx->V;
   k_cold<<<ctx->nsm * 8, 256, 0, ctx->st>>>(ctx->U, ctx->Uf, nU, nF);
   CK(cudaGetLastError());
@@ -739,6 +753,7 @@ static const size_t kChunkBytes = 64u << 20;
 
 extern "C" int nspt_upload_links(nspt_ctx *ctx, const void *aos, int A) {
   if (!ctx || !aos || A < ctx->N) return NSPT_ERR_ARG;
+  ctx->lg_current = false;
   const size_t per_site = (size_t)4 * (1 + 9 * A) * sizeof(double2);
   const int cs = (int)std::max<size_t>(1, std::min<size_t>(kChunkBytes / per_site, ctx->V));
   double2 *buf = nullptr;

@@ -723,10 +723,14 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
 __global__ void k_inc(unsigned long long *c) { *c += 1ull; }
 
 // U = exp(reH(log U - MM[mu]/V)) per link: zero_modes_subtraction,
-// nspt.cc:605-654 (log U is the per-link log stored by the sweep).
+// nspt.cc:605-654 (log U is the per-link log stored by the sweep).  The
+// exponent Y = reH(log U - MM/V) goes back into Lg: log(exp(Y)) = Y holds
+// exactly for truncated series (one variable, so the log and exp series
+// invert each other order by order), so Lg then holds log U of the new
+// field, which FA gauge fixing would otherwise recompute (nspt.cc:874-875).
 template <bool LOW = false>
 __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
-    k_zero_modes(double2 *U, double2 *Uf, const double2 *Lg, const double2 *MMs, int N, int SS,
+    k_zero_modes(double2 *U, double2 *Uf, double2 *Lg, const double2 *MMs, int N, int SS,
                  Geo geo) {
   extern __shared__ double2 sm[];
   Lane L;
@@ -757,8 +761,12 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
   __syncwarp(L.mask);
   ser_exp<(LOW ? MO_LOW : MO)>(P, Y2, R, N, L);
   double2 *dst = U + (size_t)mu * 9 * N * V + site;
+  double2 *lg = Lg + (size_t)mu * 9 * N * V + site;
   const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
-  for (int k = 1; k <= N; k++) dst[(size_t)(9 * (k - 1) + L.j) * V] = R[sidx(k, r, c)];
+  for (int k = 1; k <= N; k++) {
+    dst[(size_t)(9 * (k - 1) + L.j) * V] = R[sidx(k, r, c)];
+    lg[(size_t)(9 * (k - 1) + L.j) * V] = P[sidx(k, r, c)];
+  }
   if (L.j == 0) Uf[(size_t)mu * V + site] = make_double2(1.0, 0.0);
 }
 
