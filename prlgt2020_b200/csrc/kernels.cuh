@@ -84,6 +84,28 @@ __device__ __forceinline__ double2 ld_link(const double2 *p) {
   return RW ? __ldcg(p) : __ldg(p);
 }
 
+// The twisted case of stage(): a link read across a twisted face, loaded
+// through registers and turned by the twist matrices.  Out of line: only
+// boundary links take it, and inlined at every staging site its 3x3
+// products would spread the kernels' hot code over many more instruction
+// cache lines.
+template <bool RW>
+__device__ __noinline__ void stage_twisted(double2 *slot, const double2 *src, size_t V, unsigned tb,
+                                           unsigned tf, int N, const Lane &L, bool dag) {
+  for (int k = 1 + L.j; k <= N; k += GROUP) {
+    double2 m[9];
+#pragma unroll
+    for (int e = 0; e < 9; e++) m[e] = ld_link<RW>(src + (size_t)(9 * (k - 1) + e) * V);
+    twist3(m, tb, tf);
+    double2 *p = slot + 1 + 9 * (k - 1);
+#pragma unroll
+    for (int r = 0; r < 3; r++)
+#pragma unroll
+      for (int c = 0; c < 3; c++) p[dag ? 3 * r + c : 3 * c + r] = dag ? cconj(m[3 * r + c]) : m[3 * r + c];
+  }
+  if (L.j == 0) slot[0] = make_double2(1.0, 0.0);
+}
+
 template <bool RW = false>
 __device__ __forceinline__ void stage(double2 *slot, const double2 *U, const double2 *Uf, int mu,
                                       Nb n, const Geo &g, int N, const Lane &L, bool dag = false) {
@@ -115,18 +137,7 @@ __device__ __forceinline__ void stage(double2 *slot, const double2 *U, const dou
       slot[0] = dag ? cconj(f) : f;
     }
   } else {
-    for (int k = 1 + L.j; k <= N; k += GROUP) {
-      double2 m[9];
-#pragma unroll
-      for (int e = 0; e < 9; e++) m[e] = ld_link<RW>(src + (size_t)(9 * (k - 1) + e) * V);
-      twist3(m, tb, tf);
-      double2 *p = slot + 1 + 9 * (k - 1);
-#pragma unroll
-      for (int r = 0; r < 3; r++)
-#pragma unroll
-        for (int c = 0; c < 3; c++) p[dag ? 3 * r + c : 3 * c + r] = dag ? cconj(m[3 * r + c]) : m[3 * r + c];
-    }
-    if (L.j == 0) slot[0] = make_double2(1.0, 0.0);
+    stage_twisted<RW>(slot, src, V, tb, tf, N, L, dag);
   }
   __syncwarp(L.mask);
 }
