@@ -669,6 +669,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   // the sweep's site tiles (sweep_link): 4 x 4 where the extents allow
   g.t0 = L[0] % 4 == 0 ? 4 : L[0] % 2 == 0 ? 2 : 1;
   g.t1 = L[1] % 4 == 0 ? 4 : L[1] % 2 == 0 ? 2 : 1;
+  g.t2 = L[2];
   if (flags & NSPT_TWIST_Y) g.twist |= 2u;
   if (flags & NSPT_TWIST_Z) g.twist |= 4u;
   if (flags & NSPT_TWIST_T) g.twist |= 8u;

@@ -30,7 +30,7 @@ struct Geo {
   int V;
   int s0, s1, s2;  // site strides of directions 0, 1, 2 (direction 3: 1)
   unsigned twist;  // bit d: direction d twisted
-  int t0, t1;      // the sweep's site tiles: t0 x t1 sites in directions 0, 1 (sweep_link)
+  int t0, t1, t2;  // the sweep's site tiles: t0 x t1 x t2 sites in directions 0-2 (sweep_link)
 };
 
 
@@ -84,28 +84,6 @@ __device__ __forceinline__ double2 ld_link(const double2 *p) {
   return RW ? __ldcg(p) : __ldg(p);
 }
 
-// The twisted case of stage(): a link read across a twisted face, loaded
-// through registers and turned by the twist matrices.  Out of line: only
-// boundary links take it, and inlined at every staging site its 3x3
-// products would spread the kernels' hot code over many more instruction
-// cache lines.
-template <bool RW>
-__device__ __noinline__ void stage_twisted(double2 *slot, const double2 *src, size_t V, unsigned tb,
-                                           unsigned tf, int N, const Lane &L, bool dag) {
-  for (int k = 1 + L.j; k <= N; k += GROUP) {
-    double2 m[9];
-#pragma unroll
-    for (int e = 0; e < 9; e++) m[e] = ld_link<RW>(src + (size_t)(9 * (k - 1) + e) * V);
-    twist3(m, tb, tf);
-    double2 *p = slot + 1 + 9 * (k - 1);
-#pragma unroll
-    for (int r = 0; r < 3; r++)
-#pragma unroll
-      for (int c = 0; c < 3; c++) p[dag ? 3 * r + c : 3 * c + r] = dag ? cconj(m[3 * r + c]) : m[3 * r + c];
-  }
-  if (L.j == 0) slot[0] = make_double2(1.0, 0.0);
-}
-
 template <bool RW = false>
 __device__ __forceinline__ void stage(double2 *slot, const double2 *U, const double2 *Uf, int mu,
                                       Nb n, const Geo &g, int N, const Lane &L, bool dag = false) {
@@ -137,7 +115,18 @@ __device__ __forceinline__ void stage(double2 *slot, const double2 *U, const dou
       slot[0] = dag ? cconj(f) : f;
     }
   } else {
-    stage_twisted<RW>(slot, src, V, tb, tf, N, L, dag);
+    for (int k = 1 + L.j; k <= N; k += GROUP) {
+      double2 m[9];
+#pragma unroll
+      for (int e = 0; e < 9; e++) m[e] = ld_link<RW>(src + (size_t)(9 * (k - 1) + e) * V);
+      twist3(m, tb, tf);
+      double2 *p = slot + 1 + 9 * (k - 1);
+#pragma unroll
+      for (int r = 0; r < 3; r++)
+#pragma unroll
+        for (int c = 0; c < 3; c++) p[dag ? 3 * r + c : 3 * c + r] = dag ? cconj(m[3 * r + c]) : m[3 * r + c];
+    }
+    if (L.j == 0) slot[0] = make_double2(1.0, 0.0);
   }
   __syncwarp(L.mask);
 }
@@ -262,29 +251,33 @@ __device__ __forceinline__ long group_unit(int g, long nunits, bool &valid) {
 }
 
 // Link (mu, site) of the sweep's unit u.  Units run tile by tile, a tile
-// being t0 x t1 sites in directions 0 and 1 times the whole planes of
-// directions 2 and 3; inside a tile, all its sites for mu = 0, then mu = 1,
-// ... .  A link's staples read links at +-1 in every direction, and in a
-// plain (mu, site) order the neighbours one step away in direction 0 were
-// last read V / L0 sites earlier, far outside the 126 MB L2 at large
-// volumes; inside a tile they were read t1 L2 L3 sites earlier, and the
-// other mu of the tile within 4 t0 t1 L2 L3 links.  (t0 = t1 = 4: 16K sites
-// per tile at 32^4, about 57 MB of 24-order links per mu pass.)  The link
-// index mu V + site, which the observables and the noise counter use, does
-// not depend on the order.
+// being t0 x t1 x t2 sites in directions 0, 1, 2 times the whole lines of
+// direction 3, tiles ordered with direction 2 fastest; inside a tile, all
+// its sites for mu = 0, then mu = 1, ... .  A link's staples read links at
+// +-1 in every direction.  In a plain (mu, site) order the neighbours one
+// step away in direction 0 were last read V / L0 sites earlier, far outside
+// the 126 MB L2 at large volumes; inside a tile every neighbour was read at
+// most one tile earlier, and the other mu of the tile within the tile.  The
+// link index mu V + site, which the observables and the noise counter use,
+// does not depend on the order.
 __device__ __forceinline__ void sweep_link(const Geo &g, long u, int &mu, int &site) {
-  const long P = (long)g.t0 * g.t1 * g.s1;  // sites per tile
+  const int L3 = g.s2;
+  const long P = (long)g.t0 * g.t1 * g.t2 * L3;  // sites per tile
   const long tile = u / (4 * P);
   long r = u - tile * 4 * P;
   mu = (int)(r / P);
   r -= (long)mu * P;
-  const int nt1 = g.L[1] / g.t1;
-  const int tt0 = (int)(tile / nt1), tt1 = (int)(tile - (long)tt0 * nt1);
-  const int i0 = (int)(r / ((long)g.t1 * g.s1));
-  r -= (long)i0 * g.t1 * g.s1;
-  const int i1 = (int)(r / g.s1);
-  r -= (long)i1 * g.s1;
-  site = (tt0 * g.t0 + i0) * g.s0 + (tt1 * g.t1 + i1) * g.s1 + (int)r;
+  const int nt2 = g.L[2] / g.t2, nt1 = g.L[1] / g.t1;
+  const int tt2 = (int)(tile % nt2);
+  const long tq = tile / nt2;
+  const int tt1 = (int)(tq % nt1), tt0 = (int)(tq / nt1);
+  const int i0 = (int)(r / ((long)g.t1 * g.t2 * L3));
+  r -= (long)i0 * g.t1 * g.t2 * L3;
+  const int i1 = (int)(r / ((long)g.t2 * L3));
+  r -= (long)i1 * g.t2 * L3;
+  const int i2 = (int)(r / L3);
+  const int x3 = (int)(r - (long)i2 * L3);
+  site = (tt0 * g.t0 + i0) * g.s0 + (tt1 * g.t1 + i1) * g.s1 + (tt2 * g.t2 + i2) * g.s2 + x3;
 }
 
 // The rest of a link update once the force (nspt.cc:392-416) is in slot T and

@@ -285,6 +285,7 @@ extern "C" int nspt_plaquette_measure_noalloc(const void *links_dev, int allocOR
   g.s0 = L[1] * g.s1;
   g.V = (int)V;
   g.t0 = g.t1 = 1;
+  g.t2 = L[2];
   g.twist = 0;
   if (flags & NSPT_TWIST_Y) g.twist |= 2u;
   if (flags & NSPT_TWIST_Z) g.twist |= 4u;

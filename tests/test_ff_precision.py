@@ -112,3 +112,42 @@ def test_ff_options_checked(engine_mod):
         d.set_ff_scale(1)
     with pytest.raises(P.NsptError):
         d.ff_scale()
+
+
+def test_ff_error_after_1_100_1000_steps_is_fp64_rounding_sized(engine_mod):
+    """The 24^4 x 40 precision workload's accuracy claim, on 4^4 x 40: from
+    a common field (20 FP64 steps from a cold start), float-float and FP64
+    engines run on with the same noise (zero modes + FA every step, alpha =
+    +0.05), beside a second FP64 run whose dt is larger by one part in 2^52.
+    After 1, 100 and 1000 steps, the float-float per-order deviation from
+    FP64 (max|ff - fp64| / max|fp64| over the order's coefficients) must be
+    within 10x of the deviation that FP64's own rounding-level perturbation
+    produces at that order, plus 1e-14: the float-float products cost no
+    accuracy beyond what an FP64 run has anyway at every order."""
+    P = engine_mod
+    L, N, dt, alpha, warm = (4, 4, 4, 4), 40, 0.01, 0.05, 20
+    kw = dict(zero_modes=True, fa=True, alpha=alpha)
+    with P.NsptEngine(L, N, **kw) as base:
+        base.seed(5150, 0)
+        base.NsptEvolve(dt, warm, 1)
+        start = base.download()
+    ff = P.NsptEngine(L, N, precision="ff", **kw)
+    ref = P.NsptEngine(L, N, **kw)
+    pert = P.NsptEngine(L, N, **kw)
+    for e in (ff, ref, pert):
+        e.upload(start)
+        e.seed(5150, warm)
+    done = 0
+    for m in (1, 100, 1000):
+        ff.NsptEvolve(dt, m - done, 1)
+        ref.NsptEvolve(dt, m - done, 1)
+        pert.NsptEvolve(dt * (1.0 + 2.0 ** -52), m - done, 1)
+        done = m
+        r = ref.download()
+        assert np.isfinite(r).all()
+        e_ff = per_order_rel(ff.download(), r, N)
+        e_64 = per_order_rel(pert.download(), r, N)
+        bad = np.nonzero(e_ff > 10.0 * e_64 + 1e-14)[0]
+        assert bad.size == 0, (m, [(int(k) + 1, float(e_ff[k]), float(e_64[k])) for k in bad])
+    for e in (ff, ref, pert):
+        e.close()
