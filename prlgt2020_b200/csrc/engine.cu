@@ -675,9 +675,9 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   if (flags & NSPT_TWIST_Y) g.twist |= 2u;
   if (flags & NSPT_TWIST_Z) g.twist |= 4u;
   if (flags & NSPT_TWIST_T) g.twist |= 8u;
-  // slot stride = 1 (mod 8) 16-byte quads: see series.cuh on bank quads
+  // slot stride = 3 (mod 8) 16-byte quads: see series.cuh on bank quads
   ctx->SS = 1 + 9 * N;
-  while (ctx->SS % 8 != 1) ctx->SS++;
+  while (ctx->SS % 8 != 3) ctx->SS++;
   // one warp (3 link groups of 3 slots) must fit in a CTA
   if ((size_t)LPW * group_bytes(ctx, SWEEP_SLOTS, 0) > ctx->smem_optin) return fail(NSPT_ERR_ORDER);
   if (ctx->c1 != 0.0 && (size_t)LPW * group_bytes(ctx, IMP_SLOTS, 0) > ctx->smem_optin)

@@ -277,7 +277,7 @@ extern "C" int nspt_plaquette_measure_noalloc(const void *links_dev, int allocOR
   f.A = allocORD;
   f.N = N;
   f.SS = 1 + 9 * N;
-  while (f.SS % 8 != 1) f.SS++;
+  while (f.SS % 8 != 3) f.SS++;  // bank quads: see series.cuh
   Geo &g = f.g;
   for (int k = 0; k < 4; k++) g.L[k] = L[k];
   g.s2 = L[3];

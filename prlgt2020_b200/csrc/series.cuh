@@ -18,9 +18,14 @@
 //     (9 complex) is one broadcast read for the group -- straight from the
 //     global planes (L1/L2, prefetched one order ahead) or from a slot;
 //   * each right column B_j[:,c] (3 complex, one 48-byte column of the slot)
-//     feeds 9 complex FMAs; the 27 lanes of a warp read 27 distinct columns
-//     that fall on distinct bank quads (slot stride = 1 mod 8 quads, column
-//     major, group stride = 3 mod 8 quads).
+//     feeds 9 complex FMAs.  A 128-bit shared load is served a quarter-warp
+//     (8 lanes) at a time, and lane (c, s) of a group reads quad
+//     (j + 3c + r + base) mod 8 of the 8 16-byte bank quads, the 9 lanes of
+//     a group on 9 consecutive quads.  With the slot stride = 3 (mod 8)
+//     quads, the group stride of a 3-slot kernel is = 1 (mod 8): the next
+//     group continues the sequence, and every quarter-warp's 8 lanes land
+//     on 8 distinct quads (4 wavefronts a load; with a slot stride = 1 the
+//     quarters that straddle two groups take 5.2 on average).
 // Accumulators of up to 3*MO orders per pass stay in registers; passes run
 // from high to low order and every lane finishes reading a pass before any
 // lane writes it, so a result may overwrite either operand in place.
