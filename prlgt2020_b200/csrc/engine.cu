@@ -151,7 +151,7 @@ static void sweep_kernel(dim3 grid, dim3 blk, size_t smem, cudaStream_t st, cons
   k_sweep<MEASURE, FF, LOW><<<grid, blk, smem, st>>>(a);
 }
 
-static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
+static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a0, bool measure) {
   const long nl = 4 * ctx->V;
   const bool ff = (ctx->flags & NSPT_PRECISION_FF) != 0;
   // low orders: the lighter variant, two CTAs per SM
@@ -161,10 +161,26 @@ static int launch_sweep(nspt_ctx *ctx, const SweepArgs &a, bool measure) {
                                ctx->sweep_warps > 0 ? std::min(ctx->sweep_warps, max_warps)
                                                     : max_warps,
                                low ? 2 : 1);
-  const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, SWEEP_SLOTS, 0);
-  const long per_cta = (long)k.warps * LPW;
-  const unsigned grid = (unsigned)((nl + per_cta - 1) / per_cta);
-  const dim3 blk(32 * k.warps);
+  int warps = k.warps, gpc = k.warps * LPW;
+  if (!low && ctx->sweep_warps == 0 && k.warps < max_warps) {
+    // shared memory, not the lattice, limits the CTA: as many link groups
+    // as it holds, over all max_warps warps (sweep_group), where that keeps
+    // at least 2.5 groups per warp.  Measured at 32^4 x 24: 22 groups as 8
+    // warps 511 ms, 21 as 7 full warps 538 ms; at 24^4 x 40, 13 groups as 8
+    // warps 732 ms, 12 as 4 full warps 671 ms.
+    const size_t per_group = group_bytes(ctx, SWEEP_SLOTS, 0);
+    const long fit = std::min<long>((long)(ctx->smem_optin / per_group), (long)max_warps * LPW);
+    const long want = (nl + 2L * ctx->nsm - 1) / (2L * ctx->nsm);  // about two CTAs per SM
+    if (fit > gpc && want >= fit && 2 * fit >= 5L * max_warps) {
+      gpc = (int)fit;
+      warps = max_warps;
+    }
+  }
+  SweepArgs a = a0;
+  a.gpc = gpc;
+  const size_t smem = (size_t)gpc * group_bytes(ctx, SWEEP_SLOTS, 0);
+  const unsigned grid = (unsigned)((nl + gpc - 1) / gpc);
+  const dim3 blk(32 * warps);
   if (measure)
     sweep_kernel<true, false>(grid, blk, smem, ctx->st, a);
   else if (ff)

@@ -227,6 +227,8 @@ struct SweepArgs {
   const int *ff_scale;  // float-float products: per-order scale exponent (device)
   double tau_g, stau;  // -dt/6, sqrt(dt)  (Quenched.cc:584-589)
   int N, SS;
+  int gpc;             // link groups per CTA of the sweep, dealt to its warps as evenly
+                       // as possible (sweep_group)
   Geo g;
 };
 
@@ -239,6 +241,22 @@ __device__ __forceinline__ bool make_lane(Lane &L, int &g) {
   L.c = L.j / 3;
   L.s = L.j - 3 * L.c;
   L.mask = ((1u << GROUP) - 1u) << (g * GROUP);
+  return true;
+}
+
+// The sweep's CTA holds gpc link groups, dealt to its warps as evenly as
+// possible (the first gpc mod nw warps take one more): a CTA that shared
+// memory limits to, say, 22 groups runs them as 8 warps of 3 or 2 groups,
+// so that each of the SM's four schedulers has two warps, rather than as 7
+// full warps split 2-2-2-1 over the schedulers.  gi: the group's index in
+// the CTA (its slots and unit).
+__device__ __forceinline__ bool sweep_group(Lane &L, int &gi, int gpc) {
+  int g;
+  if (!make_lane(L, g)) return false;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int base = gpc / nw, extra = gpc - base * nw;
+  if (g >= base + (warp < extra ? 1 : 0)) return false;
+  gi = warp * base + min(warp, extra) + g;
   return true;
 }
 
@@ -404,16 +422,14 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ?
   const int ffe = FF ? *a.ff_scale : 0;
   extern __shared__ double2 sm[];
   Lane L;
-  int g;
-  if (!make_lane(L, g)) return;
-  const int warp = threadIdx.x >> 5;
+  int gi;
+  if (!sweep_group(L, gi, a.gpc)) return;
   const int N = a.N, SS = a.SS, c = L.c;
   const size_t V = (size_t)a.g.V;
-  double2 *T = sm + (size_t)(warp * LPW + g) * (SWEEP_SLOTS * SS), *Y = T + SS;
+  double2 *T = sm + (size_t)gi * (SWEEP_SLOTS * SS), *Y = T + SS;
   double2 *W = Y + SS;
-  bool valid;
-  const long unit = group_unit(g, 4L * a.g.V, valid);
-  if (!valid) return;  // groups are independent: a group past the end has no work
+  const long unit = (long)blockIdx.x * a.gpc + gi;
+  if (unit >= 4L * a.g.V) return;  // groups are independent: a group past the end has no work
   int mu, site;
   sweep_link(a.g, unit, mu, site);
   const long link = (long)mu * a.g.V + site;

@@ -139,13 +139,16 @@ def test_twisted_boundaries(engine_mod, oracle_mod, twist, N):
     assert per_order_rel(e.download(), o.links, N).max() <= 1e-11
 
 
-@pytest.mark.parametrize("L", [(4, 4, 4, 4), (8, 8, 4, 4)])
+@pytest.mark.parametrize("L", [(4, 4, 4, 4), (8, 8, 4, 4), (8, 8, 8, 4)])
 def test_headline_combination_one_sweep(engine_mod, oracle_mod, L):
     """The benchmark's combination -- 24 orders, twisted y and z, dt = 0.005 --
     on lattices with every extent >= 4 (so x + mu and x - mu are distinct
     sites) and, at 8 x 8 x 4 x 4, extents above 4 in a twisted direction.
-    One sweep from a random start: <= 1e-12 per order, flags exact
-    (gauge_wilson nspt.cc:362-439, twist nspt.cc:163-255)."""
+    8 x 8 x 8 x 4 (8192 links) is large enough for the sweep's CTA shape of
+    large lattices (22 link groups over 8 warps, launch_sweep) and for
+    several of its 4 x 4 x 4 site tiles.  One sweep from a random start:
+    <= 1e-12 per order, flags exact (gauge_wilson nspt.cc:362-439, twist
+    nspt.cc:163-255)."""
     N = 24
     e, o = make_pair(engine_mod, oracle_mod, L, N, twist="yz", start=2400 + L[0])
     rng = oracle_mod.Rand55(2424)
