@@ -819,6 +819,7 @@ def run_qcfg(args, world, rank, local):
     torch.cuda.set_device(local)
     L, N, dt, alpha = (12, 12, 12, 12), 8, 0.005, -0.05
     eng = P.NsptEngine(L, N, zero_modes=True, local_gf=True, alpha=alpha)
+    eng.set_local_gf_form(args.lgf_form)
     eng.seed(replica_seed(8000, rank), 0)
     eng.NsptEvolve(dt, args.warmup, 1)
     eng.NsptEvolve(dt, args.steps, 1)
@@ -832,7 +833,8 @@ def run_qcfg(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (cold start + warm-up, device Philox noise)",
             "config": {"workload": "qcfg_12^4_N8_zm_localgf", "L": list(L), "N": N, "dt": dt,
-                       "alpha": alpha, "bc": "periodic", "gf_every": 1},
+                       "alpha": alpha, "bc": "periodic", "gf_every": 1,
+                       "local_gf_form": args.lgf_form},
         }
         print(json.dumps(line), flush=True)
     eng.close()
@@ -850,6 +852,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-gf", action="store_true", help="skip the gauge-fixing figure")
+    ap.add_argument("--lgf-form", default="auto", choices=["auto", "group", "team"],
+                    help="local gauge fixing kernel of the qcfg workload")
     ap.add_argument("--c4-therm", type=int, default=600,
                     help="c4: thermalisation steps before the dt -> 0 measurement")
     ap.add_argument("--c4-meas", type=int, default=600,

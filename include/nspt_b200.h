@@ -129,6 +129,17 @@ int nspt_local_gauge_fixing(nspt_ctx *ctx, double alpha);
 /* grid[d] threads along direction d; every L[d] % grid[d] == 0 and
  * L[d] / grid[d] >= 2 where grid[d] > 1, else NSPT_ERR_ARG. */
 int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]);
+/* Which kernel runs the local gauge fixing; both visit the sites in the
+ * grid's order and give the same links.  NSPT_LGF_GROUP: one 9-lane link
+ * group per reference thread.  NSPT_LGF_TEAM: a warp of three groups per
+ * thread, the site's stagings and link products spread over them (shorter
+ * per-site latency, for grids with few threads).  NSPT_LGF_AUTO (the
+ * default): the team form when all the barrier step's teams fit on the GPU
+ * at once.  Anything else: NSPT_ERR_ARG. */
+#define NSPT_LGF_AUTO 0
+#define NSPT_LGF_GROUP 1
+#define NSPT_LGF_TEAM 2
+int nspt_set_local_gf_form(nspt_ctx *ctx, int form);
 
 /* Observables of the last sweep, normalised as nspt.cc:570-597:
  * plaq[(N+1)*2] (/72V), norm[N] (/12V), trU[4*N*2] (/3V, mu major).

@@ -281,6 +281,17 @@ class NsptEngine:
         g = (ctypes.c_int * 4)(*[int(x) for x in grid])
         self._check(load_library().nspt_set_gf_grid(self._h, g), "nspt_set_gf_grid")
 
+    def set_local_gf_form(self, form: str):
+        """Kernel of the local gauge fixing: "group" (one 9-lane link group
+        per reference thread), "team" (a warp of three groups per thread) or
+        "auto" (the team form when the barrier step's teams all fit on the
+        GPU at once).  Both forms give the same links."""
+        code = {"auto": 0, "group": 1, "team": 2}.get(form)
+        if code is None:
+            raise ValueError(f"local gauge fixing form {form!r}: auto, group or team")
+        self._check(load_library().nspt_set_local_gf_form(self._h, code),
+                    "nspt_set_local_gf_form")
+
     def twist_boundary(self):
         """No-op: twisted boundaries are applied inside every neighbour read,
         so there are no copy sites to refresh (nspt.cc:163-255)."""

@@ -60,6 +60,7 @@ SIGNATURES = {
     "nspt_fa_gauge_fixing": (_I, [_P, ctypes.c_double]),
     "nspt_local_gauge_fixing": (_I, [_P, ctypes.c_double]),
     "nspt_set_gf_grid": (_I, [_P, ctypes.POINTER(ctypes.c_int)]),
+    "nspt_set_local_gf_form": (_I, [_P, _I]),
     "nspt_observables": (_I, [_P, _D, _D, _D]),
     "nspt_plaquette_measure": (_I, [_P, _D]),
     "nspt_rect_observables": (_I, [_P, _D]),

@@ -59,6 +59,7 @@ struct nspt_ctx {
   double *p2;     // lattice momenta p2hat[4][128] of this context's extents
   double2 *ftw;   // FFT twiddles exp(-2 pi i t / L_d), [4][128] (FA only)
   int gf_grid[4]; // local gauge fixing: the reference's thread grid (ntt, ntx, nty, ntz)
+  int gf_form;    // local gauge fixing kernel: NSPT_LGF_AUTO, NSPT_LGF_GROUP or NSPT_LGF_TEAM
   unsigned long long *dcounter;  // Philox step counter on the device (advanced by k_inc)
   int sweep_warps;               // warps per CTA of the sweep, 0 = as many as fit
   // orders per lane and pass of the series kernels: 0 = by N (the low-order
@@ -520,6 +521,35 @@ static int do_local_gf(nspt_ctx *ctx, double alpha) {
   double2 *U = ctx->U, *Uf = ctx->Uf;
   const bool low = use_low(ctx);
   ctx->lg_current = false;
+  // The team form (a warp of three groups per reference thread) shortens
+  // each thread's chain of dependent stagings and products about threefold
+  // but keeps a third of its lanes idle in the exps: automatic choice takes
+  // it when every team of the barrier step is resident at once.
+  const size_t team_bytes = (size_t)LGF_TEAM_SLOTS * SS * sizeof(double2);
+  const int team_warps = 2 * team_bytes <= ctx->smem_optin ? 2 : 1;
+  bool team = team_bytes <= ctx->smem_optin && ctx->gf_form != NSPT_LGF_GROUP;
+  if (team && ctx->gf_form == NSPT_LGF_AUTO) {
+    const long per_sm = std::min<long>((long)((size_t)228 * 1024 / team_bytes), low ? 12 : 8);
+    team = gr.nthr <= per_sm * ctx->nsm;
+  }
+  if (team) {
+    const size_t smem = (size_t)team_warps * team_bytes;
+    const void *fn = low ? (const void *)k_local_gf_team<true> : (const void *)k_local_gf_team<false>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const unsigned grid = (unsigned)((gr.nthr + team_warps - 1) / team_warps);
+    for (long p = 0; p < steps; p++) {
+      if (low)
+        k_local_gf_team<true><<<grid, 32 * team_warps, smem, st>>>(U, Uf, N, SS, geo, alpha, gr, p);
+      else
+        k_local_gf_team<false><<<grid, 32 * team_warps, smem, st>>>(U, Uf, N, SS, geo, alpha, gr, p);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+      ctx->err = std::string("local gauge fixing: ") + cudaGetErrorString(e);
+      return NSPT_ERR_CUDA;
+    }
+    return NSPT_OK;
+  }
   for (long p = 0; p < steps; p++) {
     int rc = launch_groups(
         ctx, low ? (const void *)k_local_gf<true> : (const void *)k_local_gf<false>, 4, gr.nthr,
@@ -657,6 +687,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
                                         : 0.0;
   // finest thread grid the reference accepts: blocks of 2 sites where L is even
   for (int d = 0; d < 4; d++) ctx->gf_grid[d] = (L[d] % 2 == 0) ? L[d] / 2 : 1;
+  ctx->gf_form = NSPT_LGF_AUTO;
   ctx->obs_tr = ctx->obs_tru = ctx->red2 = nullptr;
   ctx->obs_norm = ctx->red1 = ctx->noise = nullptr;
   ctx->noise_pending = false;
@@ -1020,6 +1051,14 @@ extern "C" int nspt_local_gauge_fixing(nspt_ctx *ctx, double alpha) {
 extern "C" int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]) {
   if (!ctx || !grid || !grid_ok(ctx->L, grid)) return NSPT_ERR_ARG;
   for (int d = 0; d < 4; d++) ctx->gf_grid[d] = grid[d];
+  ctx->launch_gen++;
+  return NSPT_OK;
+}
+
+extern "C" int nspt_set_local_gf_form(nspt_ctx *ctx, int form) {
+  if (!ctx) return NSPT_ERR_ARG;
+  if (form != NSPT_LGF_AUTO && form != NSPT_LGF_GROUP && form != NSPT_LGF_TEAM) return NSPT_ERR_ARG;
+  ctx->gf_form = form;
   ctx->launch_gen++;
   return NSPT_OK;
 }

@@ -943,6 +943,38 @@ struct LgfGrid {
   long seg;
 };
 
+// The sites one reference thread visits in one barrier step of
+// stochastic_gauge_fixing (nspt.cc:731-828): thread tid owns block b of the
+// grid; the barrier step fixes the offset rel inside the split directions;
+// the directions that are not split are walked whole, the last fastest.
+struct LgfWalk {
+  int b[4], rel[4];
+  __device__ __forceinline__ LgfWalk(const LgfGrid &gr, long tid, long step) {
+    b[0] = (int)(tid / ((long)gr.n[1] * gr.n[2] * gr.n[3]));
+    b[1] = (int)((tid / ((long)gr.n[2] * gr.n[3])) % gr.n[1]);
+    b[2] = (int)((tid / gr.n[3]) % gr.n[2]);
+    b[3] = (int)(tid % gr.n[3]);
+    for (int d = 0; d < 4; d++) rel[d] = 0;
+    long q = step;
+    for (int d = gr.dmax; d >= 0; d--) {
+      rel[d] = (int)(q % gr.bs[d]);
+      q /= gr.bs[d];
+    }
+  }
+  // coordinates of the r-th site of the walk
+  __device__ __forceinline__ void site(const LgfGrid &gr, const Geo &geo, long r, int *x) const {
+    long t = r;
+    for (int d = 3; d >= 0; d--) {
+      if (d <= gr.dmax) {
+        x[d] = gr.bs[d] * b[d] + rel[d];
+      } else {
+        x[d] = (int)(t % geo.L[d]);
+        t /= geo.L[d];
+      }
+    }
+  }
+};
+
 // A <- A - A^dag, then Trless (W -= dag(W); W.Trless(), nspt.cc:679-682,
 // QCDpt.cc:124-136 and 185-194): flag 0.  Lanes split the orders.
 __device__ __forceinline__ void ser_aherm_trless(double2 *P, int N, const Lane &L) {
@@ -992,30 +1024,10 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
   const size_t plane = (size_t)9 * N * V;
   const int c = L.c;
   const double2 one = make_double2(1.0, 0.0);
-  int b[4];
-  b[0] = (int)(tid / ((long)gr.n[1] * gr.n[2] * gr.n[3]));
-  b[1] = (int)((tid / ((long)gr.n[2] * gr.n[3])) % gr.n[1]);
-  b[2] = (int)((tid / gr.n[3]) % gr.n[2]);
-  b[3] = (int)(tid % gr.n[3]);
-  int rel[4] = {0, 0, 0, 0};
-  {
-    long q = step;
-    for (int d = gr.dmax; d >= 0; d--) {
-      rel[d] = (int)(q % gr.bs[d]);
-      q /= gr.bs[d];
-    }
-  }
+  const LgfWalk walk(gr, tid, step);
   for (long r = 0; r < gr.seg; r++) {
     int x[4];
-    long t = r;
-    for (int d = 3; d >= 0; d--) {
-      if (d <= gr.dmax) {
-        x[d] = gr.bs[d] * b[d] + rel[d];
-      } else {
-        x[d] = (int)(t % geo.L[d]);
-        t /= geo.L[d];
-      }
-    }
+    walk.site(gr, geo, r, x);
     Nb self;
     self.site = x[0] * geo.s0 + x[1] * geo.s1 + x[2] * geo.s2 + x[3];
     self.fwd = self.bwd = 0;
@@ -1032,32 +1044,199 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
     __syncwarp(L.mask);
     // E1 = exp(alpha W), E2 = exp(-alpha W), sharing (alpha W)^2
     ser_square<(LOW ? MO_LOW : MO)>(A, Y2, N, L);
-    ser_horner2<(LOW ? MO_LOW : MO)>(A, Y2, E1, N, L, [](int n) { return inv_factorial(n); },
-                    [&](int k, int rr, double2 v) { E1[sidx(k, rr, c)] = v; });
-    ser_horner2<(LOW ? MO_LOW : MO)>(A, Y2, E2, N, L,
-                    [](int n) { return (n & 1) ? -inv_factorial(n) : inv_factorial(n); },
-                    [&](int k, int rr, double2 v) { E2[sidx(k, rr, c)] = v; });
+    // one call site for both (the odd terms negated for E2): the inlined
+    // series code once instead of twice
+    for (int h = 0; h < 2; h++) {
+      double2 *E = h == 0 ? E1 : E2;
+      const double odd = h == 0 ? 1.0 : -1.0;
+      ser_horner2<(LOW ? MO_LOW : MO)>(
+          A, Y2, E, N, L,
+          [odd](int n) { return (n & 1) ? odd * inv_factorial(n) : inv_factorial(n); },
+          [&](int k, int rr, double2 v) { E[sidx(k, rr, c)] = v; });
+    }
     if (L.j == 0) E1[0] = E2[0] = one;
     __syncwarp(L.mask);
     for (int mu = 0; mu < 4; mu++) {
-      // U_mu(x) <- E1 U_mu(x)
-      stage<true>(Y2, U, Uf, mu, self, geo, N, L);
-      {
-        double2 *dst = U + mu * plane + self.site;
-        const double2 yf = Y2[0];
-        product<(LOW ? MO_LOW : MO), false>(LeftS{E1}, one, Y2, yf, N, L, [&](int k, int rr, double2 v) {
-          dst[(size_t)(9 * (k - 1) + 3 * rr + c) * V] = v;
-        });
-        if (L.j == 0) Uf[(size_t)mu * V + self.site] = flag_mul(one, yf);
-      }
-      // U_mu(x-mu) <- U_mu(x-mu) E2
       const Nb back = neighbour(geo, x, mu, -1);
-      Nb at;
-      at.site = back.site;
-      at.fwd = at.bwd = 0;
-      stage<true>(A, U, Uf, mu, at, geo, N, L);
+      for (int h = 0; h < 2; h++) {
+        // h = 0: U_mu(x) <- E1 U_mu(x); h = 1: U_mu(x-mu) <- U_mu(x-mu) E2,
+        // E2 twisted across a twisted face.  One product call site for both.
+        Nb at;
+        at.site = h == 0 ? self.site : back.site;
+        at.fwd = at.bwd = 0;
+        double2 *Sl = h == 0 ? Y2 : A;
+        stage<true>(Sl, U, Uf, mu, at, geo, N, L);
+        const double2 *R = E2;
+        if (h == 1 && ((back.bwd & geo.twist) >> mu & 1u)) {
+          for (int k = 1 + L.j; k <= N; k += GROUP) {
+            const double2 *src = E2 + 1 + 9 * (k - 1);
+            double2 m[9];
+#pragma unroll
+            for (int rr = 0; rr < 3; rr++)
+#pragma unroll
+              for (int q = 0; q < 3; q++) m[3 * rr + q] = src[3 * q + rr];
+            twist3(m, 0u, 1u << mu);
+            double2 *o = Y2 + 1 + 9 * (k - 1);
+#pragma unroll
+            for (int rr = 0; rr < 3; rr++)
+#pragma unroll
+              for (int q = 0; q < 3; q++) o[3 * q + rr] = m[3 * rr + q];
+          }
+          if (L.j == 0) Y2[0] = one;  // twist_* returns flag VACUUM
+          __syncwarp(L.mask);
+          R = Y2;
+        }
+        const double2 *left = h == 0 ? E1 : A, *right = h == 0 ? Y2 : R;
+        const double2 lf = left[0], rf = right[0];
+        double2 *dst = U + mu * plane + at.site;
+        product<(LOW ? MO_LOW : MO), false>(LeftS{left}, lf, right, rf, N, L,
+                                            [&](int k, int rr, double2 v) {
+                                              dst[(size_t)(9 * (k - 1) + 3 * rr + c) * V] = v;
+                                            });
+        if (L.j == 0) Uf[(size_t)mu * V + at.site] = flag_mul(lf, rf);
+        __syncwarp(L.mask);
+      }
+    }
+  }
+}
+
+// Copy link (mu, site) as stored (no twist, no dagger) into a slot without
+// waiting: the caller commits and waits for the copies of all its stagings
+// at once.  Lane j copies colour component j of every order, as in stage().
+__device__ __forceinline__ void stage_issue(double2 *slot, const double2 *U, const double2 *Uf,
+                                            int mu, int site, size_t V, int N, const Lane &L) {
+  const double2 *src = U + (size_t)mu * 9 * N * V + site;
+  const int r = L.j / 3, c = L.j - 3 * (L.j / 3);
+  for (int k = 1; k <= N; k++) {
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(slot + 1 + 9 * (k - 1) + 3 * c + r);
+    const double2 *gp = src + (size_t)(9 * (k - 1) + L.j) * V;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gp) : "memory");
+  }
+  if (L.j == 0) slot[0] = __ldcg(Uf + (size_t)mu * V + site);
+}
+
+// The team form of k_local_gf, for barrier steps with too few reference
+// threads to fill the GPU (the 12^4 lattice's 6^4 threads, one site each):
+// one warp of three link groups per reference thread, visiting the same
+// sites in the same order.  Per site the team
+//   - stages the eight links U_mu(x), U_mu(x-mu) at once (group g the links
+//     of tasks g, g+3, g+6; task t < 4 is U_t(x), t >= 4 is U_{t-4}(x-mu)),
+//   - forms alpha Trless(W - W^dag), W = sum_mu U_mu(x) - U_mu(x-mu), with
+//     all 27 lanes (one order each, the back link twisted across a twisted
+//     face as stage() twists it),
+//   - squares it in group 0, then runs exp(alpha W) in group 0 and
+//     exp(-alpha W) in group 1 side by side,
+//   - and multiplies the eight links by them, the tasks dealt over the
+//     three groups as the stagings were, from the staged copies (no other
+//     thread writes those links between the barriers, and L_d >= 2 keeps
+//     U_mu(x-mu) apart from the site's forward links).
+// The operations and their order per value are those of k_local_gf.  Slots
+// per team: the eight links, alpha W, (alpha W)^2, E1, E2, and one scratch
+// slot per group for a twisted E2.
+constexpr int LGF_TEAM_SLOTS = 15;
+
+template <bool LOW = false>
+__global__ void __launch_bounds__(64, LOW ? 5 : 4)
+    k_local_gf_team(double2 *U, double2 *Uf, int N, int SS, Geo geo, double alpha, LgfGrid gr,
+                    long step) {
+  constexpr int MOK = LOW ? MO_LOW : MO;
+  constexpr int TEAM = LPW * GROUP;
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long tid = (long)blockIdx.x * nw + warp;
+  if (tid >= gr.nthr) return;
+  const int tl = g * GROUP + L.j;
+  const unsigned tmask = (1u << TEAM) - 1u;
+  double2 *S = sm + (size_t)warp * LGF_TEAM_SLOTS * SS;
+  double2 *X = S + 8 * SS, *X2 = X + SS, *E1 = X2 + SS, *E2 = E1 + SS;
+  double2 *Tw = E2 + SS + (size_t)g * SS;
+  const size_t V = (size_t)geo.V;
+  const size_t plane = (size_t)9 * N * V;
+  const int c = L.c;
+  const double2 one = make_double2(1.0, 0.0);
+  const double D3 = 1.0 / 3.0;
+  const LgfWalk walk(gr, tid, step);
+  for (long r = 0; r < gr.seg; r++) {
+    int x[4];
+    walk.site(gr, geo, r, x);
+    const int self = x[0] * geo.s0 + x[1] * geo.s1 + x[2] * geo.s2 + x[3];
+    for (int t = g; t < 8; t += LPW) {
+      const int mu = t & 3;
+      stage_issue(S + (size_t)t * SS, U, Uf, mu, t < 4 ? self : neighbour(geo, x, mu, -1).site,
+                  V, N, L);
+    }
+    cp_commit();
+    cp_wait0();
+    __syncwarp(tmask);
+    // alpha Trless(W - W^dag), order k by team lane k-1 (slots column major)
+    for (int k = 1 + tl; k <= N; k += TEAM) {
+      double2 w[9];
+#pragma unroll
+      for (int mu = 0; mu < 4; mu++) {
+        const double2 *f = S + (size_t)mu * SS + 1 + 9 * (k - 1);
+        const double2 *bk = S + (size_t)(4 + mu) * SS + 1 + 9 * (k - 1);
+        const unsigned tb = neighbour(geo, x, mu, -1).bwd & geo.twist;
+        double2 bv[9];
+        if (tb) {
+          double2 m[9];
+#pragma unroll
+          for (int rr = 0; rr < 3; rr++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) m[3 * rr + q] = bk[3 * q + rr];
+          twist3(m, tb, 0u);
+#pragma unroll
+          for (int rr = 0; rr < 3; rr++)
+#pragma unroll
+            for (int q = 0; q < 3; q++) bv[3 * q + rr] = m[3 * rr + q];
+        } else {
+#pragma unroll
+          for (int e = 0; e < 9; e++) bv[e] = bk[e];
+        }
+#pragma unroll
+        for (int e = 0; e < 9; e++) w[e] = cadd(mu == 0 ? cz() : w[e], csub(f[e], bv[e]));
+      }
+      double2 b[9];
+#pragma unroll
+      for (int rr = 0; rr < 3; rr++)
+#pragma unroll
+        for (int q = 0; q < 3; q++) b[3 * rr + q] = csub(w[3 * rr + q], cconj(w[3 * q + rr]));
+      const double2 tr = cadd(cadd(b[0], b[4]), b[8]);
+      const double2 z = make_double2(D3 * tr.x, D3 * tr.y);
+      b[0] = csub(b[0], z);
+      b[4] = csub(b[4], z);
+      b[8] = csub(b[8], z);
+      double2 *o = X + 1 + 9 * (k - 1);
+#pragma unroll
+      for (int e = 0; e < 9; e++) o[e] = cscale(b[e], alpha);
+    }
+    if (tl == 0) X[0] = cscale(cz(), alpha);
+    __syncwarp(tmask);
+    // E1 = exp(alpha W), E2 = exp(-alpha W), sharing (alpha W)^2
+    if (g == 0) ser_square<MOK>(X, X2, N, L);
+    __syncwarp(tmask);
+    if (g < 2) {
+      // group 0: exp(alpha W); group 1: exp(-alpha W), the odd terms negated
+      double2 *E = g == 0 ? E1 : E2;
+      const double odd = g == 0 ? 1.0 : -1.0;
+      ser_horner2<MOK>(X, X2, E, N, L,
+                       [odd](int n) { return (n & 1) ? odd * inv_factorial(n) : inv_factorial(n); },
+                       [&](int k, int rr, double2 v) { E[sidx(k, rr, c)] = v; });
+    }
+    __syncwarp(tmask);
+    if (tl == 0) E1[0] = E2[0] = one;
+    __syncwarp(tmask);
+    for (int t = g; t < 8; t += LPW) {
+      // t < 4: U_mu(x) <- E1 U_mu(x); t >= 4: U_mu(x-mu) <- U_mu(x-mu) E2,
+      // E2 twisted across a twisted face
+      const int mu = t & 3;
+      const double2 *Sl = S + (size_t)t * SS;
+      const bool fwd = t < 4;
+      const Nb back = neighbour(geo, x, mu, -1);
       const double2 *R = E2;
-      if ((back.bwd & geo.twist) >> mu & 1u) {
+      if (!fwd && ((back.bwd & geo.twist) >> mu & 1u)) {
         for (int k = 1 + L.j; k <= N; k += GROUP) {
           const double2 *src = E2 + 1 + 9 * (k - 1);
           double2 m[9];
@@ -1066,26 +1245,28 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
 #pragma unroll
             for (int q = 0; q < 3; q++) m[3 * rr + q] = src[3 * q + rr];
           twist3(m, 0u, 1u << mu);
-          double2 *o = Y2 + 1 + 9 * (k - 1);
+          double2 *o = Tw + 1 + 9 * (k - 1);
 #pragma unroll
           for (int rr = 0; rr < 3; rr++)
 #pragma unroll
             for (int q = 0; q < 3; q++) o[3 * q + rr] = m[3 * rr + q];
         }
-        if (L.j == 0) Y2[0] = one;  // twist_* returns flag VACUUM
+        if (L.j == 0) Tw[0] = one;  // twist_* returns flag VACUUM
         __syncwarp(L.mask);
-        R = Y2;
+        R = Tw;
       }
-      {
-        double2 *dst = U + mu * plane + back.site;
-        const double2 af = A[0], rf = R[0];
-        product<(LOW ? MO_LOW : MO), false>(LeftS{A}, af, R, rf, N, L, [&](int k, int rr, double2 v) {
-          dst[(size_t)(9 * (k - 1) + 3 * rr + c) * V] = v;
-        });
-        if (L.j == 0) Uf[(size_t)mu * V + back.site] = flag_mul(af, rf);
-      }
+      const double2 *left = fwd ? E1 : Sl, *right = fwd ? Sl : R;
+      const double2 lf = left[0], rf = right[0];
+      const int site = fwd ? self : back.site;
+      double2 *dst = U + mu * plane + site;
+      product<MOK, false>(LeftS{left}, lf, right, rf, N, L, [&](int k, int rr, double2 v) {
+        dst[(size_t)(9 * (k - 1) + 3 * rr + c) * V] = v;
+      });
+      if (L.j == 0) Uf[(size_t)mu * V + site] = flag_mul(lf, rf);
       __syncwarp(L.mask);
     }
+    // the next site's stagings read links written here
+    __syncwarp(tmask);
   }
 }
 

@@ -333,12 +333,16 @@ def test_two_contexts_with_different_extents_interleaved(engine_mod, oracle_mod)
     ((4, 4, 4, 4), 5, "yz", (1, 2, 2, 1)),
     ((4, 4, 4, 4), 12, "yzt", (2, 1, 2, 2)),
 ], ids=["sequential", "grid2222", "grid1312_6x", "twisted_yz_grid1221", "twisted_yzt_n12"])
-def test_local_gauge_fixing_matches_oracle_thread_grid(engine_mod, oracle_mod, L, N, twist, grid):
+@pytest.mark.parametrize("form", ["group", "team"])
+def test_local_gauge_fixing_matches_oracle_thread_grid(engine_mod, oracle_mod, L, N, twist, grid,
+                                                        form):
     """stochastic_gauge_fixing in the order the reference's OpenMP thread grid
-    fixes (the oracle is pinned to the reference's builds of those grids)."""
+    fixes (the oracle is pinned to the reference's builds of those grids),
+    by either kernel form."""
     e, o = make_pair(engine_mod, oracle_mod, L, N, twist=twist, start=61)
     alpha = -0.08
     e.set_gf_grid(grid)
+    e.set_local_gf_form(form)
     for _ in range(2):
         e.stochastic_gauge_fixing(alpha)
         o.local_gauge_fix(alpha, grid=grid)
@@ -366,6 +370,37 @@ def test_local_gauge_fixing_in_the_step_with_default_grid(engine_mod, oracle_mod
         o.local_gauge_fix(alpha, grid=(2, 2, 1, 2))
         check_obs(e.observables(), oo, 1e-11)
     assert per_order_rel(e.download(), o.links, N).max() <= 1e-11
+
+
+@pytest.mark.parametrize("L,N,twist,grid", [
+    ((4, 4, 4, 4), 24, "yz", (2, 2, 2, 2)),
+    ((6, 4, 4, 8), 8, "yzt", (3, 2, 1, 4)),
+], ids=["n24_twisted_yz", "n8_twisted_yzt_grid3214"])
+def test_local_gauge_fixing_forms_agree(engine_mod, oracle_mod, L, N, twist, grid):
+    """The team and group kernels on the same field: both within 1e-12 of the
+    oracle per order, flags exact, and within rounding of each other."""
+    P, O = engine_mod, oracle_mod
+    alpha = -0.06
+    outs = []
+    for form in ("group", "team"):
+        e, o = make_pair(P, O, L, N, twist=twist, start=83)
+        e.set_gf_grid(grid)
+        e.set_local_gf_form(form)
+        e.stochastic_gauge_fixing(alpha)
+        outs.append(e.download())
+    o.local_gauge_fix(alpha, grid=grid)
+    for out in outs:
+        assert per_order_rel(out, o.links, N).max() <= 1e-12
+        assert flag_diff(out, o.links, N) == 0.0
+    assert per_order_rel(outs[0], outs[1], N).max() <= 1e-13
+
+
+def test_local_gf_form_rejects_unknown(engine_mod):
+    P = engine_mod
+    e = P.NsptEngine((4, 4, 4, 4), 3, local_gf=True)
+    with pytest.raises(ValueError):
+        e.set_local_gf_form("warp")
+    assert P.load_library().nspt_set_local_gf_form(e._h, 7) != 0
 
 
 def test_gf_grid_rejects_what_the_reference_rejects(engine_mod):
