@@ -200,106 +200,6 @@ __device__ __forceinline__ void product(const Left &A, double2 a0, const double2
   }
 }
 
-// product() with the left orders taken in pairs i, i+3.  Order i meets the
-// right column B_{k-i} in the lane's order k, and order i+3 meets the same
-// column in the lane's next order k+3, so every column loaded from shared
-// memory feeds two 3x3 multiply-adds: per pair 18 left loads and about MO
-// column loads for 2 MO blocks, against 2 (9 + 3 MO) loads in product().
-// The pairs are (ib + r, ib + r + 3), r = 0..2, ib = i0, i0 + 6, ...; a
-// lane's orders collect their terms in that order rather than ascending i
-// (the sums differ from product()'s by rounding only).
-template <int MO, bool DA, class Left, class Emit>
-__device__ __forceinline__ void product2(const Left &A, double2 a0, const double2 *B, double2 b0,
-                                         int M, const Lane &L, Emit emit, int i0 = 1) {
-  const int c = L.c;
-  constexpr int PASS = 3 * MO;
-  const int npass = (M + PASS - 1) / PASS;
-  for (int ps = npass - 1; ps >= 0; --ps) {
-    const int kb = ps * PASS;
-    const int kend = min(kb + PASS, M);  // last order of the pass
-    const int k0 = kb + L.s + 1;         // the lane's first order of the pass
-    double2 acc[MO][3];
-#pragma unroll
-    for (int q = 0; q < MO; q++)
-#pragma unroll
-      for (int r = 0; r < 3; r++) acc[q][r] = cz();
-    double2 a[9], a2[9];
-    for (int ib = i0; ib < kend; ib += 6) {
-      for (int r3 = 0; r3 < 3; r3++) {
-        const int i = ib + r3;
-        if (i >= kend) break;
-        const int i2 = i + 3;
-        const bool two = i2 < kend;
-        A.template load<DA>(i, a);
-        if (two) {
-          A.template load<DA>(i2, a2);
-          // the partner's term in the lane's first order has no column in
-          // the loop below (only in a pass that starts above order i2)
-          if (k0 <= kend && k0 > i2) {
-            const double2 *bj = B + 1 + 9 * (k0 - i2 - 1) + 3 * c;
-            const double2 w0 = bj[0], w1 = bj[1], w2 = bj[2];
-#pragma unroll
-            for (int r = 0; r < 3; r++) {
-              cfma(acc[0][r], a2[3 * r], w0);
-              cfma(acc[0][r], a2[3 * r + 1], w1);
-              cfma(acc[0][r], a2[3 * r + 2], w2);
-            }
-          }
-        }
-#pragma unroll
-        for (int q = 0; q < MO; q++) {
-          const int k = k0 + 3 * q;
-          if (k <= kend && k > i) {
-            const double2 *bj = B + 1 + 9 * (k - i - 1) + 3 * c;
-            const double2 w0 = bj[0], w1 = bj[1], w2 = bj[2];
-#pragma unroll
-            for (int r = 0; r < 3; r++) {
-              cfma(acc[q][r], a[3 * r], w0);
-              cfma(acc[q][r], a[3 * r + 1], w1);
-              cfma(acc[q][r], a[3 * r + 2], w2);
-            }
-            // order k + 3 from order i + 3 (k + 3 > i + 3 holds with k > i)
-            if (q + 1 < MO && two && k + 3 <= kend) {
-#pragma unroll
-              for (int r = 0; r < 3; r++) {
-                cfma(acc[q + 1][r], a2[3 * r], w0);
-                cfma(acc[q + 1][r], a2[3 * r + 1], w1);
-                cfma(acc[q + 1][r], a2[3 * r + 2], w2);
-              }
-            }
-          }
-        }
-      }
-    }
-    __syncwarp(L.mask);
-    const bool fa = !cis0(a0), fb = !cis0(b0);
-#pragma unroll
-    for (int q = 0; q < MO; q++) {
-      const int k = k0 + 3 * q;
-      if (k <= kend) {
-        double2 ak[3];
-        if (fb) A.template col<DA>(k, c, ak);
-#pragma unroll
-        for (int r = 0; r < 3; r++) {
-          double2 v = acc[q][r];
-          if (fa || fb) {
-            double2 u;
-            if (!fa)
-              u = cmul(b0, ak[r]);
-            else if (!fb)
-              u = cmul(a0, B[sidx(k, r, c)]);
-            else
-              u = cadd(cmul(b0, ak[r]), cmul(a0, B[sidx(k, r, c)]));
-            v = cadd(v, u);
-          }
-          emit(k, r, v);
-        }
-      }
-    }
-    __syncwarp(L.mask);
-  }
-}
-
 // ---------------- compensated float-float Cauchy product ----------------
 //
 // The same truncated product as product(), with every 3x3 multiply-add of
