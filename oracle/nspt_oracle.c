@@ -47,6 +47,10 @@ struct oracle_ctx {
   long V;
   long sYZT, sZT, sT;
   cx *U, *F, *MM;
+  /* on-the-fly update with twisted boundaries: the field as it was when the
+   * reference's twisted copy sites were last refreshed (twist_boundary);
+   * reads that cross a twisted face come from here.  NULL otherwise. */
+  cx *snap;
   cx omega[4][9], omegadag[4][9];
   double *p2hat[4];
   double c1;          /* improved action: 0 = Wilson (Quenched.cc:311-322) */
@@ -277,7 +281,13 @@ static void fetch_link(const oracle_ctx *c, const cx *field, const int *y,
       fwd[d] = 1;
     }
   }
-  const cx *src = field + ((size_t)site_of(c, x) * 4 + mu) * SER(N);
+  int crosses = 0;
+  for (int d = 0; d < 4; d++)
+    if ((bwd[d] || fwd[d]) && ((c->tw >> d) & 1)) crosses = 1;
+  /* the reference reads a twisted copy site there (lattice.h:236-300),
+   * refreshed only by twist_boundary (nspt.cc:163-255) */
+  const cx *base = crosses && c->snap ? c->snap : field;
+  const cx *src = base + ((size_t)site_of(c, x) * 4 + mu) * SER(N);
   s_copy(out, src, N);
   int any = 0;
   cx t[9], u[9];
@@ -317,6 +327,7 @@ oracle_ctx *oracle_create(const int L[4], int N, int twist_mask) {
   size_t n = (size_t)c->V * 4 * SER(N);
   c->U = (cx *)calloc(n, sizeof(cx));
   c->F = (cx *)calloc(n, sizeof(cx));
+  c->snap = NULL;
   c->MM = (cx *)calloc(4 * (size_t)SER(N), sizeof(cx));
   /* twist matrices, twistmatrices.h:158-240 (y, z, t) */
   memset(c->omega, 0, sizeof(c->omega));
@@ -358,6 +369,7 @@ void oracle_destroy(oracle_ctx *c) {
   if (!c) return;
   free(c->U);
   free(c->F);
+  free(c->snap);
   free(c->MM);
   for (int d = 0; d < 4; d++) free(c->p2hat[d]);
   free(c);
@@ -603,111 +615,120 @@ static void staple2x1(const oracle_ctx *c, const cx *field, const int *x, int mu
 #undef LK
 }
 
-/* ---------------- Langevin sweep (nspt.cc:258-600, Jacobi) ---------------- */
+/* ---------------- Langevin sweep (nspt.cc:258-600) ---------------- */
 
-void oracle_sweep(oracle_ctx *c, double dt, const double *noise, double *plaq,
-                  double *norm, double *tru, int zero_modes) {
-  int N = c->N, n = SER(N);
-  long nl = c->V * 4;
-  /* QuenchedAllocate, Quenched.cc:584-589 */
-  double stau = sqrt(dt);
-  double tau_g = dt;
-  tau_g /= -(2 * 3);
-  cx *tr = (cx *)calloc((size_t)nl * (N + 1), sizeof(cx));
-  double *nrm = (double *)calloc((size_t)nl * N, sizeof(double));
-  cx *tu = (cx *)calloc((size_t)nl * N, sizeof(cx));
-  cx *lg = zero_modes ? (cx *)calloc((size_t)nl * n, sizeof(cx)) : NULL;
+/* Per-link observables of a sweep, reduced in link order afterwards. */
+typedef struct {
+  cx *tr;      /* [nl][N+1] Tr(U W), nspt.cc:393 */
+  double *nrm; /* [nl][N]   Tr(U_k U_k^dag), nspt.cc:398 */
+  cx *tu;      /* [nl][N]   Tr U_k, nspt.cc:400 */
+  cx *lg;      /* [nl][SER] log of the new link (zero modes), or NULL */
+  cx *tr2;     /* [nl][N+1] Tr(U W2), improved actions, or NULL */
+} sweep_obs;
+
+/* One link of gauge_wilson (nspt.cc:362-439): the staples of (x, mu) from
+ * the field c->U (twisted crossings from c->snap when set), the force
+ * reH(U W) tau_g, the noise, and the new link exp(W1) U into out, which may
+ * be the link itself (the on-the-fly update).  l: the link's index.
+ * Scratch: 24 series. */
+static void sweep_link(oracle_ctx *c, const int *x, int mu, long l, double tau_g, double stau,
+                       const double *noise, cx *out, sweep_obs *ob, cx *scr) {
+  const int N = c->N, n = SER(N);
   const int imp = c->c1 != 0.0;
-  cx *tr2 = imp ? (cx *)calloc((size_t)nl * (N + 1), sizeof(cx)) : NULL;
-#pragma omp parallel
-  {
-    cx *scr = (cx *)malloc(sizeof(cx) * n * 24);
-    cx *W2 = scr + 14 * n, *S2 = scr + 15 * n, *P2 = scr + 16 * n, *rs = scr + 17 * n;
-    cx *W = scr + 7 * n, *S = scr + 8 * n, *P = scr + 9 * n, *E = scr + 10 * n,
-       *B = scr + 11 * n, *Bn = scr + 12 * n;
-    cx t[9], d[9];
-#pragma omp for schedule(static)
-    for (long l = 0; l < nl; l++) {
-      long s = l / 4;
-      int mu = (int)(l % 4), x[4];
-      coords_of(c, s, x);
-      const cx *u = link_ptr(c->U, c, s, mu);
-      s_zero(W, N);
-      if (imp) s_zero(W2, N);
-      for (int nu = 0; nu < 4; nu++) {
-        if (nu == mu) continue;
-        staple(c, c->U, x, mu, nu, S, scr);
-        s_acc(W, S, N);
-        if (imp) {
-          staple2x1(c, c->U, x, mu, nu, S2, rs);
-          s_acc(W2, S2, N);
-        }
-      }
-      s_mul(P, u, W, N);
-      /* ptSU3::Tr QCDpt.cc:115-122 */
-      cx *trl = tr + (size_t)l * (N + 1);
-      trl[0].re = 3. * P[0].re;
-      trl[0].im = 3. * P[0].im;
-      for (int k = 0; k < N; k++) {
-        trl[k + 1] = m_tr(P + 1 + 9 * k);
-        m_dag(d, u + 1 + 9 * k);
-        m_mul(t, u + 1 + 9 * k, d);
-        nrm[(size_t)l * N + k] = m_tr(t).re;
-        tu[(size_t)l * N + k] = m_tr(u + 1 + 9 * k);
-      }
-      if (imp) { /* nspt.cc:294-303: W1 = c0 W1 + c1 (U W2) */
-        s_mul(P2, u, W2, N);
-        cx *t2l = tr2 + (size_t)l * (N + 1);
-        t2l[0].re = 3. * P2[0].re;
-        t2l[0].im = 3. * P2[0].im;
-        for (int k = 0; k < N; k++) t2l[k + 1] = m_tr(P2 + 1 + 9 * k);
-        const double c0 = 1. - 8. * c->c1;
-        for (int k = 0; k < n; k++) {
-          cx a0 = {c0 * P[k].re, c0 * P[k].im}, b0 = {c->c1 * P2[k].re, c->c1 * P2[k].im};
-          P[k] = cadd(a0, b0);
-        }
-      }
-      s_reH(P, N);
-      s_scale(P, tau_g, N);
-      /* W1.ptU[0] -= stau*SU3rand(Rand) nspt.cc:423 */
-      cx eta[9];
-      oracle_su3rand(noise + (size_t)l * 8, (double *)eta);
-      for (int e = 0; e < 9; e++) {
-        cx v = {stau * eta[e].re, stau * eta[e].im};
-        P[1 + e] = csub(P[1 + e], v);
-      }
-      s_exp(E, P, N, B, Bn);
-      cx *f = link_ptr(c->F, c, s, mu);
-      s_mul(f, E, u, N); /* F[link] = exp(W1)*U[link] nspt.cc:429 */
-      if (zero_modes) s_log(lg + (size_t)l * n, f, N, B, Bn);
+  cx *W2 = scr + 14 * n, *S2 = scr + 15 * n, *P2 = scr + 16 * n, *rs = scr + 17 * n;
+  cx *W = scr + 7 * n, *S = scr + 8 * n, *P = scr + 9 * n, *E = scr + 10 * n,
+     *B = scr + 11 * n, *Bn = scr + 12 * n, *Fn = scr + 13 * n;
+  cx t[9], d[9];
+  const long s = site_of(c, x);
+  const cx *u = link_ptr(c->U, c, s, mu);
+  s_zero(W, N);
+  if (imp) s_zero(W2, N);
+  for (int nu = 0; nu < 4; nu++) {
+    if (nu == mu) continue;
+    staple(c, c->U, x, mu, nu, S, scr);
+    s_acc(W, S, N);
+    if (imp) {
+      staple2x1(c, c->U, x, mu, nu, S2, rs);
+      s_acc(W2, S2, N);
     }
-    free(scr);
   }
-  /* deterministic reductions in the reference's site order (nspt.cc:467-485) */
+  s_mul(P, u, W, N);
+  /* ptSU3::Tr QCDpt.cc:115-122 */
+  cx *trl = ob->tr + (size_t)l * (N + 1);
+  trl[0].re = 3. * P[0].re;
+  trl[0].im = 3. * P[0].im;
+  for (int k = 0; k < N; k++) {
+    trl[k + 1] = m_tr(P + 1 + 9 * k);
+    m_dag(d, u + 1 + 9 * k);
+    m_mul(t, u + 1 + 9 * k, d);
+    ob->nrm[(size_t)l * N + k] = m_tr(t).re;
+    ob->tu[(size_t)l * N + k] = m_tr(u + 1 + 9 * k);
+  }
+  if (imp) { /* nspt.cc:294-303: W1 = c0 W1 + c1 (U W2) */
+    s_mul(P2, u, W2, N);
+    cx *t2l = ob->tr2 + (size_t)l * (N + 1);
+    t2l[0].re = 3. * P2[0].re;
+    t2l[0].im = 3. * P2[0].im;
+    for (int k = 0; k < N; k++) t2l[k + 1] = m_tr(P2 + 1 + 9 * k);
+    const double c0 = 1. - 8. * c->c1;
+    for (int k = 0; k < n; k++) {
+      cx a0 = {c0 * P[k].re, c0 * P[k].im}, b0 = {c->c1 * P2[k].re, c->c1 * P2[k].im};
+      P[k] = cadd(a0, b0);
+    }
+  }
+  s_reH(P, N);
+  s_scale(P, tau_g, N);
+  /* W1.ptU[0] -= stau*SU3rand(Rand) nspt.cc:423 */
+  cx eta[9];
+  oracle_su3rand(noise + (size_t)l * 8, (double *)eta);
+  for (int e = 0; e < 9; e++) {
+    cx v = {stau * eta[e].re, stau * eta[e].im};
+    P[1 + e] = csub(P[1 + e], v);
+  }
+  s_exp(E, P, N, B, Bn);
+  /* F[link] = exp(W1)*U[link] (nspt.cc:429), or U[link] on the fly (:427) */
+  s_mul(Fn, E, u, N);
+  s_copy(out, Fn, N);
+  if (ob->lg) s_log(ob->lg + (size_t)l * n, out, N, B, Bn);
+}
+
+static void obs_alloc(const oracle_ctx *c, int zero_modes, sweep_obs *ob) {
+  const int N = c->N;
+  const long nl = c->V * 4;
+  ob->tr = (cx *)calloc((size_t)nl * (N + 1), sizeof(cx));
+  ob->nrm = (double *)calloc((size_t)nl * N, sizeof(double));
+  ob->tu = (cx *)calloc((size_t)nl * N, sizeof(cx));
+  ob->lg = zero_modes ? (cx *)calloc((size_t)nl * SER(N), sizeof(cx)) : NULL;
+  ob->tr2 = c->c1 != 0.0 ? (cx *)calloc((size_t)nl * (N + 1), sizeof(cx)) : NULL;
+}
+
+/* The sweep's sums (w1, norm, trU, MM, w2) in link order and normalised as
+ * nspt.cc:570-597 prints them; frees the per-link arrays. */
+static void obs_reduce(oracle_ctx *c, sweep_obs *ob, double *plaq, double *norm, double *tru) {
+  const int N = c->N, n = SER(N);
+  const long nl = c->V * 4;
   cx *w1 = (cx *)calloc(N + 1, sizeof(cx));
   double *nm = (double *)calloc(N, sizeof(double));
   cx *tm = (cx *)calloc(4 * (size_t)N, sizeof(cx));
   for (int mu = 0; mu < 4; mu++) s_zero(c->MM + (size_t)mu * n, N);
   for (long l = 0; l < nl; l++) {
     int mu = (int)(l % 4);
-    for (int k = 0; k <= N; k++) w1[k] = cadd(w1[k], tr[(size_t)l * (N + 1) + k]);
+    for (int k = 0; k <= N; k++) w1[k] = cadd(w1[k], ob->tr[(size_t)l * (N + 1) + k]);
     for (int k = 0; k < N; k++) {
-      nm[k] += nrm[(size_t)l * N + k];
-      tm[mu * N + k] = cadd(tm[mu * N + k], tu[(size_t)l * N + k]);
+      nm[k] += ob->nrm[(size_t)l * N + k];
+      tm[mu * N + k] = cadd(tm[mu * N + k], ob->tu[(size_t)l * N + k]);
     }
-    if (zero_modes) s_acc(c->MM + (size_t)mu * n, lg + (size_t)l * n, N);
+    if (ob->lg) s_acc(c->MM + (size_t)mu * n, ob->lg + (size_t)l * n, N);
   }
-  double V = (double)c->V;
-  if (imp) {
+  if (ob->tr2) {
     cx *w2 = (cx *)calloc(N + 1, sizeof(cx));
     for (long l = 0; l < nl; l++)
-      for (int k = 0; k <= N; k++) w2[k] = cadd(w2[k], tr2[(size_t)l * (N + 1) + k]);
+      for (int k = 0; k <= N; k++) w2[k] = cadd(w2[k], ob->tr2[(size_t)l * (N + 1) + k]);
     for (int k = 0; k <= N; k++) {
       c->last_w2[2 * k] = w2[k].re / (double)(72 * c->V);
       c->last_w2[2 * k + 1] = w2[k].im / (double)(72 * c->V);
     }
     free(w2);
-    free(tr2);
   }
   if (plaq)
     for (int k = 0; k <= N; k++) {
@@ -722,18 +743,152 @@ void oracle_sweep(oracle_ctx *c, double dt, const double *noise, double *plaq,
         tru[2 * (mu * N + k)] = tm[mu * N + k].re / (double)(3 * c->V);
         tru[2 * (mu * N + k) + 1] = tm[mu * N + k].im / (double)(3 * c->V);
       }
-  (void)V;
   free(w1);
   free(nm);
   free(tm);
-  free(tr);
-  free(nrm);
-  free(tu);
-  free(lg);
+  free(ob->tr);
+  free(ob->nrm);
+  free(ob->tu);
+  free(ob->lg);
+  free(ob->tr2);
+}
+
+/* gauge_wilson(Umu, Fmu) with UPDATE_ONTHEFLY off (the Jacobi update,
+ * nspt.cc:428-430), then Umu = Fmu (nspt.cc:992).  QuenchedAllocate sets
+ * stau = sqrt(dt), tau_g = -dt/6 (Quenched.cc:584-589). */
+void oracle_sweep(oracle_ctx *c, double dt, const double *noise, double *plaq,
+                  double *norm, double *tru, int zero_modes) {
+  const long nl = c->V * 4;
+  double stau = sqrt(dt);
+  double tau_g = dt;
+  tau_g /= -(2 * 3);
+  sweep_obs ob;
+  obs_alloc(c, zero_modes, &ob);
+  free(c->snap); /* every read sees the field as it was: no stale copies */
+  c->snap = NULL;
+#pragma omp parallel
+  {
+    cx *scr = (cx *)malloc(sizeof(cx) * SER(c->N) * 24);
+#pragma omp for schedule(static)
+    for (long l = 0; l < nl; l++) {
+      long s = l / 4;
+      int mu = (int)(l % 4), x[4];
+      coords_of(c, s, x);
+      sweep_link(c, x, mu, l, tau_g, stau, noise, link_ptr(c->F, c, s, mu), &ob, scr);
+    }
+    free(scr);
+  }
+  obs_reduce(c, &ob, plaq, norm, tru);
   /* Umu = Fmu, nspt.cc:992 */
   cx *sw = c->U;
   c->U = c->F;
   c->F = sw;
+}
+
+/* The order in which the reference built with the OpenMP thread grid
+ * grid = {ntt, ntx, nty, ntz} (choices.h:124-128, blocks set up at
+ * Quenched.cc:518-531) visits the sites in gauge_wilson (nspt.cc:355-460)
+ * and stochastic_gauge_fixing (nspt.cc:723-815): thread tid owns a block of
+ * L_d / n_d sites per direction and walks it lexicographically; all threads
+ * take a barrier after every iteration of the deepest split direction's
+ * loop.  Threads between two barriers touch disjoint links (their sites are
+ * >= 2 apart in a split direction), so running them one after another in
+ * thread order gives the same field.  Fills order[V] with site indices in
+ * that serial order; -1 for a grid the reference rejects. */
+static int grid_order(const oracle_ctx *c, const int *grid, long *order) {
+  int bs[4], dmax = -1;
+  for (int d = 0; d < 4; d++) {
+    if (grid[d] < 1 || c->L[d] % grid[d]) return -1;
+    bs[d] = c->L[d] / grid[d];
+    if (grid[d] > 1) {
+      if (bs[d] < 2) return -1;
+      dmax = d;
+    }
+  }
+  const int nthr = grid[0] * grid[1] * grid[2] * grid[3];
+  long steps = 1, seg = 1, m = 0;
+  for (int d = 0; d < 4; d++) {
+    if (d <= dmax)
+      steps *= bs[d];
+    else
+      seg *= c->L[d];
+  }
+  for (long p = 0; p < steps; p++) {
+    int rel[4] = {0, 0, 0, 0};
+    long q = p;
+    for (int d = dmax; d >= 0; d--) {
+      rel[d] = (int)(q % bs[d]);
+      q /= bs[d];
+    }
+    for (int tid = 0; tid < nthr; tid++) {
+      int b[4];
+      b[0] = tid / (grid[1] * grid[2] * grid[3]);
+      b[1] = (tid / (grid[2] * grid[3])) % grid[1];
+      b[2] = (tid / grid[3]) % grid[2];
+      b[3] = tid % grid[3];
+      for (long r = 0; r < seg; r++) {
+        int x[4];
+        long t = r;
+        for (int d = 3; d >= 0; d--) {
+          if (d <= dmax) {
+            x[d] = bs[d] * b[d] + rel[d];
+          } else {
+            x[d] = (int)(t % c->L[d]);
+            t /= c->L[d];
+          }
+        }
+        order[m++] = site_of(c, x);
+      }
+    }
+  }
+  return 0;
+}
+
+/* gauge_wilson(Umu) with UPDATE_ONTHEFLY, the reference's default
+ * (choices.h:61): every link updated in place, U = exp(W1) U (nspt.cc:427),
+ * sites in the thread grid's order, mu = 0..3 inner, so that a link's
+ * staples see the links updated before it.  With twisted boundaries a read
+ * across a twisted face sees the reference's copy site, which holds the
+ * field of the last twist_boundary (the start of the step): the oracle keeps
+ * that field in c->snap until oracle_twist_boundary.  The log of each new
+ * link goes to MM (nspt.cc:432-437). */
+int oracle_sweep_onthefly(oracle_ctx *c, double dt, const double *noise, const int *grid,
+                          double *plaq, double *norm, double *tru, int zero_modes) {
+  const int N = c->N;
+  long *order = (long *)malloc(sizeof(long) * c->V);
+  if (grid_order(c, grid, order)) {
+    free(order);
+    return -1;
+  }
+  double stau = sqrt(dt);
+  double tau_g = dt;
+  tau_g /= -(2 * 3);
+  const size_t bytes = sizeof(cx) * (size_t)c->V * 4 * SER(N);
+  if (c->tw) {
+    if (!c->snap) c->snap = (cx *)malloc(bytes);
+    memcpy(c->snap, c->U, bytes);
+  }
+  sweep_obs ob;
+  obs_alloc(c, zero_modes, &ob);
+  cx *scr = (cx *)malloc(sizeof(cx) * SER(N) * 24);
+  for (long i = 0; i < c->V; i++) {
+    const long s = order[i];
+    int x[4];
+    coords_of(c, s, x);
+    for (int mu = 0; mu < 4; mu++)
+      sweep_link(c, x, mu, s * 4 + mu, tau_g, stau, noise, link_ptr(c->U, c, s, mu), &ob, scr);
+  }
+  free(scr);
+  free(order);
+  obs_reduce(c, &ob, plaq, norm, tru);
+  return 0;
+}
+
+/* twist_boundary (nspt.cc:163-255): the reference's copy sites are
+ * refreshed, so reads across a twisted face see the field again. */
+void oracle_twist_boundary(oracle_ctx *c) {
+  free(c->snap);
+  c->snap = NULL;
 }
 
 /* zero_modes_subtraction, nspt.cc:605-654 */
@@ -913,53 +1068,19 @@ static void local_gf_site(oracle_ctx *c, const int *x, double alpha, cx *scr) {
  * sweep (nspt.cc:658-720).  Returns -1 if a block is not a whole number of
  * sites >= 2 in a split direction. */
 int oracle_local_gauge_fix_grid(oracle_ctx *c, double alpha, const int *grid) {
-  int bs[4], dmax = -1;
-  for (int d = 0; d < 4; d++) {
-    if (grid[d] < 1 || c->L[d] % grid[d]) return -1;
-    bs[d] = c->L[d] / grid[d];
-    if (grid[d] > 1) {
-      if (bs[d] < 2) return -1;
-      dmax = d;
-    }
-  }
-  const int nthr = grid[0] * grid[1] * grid[2] * grid[3];
-  long steps = 1, seg = 1;
-  for (int d = 0; d < 4; d++) {
-    if (d <= dmax)
-      steps *= bs[d];
-    else
-      seg *= c->L[d];
+  long *order = (long *)malloc(sizeof(long) * c->V);
+  if (grid_order(c, grid, order)) {
+    free(order);
+    return -1;
   }
   cx *scr = (cx *)malloc(sizeof(cx) * SER(c->N) * 8);
-  for (long p = 0; p < steps; p++) {
-    int rel[4] = {0, 0, 0, 0};
-    long q = p;
-    for (int d = dmax; d >= 0; d--) {
-      rel[d] = (int)(q % bs[d]);
-      q /= bs[d];
-    }
-    for (int tid = 0; tid < nthr; tid++) {
-      int b[4];
-      b[0] = tid / (grid[1] * grid[2] * grid[3]);
-      b[1] = (tid / (grid[2] * grid[3])) % grid[1];
-      b[2] = (tid / grid[3]) % grid[2];
-      b[3] = tid % grid[3];
-      for (long r = 0; r < seg; r++) {
-        int x[4];
-        long t = r;
-        for (int d = 3; d >= 0; d--) {
-          if (d <= dmax) {
-            x[d] = bs[d] * b[d] + rel[d];
-          } else {
-            x[d] = (int)(t % c->L[d]);
-            t /= c->L[d];
-          }
-        }
-        local_gf_site(c, x, alpha, scr);
-      }
-    }
+  for (long i = 0; i < c->V; i++) {
+    int x[4];
+    coords_of(c, order[i], x);
+    local_gf_site(c, x, alpha, scr);
   }
   free(scr);
+  free(order);
   return 0;
 }
 

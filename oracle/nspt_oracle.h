@@ -46,6 +46,16 @@ void oracle_unitarise(oracle_ctx *c);
  */
 void oracle_sweep(oracle_ctx *c, double dt, const double *noise, double *plaq,
                   double *norm, double *tru, int zero_modes);
+/* gauge_wilson with UPDATE_ONTHEFLY (the reference's default, choices.h:61):
+ * links updated in place, in the order of the OpenMP thread grid
+ * grid = {ntt, ntx, nty, ntz}; same noise layout and outputs as
+ * oracle_sweep.  With twisted boundaries, reads across a twisted face see
+ * the field of the step's start (the reference's copy sites) until
+ * oracle_twist_boundary.  -1 for a grid the reference rejects. */
+int oracle_sweep_onthefly(oracle_ctx *c, double dt, const double *noise, const int *grid,
+                          double *plaq, double *norm, double *tru, int zero_modes);
+/* twist_boundary, nspt.cc:163-255: the copy sites refreshed */
+void oracle_twist_boundary(oracle_ctx *c);
 /* zero_modes_subtraction, nspt.cc:605-654 (uses MM from the last sweep) */
 void oracle_zero_modes(oracle_ctx *c);
 /* FAstochastic_gauge_fixing, nspt.cc:866-948 (periodic only) */

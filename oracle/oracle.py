@@ -47,6 +47,10 @@ def lib():
         L.oracle_random_start.argtypes = [P, ctypes.c_long, ctypes.c_double]
         L.oracle_unitarise.argtypes = [P]
         L.oracle_sweep.argtypes = [P, ctypes.c_double, D, D, D, D, ctypes.c_int]
+        L.oracle_sweep_onthefly.argtypes = [P, ctypes.c_double, D, ctypes.POINTER(ctypes.c_int),
+                                            D, D, D, ctypes.c_int]
+        L.oracle_sweep_onthefly.restype = ctypes.c_int
+        L.oracle_twist_boundary.argtypes = [P]
         L.oracle_zero_modes.argtypes = [P]
         L.oracle_fa_gauge_fix.argtypes = [P, ctypes.c_double]
         L.oracle_local_gauge_fix.argtypes = [P, ctypes.c_double]
@@ -163,16 +167,32 @@ class Oracle:
         self.unitarise()
         return plaq
 
-    def sweep(self, dt: float, noise: np.ndarray, zero_modes: bool = False) -> SweepObs:
+    def sweep(self, dt: float, noise: np.ndarray, zero_modes: bool = False,
+              onthefly: bool = False, grid=(1, 1, 1, 1)) -> SweepObs:
+        """gauge_wilson: the Jacobi update (Umu = Fmu after the sweep), or
+        with onthefly the reference's default in-place update in the order
+        of the OpenMP thread grid (ntt, ntx, nty, ntz).  noise: V*4*8
+        Gaussians by link (site lexicographic, mu inner)."""
         N = self.N
         noise = np.ascontiguousarray(noise, dtype=np.float64)
         assert noise.size == self.V * 4 * 8
         plaq = np.zeros((N + 1, 2))
         norm = np.zeros(N)
         tru = np.zeros((4, N, 2))
-        lib().oracle_sweep(self._h, float(dt), _dp(noise), _dp(plaq), _dp(norm), _dp(tru),
-                           1 if zero_modes else 0)
+        if onthefly:
+            g = (ctypes.c_int * 4)(*[int(x) for x in grid])
+            if lib().oracle_sweep_onthefly(self._h, float(dt), _dp(noise), g, _dp(plaq), _dp(norm),
+                                           _dp(tru), 1 if zero_modes else 0) != 0:
+                raise ValueError("thread grid %r rejected" % (tuple(grid),))
+        else:
+            lib().oracle_sweep(self._h, float(dt), _dp(noise), _dp(plaq), _dp(norm), _dp(tru),
+                               1 if zero_modes else 0)
         return SweepObs(plaq, norm, tru)
+
+    def twist_boundary(self):
+        """twist_boundary (nspt.cc:163-255): after an on-the-fly sweep, reads
+        across a twisted face see the current field again."""
+        lib().oracle_twist_boundary(self._h)
 
     def zero_modes(self):
         lib().oracle_zero_modes(self._h)

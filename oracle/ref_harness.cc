@@ -19,11 +19,13 @@
  * with 17 significant digits so that parity checks can read them.
  *
  * Extra options, none of which changes the reference's arithmetic:
- *   --noise FILE   replay a second MyRand with the same seed and dump the
- *                  8 Gaussians SU3rand draws per link (MyMath.cc:256-292), in
- *                  the reference's draw order (site lexicographic, mu inner;
- *                  nspt.cc:365-423 with one thread) -- one record of
- *                  V*4*8 doubles per step;
+ *   --noise FILE   replay second MyRands with the same seeds and dump the
+ *                  8 Gaussians SU3rand draws per link (MyMath.cc:256-292),
+ *                  by link (site lexicographic, mu inner) -- one record of
+ *                  V*4*8 doubles per step.  Thread tid of an OpenMP build
+ *                  draws from Rand[tid] for the sites of its block, in the
+ *                  block's lexicographic order with mu inner (nspt.cc:
+ *                  355-440); with one thread that is the lattice's order;
  *   --twist-init   refresh the twisted copy sites once after a file start
  *                  (Quenched.cc does not; the copies would otherwise hold the
  *                  identity for the first step);
@@ -273,14 +275,10 @@ int main(int argc, char **argv) {
 #endif
 
   FILE *fnoise = NULL;
-  MyRand replay;
+  std::vector<MyRand> replay(NTHR);
   if (!noise_path.empty()) {
-    if (NTHR != 1) {
-      fprintf(stderr, "ref_harness: --noise needs a one-thread build\n");
-      return 2;
-    }
     fnoise = fopen(noise_path.c_str(), "wb");
-    replay.init(seed);
+    for (int tid = 0; tid < NTHR; tid++) replay[tid].init(seed + tid);
   }
 
   /* initial static plaquette (nspt.cc:1316-1406) */
@@ -296,10 +294,19 @@ int main(int argc, char **argv) {
   std::vector<double> step_secs;
   for (int s = 0; s < steps; s++) {
     if (fnoise) {
-      /* same draws, same order as gauge_wilson with one thread */
+      /* the draws of gauge_wilson: each thread's stream over its block */
       size_t n = (size_t)act_pars.iVol * dim * 8;
       double *buf = new double[n];
-      for (size_t k = 0; k < n; k++) buf[k] = replay.generate_gauss();
+      for (int tid = 0; tid < NTHR; tid++)
+        for (int y0 = thr_pars[tid].xi[0]; y0 < thr_pars[tid].xf[0]; y0++)
+          for (int y1 = thr_pars[tid].xi[1]; y1 < thr_pars[tid].xf[1]; y1++)
+            for (int y2 = thr_pars[tid].xi[2]; y2 < thr_pars[tid].xf[2]; y2++)
+              for (int y3 = thr_pars[tid].xi[3]; y3 < thr_pars[tid].xf[3]; y3++) {
+                const size_t site =
+                    y3 + (size_t)sz[3] * (y2 + (size_t)sz[2] * (y1 + (size_t)sz[1] * y0));
+                for (int k = 0; k < dim * 8; k++)
+                  buf[site * dim * 8 + k] = replay[tid].generate_gauss();
+              }
       fwrite(buf, sizeof(double), n, fnoise);
       delete[] buf;
     }

@@ -155,3 +155,46 @@ def test_oracle_improved_action_matches_reference(oracle_mod, action, c1):
         assert np.allclose(r["w2"][s][N], cum, rtol=1e-12, atol=1e-30), s
         o.zero_modes()
     assert per_order_rel(o.links, r["links"], N).max() <= 1e-12
+
+
+@pytest.mark.parametrize("case", [
+    dict(L=(4, 4, 4, 4), N=4, bc="pbc", grid=(1, 1, 1), zm=True, start=None),
+    dict(L=(4, 4, 4, 4), N=4, bc="pbc", grid=(2, 2, 2), zm=True, start=21),
+    dict(L=(4, 4, 4, 4), N=5, bc="tw", grid=(1, 1, 1), zm=False, start=5),
+    dict(L=(4, 4, 4, 4), N=5, bc="tw", grid=(2, 2, 1), zm=False, start=5),
+], ids=["pbc_sequential", "pbc_grid222", "twisted_sequential", "twisted_grid221"])
+def test_oracle_onthefly_matches_reference(oracle_mod, case):
+    """The reference's default build (UPDATE_ONTHEFLY, choices.h:61): links
+    updated in place in the thread grid's order (nspt.cc:355-460), with each
+    OpenMP thread's own noise stream (the harness replays them by link), then
+    zero modes and the local gauge fixing.  With twisted boundaries a read
+    across a twisted face sees the copy site of the last twist_boundary
+    (nspt.cc:989-1027 calls it only at the end of the step): without that
+    the plaquette differs by several per cent."""
+    O = oracle_mod
+    N, grid, alpha, steps, dt = case["N"], case["grid"], -0.05, 3, 0.01
+    b = O.ref_binary(N, case["bc"], "local", grid, update="otf")
+    if not os.path.exists(b):
+        if not os.path.exists(os.path.join(O.reference_dir(), "nspt.cc")):
+            pytest.skip("reference sources not available")
+        b = O.build_reference(N, case["bc"], "local", grid, update="otf")
+    tw = 6 if case["bc"] == "tw" else 0
+    o = O.Oracle(case["L"], N, twist_mask=tw)
+    with tempfile.TemporaryDirectory() as d:
+        start = "cold"
+        if case["start"] is not None:
+            o.random_start(case["start"], 0.5)
+            O.write_config(os.path.join(d, "s.dat"), o.links, o.plaquette())
+            start = os.path.join(d, "s.dat")
+        r = O.run_reference(b, case["L"], steps, dt, alpha, 99, d, start=start,
+                            twist_init=tw != 0)
+    g = (1,) + tuple(grid)
+    for s in range(steps):
+        ob = o.sweep(dt, r["noise"][s], zero_modes=case["zm"], onthefly=True, grid=g)
+        assert obs_close(ob.plaq, r["plaq"][s], 1e-12)[0]
+        assert obs_close(ob.norm, r["norm"][s], 1e-12)[0]
+        if case["zm"]:
+            o.zero_modes()
+        o.local_gauge_fix(alpha, grid=g)
+        o.twist_boundary()
+    assert per_order_rel(o.links, r["links"], N).max() <= 1e-12
