@@ -258,6 +258,11 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def eng_grid(L):
+    """The engine's default thread grid: blocks of 2 sites along even extents."""
+    return tuple(l // 2 if l % 2 == 0 else 1 for l in L)
+
+
 def e2e_leg(args, eng, lib, _lib, P, N, V, world, field_bytes):
     """Upload from pinned host memory, K x (sweep + observables read-back),
     download -- all through the C ABI, wall-clocked on the host."""
@@ -318,7 +323,7 @@ def run_ours(args, world, rank, local):
 
     # local gauge fixing (the reference's default with twisted boundaries) is
     # enabled for the secondary "with_gf" figure; the headline sweeps skip it
-    eng = P.NsptEngine(L, N, twist="yz", local_gf=True, alpha=GF_ALPHA)
+    eng = P.NsptEngine(L, N, twist="yz", local_gf=True, alpha=GF_ALPHA, update=args.update)
     eng.seed(replica_seed(1000, rank), 0)
     eng.cold_start()
 
@@ -376,7 +381,9 @@ def run_ours(args, world, rank, local):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (cold start, device Philox noise)",
             "config": {"workload": "sweep_32^4_N24_twisted_yz", "L": list(L), "N": N,
-                       "dt": args.dt, "bc": "twisted y,z", "update": "Jacobi",
+                       "dt": args.dt, "bc": "twisted y,z",
+                       "update": "Jacobi" if args.update == "jacobi" else
+                                 "on the fly, thread grid %s" % (list(eng_grid(L)),),
                        "gauge_fixing": "none in the timed sweep",
                        "l2": "inputs larger than L2 (field %.1f GB)" % (field_bytes / 1e9),
                        "parallelism": "replicas" if world > 1 else "single"},
@@ -818,7 +825,7 @@ def run_qcfg(args, world, rank, local):
     from prlgt2020_b200.replicas import max_over_ranks, replica_seed, whole_job_rate
     torch.cuda.set_device(local)
     L, N, dt, alpha = (12, 12, 12, 12), 8, 0.005, -0.05
-    eng = P.NsptEngine(L, N, zero_modes=True, local_gf=True, alpha=alpha)
+    eng = P.NsptEngine(L, N, zero_modes=True, local_gf=True, alpha=alpha, update=args.update)
     eng.set_local_gf_form(args.lgf_form)
     eng.seed(replica_seed(8000, rank), 0)
     eng.NsptEvolve(dt, args.warmup, 1)
@@ -834,7 +841,7 @@ def run_qcfg(args, world, rank, local):
             "data": "synthetic (cold start + warm-up, device Philox noise)",
             "config": {"workload": "qcfg_12^4_N8_zm_localgf", "L": list(L), "N": N, "dt": dt,
                        "alpha": alpha, "bc": "periodic", "gf_every": 1,
-                       "local_gf_form": args.lgf_form},
+                       "local_gf_form": args.lgf_form, "update": args.update},
         }
         print(json.dumps(line), flush=True)
     eng.close()
@@ -852,6 +859,9 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
     ap.add_argument("--no-gf", action="store_true", help="skip the gauge-fixing figure")
+    ap.add_argument("--update", default="jacobi", choices=["jacobi", "onthefly"],
+                    help="gauge_wilson update of the sweep and qcfg workloads: Jacobi, or the "
+                         "reference's default in-place update in thread-grid order")
     ap.add_argument("--lgf-form", default="auto", choices=["auto", "group", "team"],
                     help="local gauge fixing kernel of the qcfg workload")
     ap.add_argument("--c4-therm", type=int, default=600,

@@ -62,6 +62,17 @@ extern "C" {
  * accumulations and everything else stay FP64.  No reference counterpart
  * (the reference multiplies in double, QCDpt.h operator*); Wilson action. */
 #define NSPT_PRECISION_FF (1u << 10)
+/* UPDATE_ONTHEFLY (choices.h:61), the reference's default: gauge_wilson
+ * updates every link in place, U = exp(W1) U (nspt.cc:427), in the order of
+ * the OpenMP thread grid set by nspt_set_gf_grid (each thread walks its
+ * block lexicographically, mu inner; barriers as nspt.cc:440-460), so that
+ * a link's staples see the links updated before it.  With twisted
+ * boundaries a read across a twisted face sees the field of the step's
+ * start, as the reference's copy sites do until twist_boundary
+ * (nspt_twist_boundary; nspt_step calls it at the end of every step).
+ * Without the flag: the Jacobi update (F = exp(W1) U, then U = F).
+ * Wilson action, FP64; not with FA gauge fixing on twisted boundaries. */
+#define NSPT_UPDATE_ONTHEFLY (1u << 11)
 
 typedef struct nspt_ctx nspt_ctx;
 
@@ -126,6 +137,12 @@ int nspt_fa_gauge_fixing(nspt_ctx *ctx, double alpha);
  * even extent (1 thread along odd ones).  {1,1,1,1} is the sequential sweep
  * and runs one site at a time. */
 int nspt_local_gauge_fixing(nspt_ctx *ctx, double alpha);
+/* twist_boundary (nspt.cc:163-255): the engine applies twists inside every
+ * neighbour read, so this only matters after an on-the-fly gauge_wilson
+ * (NSPT_UPDATE_ONTHEFLY) on twisted boundaries, whose reads across a
+ * twisted face, and those of a local gauge fixing after it, see the step's
+ * start field until this call.  A no-op otherwise. */
+int nspt_twist_boundary(nspt_ctx *ctx);
 /* grid[d] threads along direction d; every L[d] % grid[d] == 0 and
  * L[d] / grid[d] >= 2 where grid[d] > 1, else NSPT_ERR_ARG. */
 int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]);

@@ -129,7 +129,10 @@ class NsptEngine:
 
     def __init__(self, L, N: int, twist: str = "", zero_modes: bool = False, fa: bool = False,
                  alpha: float = 0.0, local_gf: bool = False, action: str = "wil",
-                 precision: str = "fp64"):
+                 precision: str = "fp64", update: str = "jacobi"):
+        """update: "jacobi" (F = exp(W1) U, then U = F) or "onthefly", the
+        reference's default UPDATE_ONTHEFLY: links updated in place in the
+        order of the OpenMP thread grid (set_gf_grid)."""
         lib = load_library()
         self.L = tuple(int(x) for x in L)
         if len(self.L) != 4:
@@ -148,6 +151,7 @@ class NsptEngine:
         flags |= {"wil": 0, "tlsym": _lib.NSPT_ACTION_TLSYM, "iwa": _lib.NSPT_ACTION_IWA,
                   "dbw2": _lib.NSPT_ACTION_DBW2}[action]
         flags |= {"fp64": 0, "ff": _lib.NSPT_PRECISION_FF}[precision]
+        flags |= {"jacobi": 0, "onthefly": _lib.NSPT_UPDATE_ONTHEFLY}[update]
         self.flags = flags
         self.alpha = float(alpha)
         arr = (ctypes.c_int * 4)(*self.L)
@@ -293,8 +297,12 @@ class NsptEngine:
                     "nspt_set_local_gf_form")
 
     def twist_boundary(self):
-        """No-op: twisted boundaries are applied inside every neighbour read,
-        so there are no copy sites to refresh (nspt.cc:163-255)."""
+        """twist_boundary (nspt.cc:163-255).  Twists are applied inside every
+        neighbour read, so this only ends what an on-the-fly sweep on twisted
+        boundaries leaves: reads across a twisted face seeing the step's start
+        field, as the reference's copy sites do.  NsptEvolve calls it at the
+        end of every step."""
+        self._check(load_library().nspt_twist_boundary(self._h), "nspt_twist_boundary")
 
     def NsptEvolve(self, dt: float, beat: int = 1, gf_every: int = 1):
         """Beat Langevin steps (nspt.cc:953-1039)."""

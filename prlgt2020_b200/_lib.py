@@ -36,6 +36,7 @@ NSPT_ACTION_TLSYM = 1 << 7
 NSPT_ACTION_IWA = 1 << 8
 NSPT_ACTION_DBW2 = 1 << 9
 NSPT_PRECISION_FF = 1 << 10
+NSPT_UPDATE_ONTHEFLY = 1 << 11
 
 # every entry point the header declares: name -> (restype, argtypes)
 _P = ctypes.c_void_p
@@ -61,6 +62,7 @@ SIGNATURES = {
     "nspt_local_gauge_fixing": (_I, [_P, ctypes.c_double]),
     "nspt_set_gf_grid": (_I, [_P, ctypes.POINTER(ctypes.c_int)]),
     "nspt_set_local_gf_form": (_I, [_P, _I]),
+    "nspt_twist_boundary": (_I, [_P]),
     "nspt_observables": (_I, [_P, _D, _D, _D]),
     "nspt_plaquette_measure": (_I, [_P, _D]),
     "nspt_rect_observables": (_I, [_P, _D]),

@@ -49,6 +49,7 @@ int step_body(nspt_ctx *ctx, double dt, int gf_every) {
     if ((rc = do_fa(ctx, ctx->alpha))) return rc;
   if ((ctx->flags & NSPT_GF_LOCAL) && gf_every > 0 && (ctx->counter % gf_every) == 0)
     if ((rc = do_local_gf(ctx, ctx->alpha))) return rc;
+  ctx->snap_valid = false;  // twist_boundary ends the step (nspt.cc:1025-1027)
   return NSPT_OK;
 }
 

@@ -49,6 +49,8 @@ struct nspt_ctx {
   int SS;  // slot stride (double2)
   double2 *U, *Uf, *F, *Ff;
   double2 *Lg;       // per-link logs (zero modes, FA)
+  bool snap_valid;   // on the fly, twisted: F holds the step's start field, which reads
+                     // across a twisted face see until twist_boundary
   bool lg_current;   // Lg holds log U of the current field (after a sweep with
                      // zero modes and after the zero-mode subtraction)
   double2 *Wg, *Gx;  // FA work planes
@@ -253,6 +255,53 @@ static int reduce_sweep_obs(nspt_ctx *ctx) {
   return NSPT_OK;
 }
 
+// The reference's OpenMP thread grid (the context's gf_grid) as the kernels
+// walk it: steps = the number of barrier steps.
+static LgfGrid thread_grid(const nspt_ctx *ctx, long &steps) {
+  LgfGrid gr;
+  gr.dmax = -1;
+  gr.nthr = 1;
+  gr.seg = 1;
+  for (int d = 0; d < 4; d++) {
+    gr.n[d] = ctx->gf_grid[d];
+    gr.bs[d] = ctx->L[d] / gr.n[d];
+    gr.nthr *= gr.n[d];
+    if (gr.n[d] > 1) gr.dmax = d;
+  }
+  steps = 1;
+  for (int d = 0; d < 4; d++) {
+    if (d <= gr.dmax)
+      steps *= gr.bs[d];
+    else
+      gr.seg *= ctx->L[d];
+  }
+  return gr;
+}
+
+// gauge_wilson on the fly (UPDATE_ONTHEFLY, nspt.cc:355-460): one launch per
+// barrier step of the thread grid, one group per reference thread.
+static int launch_sweep_otf(nspt_ctx *ctx, const SweepArgs &a0) {
+  long steps;
+  const LgfGrid gr = thread_grid(ctx, steps);
+  const bool low = use_low(ctx);
+  const int max_warps = (low ? SWEEP_THREADS_LOW : SWEEP_THREADS) / 32;
+  const KernelShape k = choose_shape(ctx, SWEEP_SLOTS, gr.nthr, 0, max_warps, low ? 2 : 1);
+  SweepArgs a = a0;
+  a.gpc = k.warps * LPW;
+  const size_t smem = (size_t)a.gpc * group_bytes(ctx, SWEEP_SLOTS, 0);
+  const unsigned grid = (unsigned)((gr.nthr + a.gpc - 1) / a.gpc);
+  const void *fn = low ? (const void *)k_sweep_otf<true> : (const void *)k_sweep_otf<false>;
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  for (long p = 0; p < steps; p++) {
+    if (low)
+      k_sweep_otf<true><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p);
+    else
+      k_sweep_otf<false><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p);
+  }
+  CK(cudaGetLastError());
+  return NSPT_OK;
+}
+
 static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   SweepArgs a;
   a.U = ctx->U;
@@ -279,6 +328,26 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   a.N = ctx->N;
   a.SS = ctx->SS;
   a.g = ctx->geo;
+  a.Ut = ctx->U;
+  a.Utf = ctx->Uf;
+  const bool otf = (ctx->flags & NSPT_UPDATE_ONTHEFLY) != 0;
+  if (otf) {
+    // in place; with twisted boundaries F keeps the step's start field for
+    // the reads across a twisted face (the reference's copy sites)
+    a.F = ctx->U;
+    a.Ff = ctx->Uf;
+    if (ctx->geo.twist) {
+      if (!ctx->snap_valid) {
+        const size_t nb = (size_t)4 * 9 * ctx->N * ctx->V * sizeof(double2);
+        CK(cudaMemcpyAsync(ctx->F, ctx->U, nb, cudaMemcpyDeviceToDevice, ctx->st));
+        CK(cudaMemcpyAsync(ctx->Ff, ctx->Uf, (size_t)4 * ctx->V * sizeof(double2),
+                           cudaMemcpyDeviceToDevice, ctx->st));
+        ctx->snap_valid = true;
+      }
+      a.Ut = ctx->F;
+      a.Utf = ctx->Ff;
+    }
+  }
   if ((ctx->flags & NSPT_PRECISION_FF) && ctx->ff_auto) {
     // per-order scale of the float-float products, fitted to this field
     CK(cudaMemsetAsync(ctx->ff_mx, 0, ctx->N * sizeof(unsigned long long), ctx->st));
@@ -289,7 +358,9 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   }
   const bool timed = ctx->kcount < nspt_ctx::KEV;
   if (timed) CK(cudaEventRecord(ctx->kev[2 * ctx->kcount], ctx->st));
-  int rc = ctx->c1 != 0.0 ? launch_sweep_imp(ctx, a) : launch_sweep(ctx, a, false);
+  int rc = otf                 ? launch_sweep_otf(ctx, a)
+           : ctx->c1 != 0.0    ? launch_sweep_imp(ctx, a)
+                               : launch_sweep(ctx, a, false);
   if (rc) return rc;
   if (timed) {
     CK(cudaEventRecord(ctx->kev[2 * ctx->kcount + 1], ctx->st));
@@ -299,8 +370,10 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   if (rc) return rc;
   k_inc<<<1, 1, 0, ctx->st>>>(ctx->dcounter);
   CK(cudaGetLastError());
-  std::swap(ctx->U, ctx->F);
-  std::swap(ctx->Uf, ctx->Ff);
+  if (!otf) {
+    std::swap(ctx->U, ctx->F);
+    std::swap(ctx->Uf, ctx->Ff);
+  }
   ctx->counter++;
   ctx->have_obs = true;
   ctx->lg_current = a.Lg != nullptr;  // the sweep stored log U' per link
@@ -498,27 +571,15 @@ static int do_fa(nspt_ctx *ctx, double alpha) {
 // stochastic_gauge_fixing (nspt.cc:660-862) with the context's thread
 // grid: one launch per barrier step, one group per reference thread.
 static int do_local_gf(nspt_ctx *ctx, double alpha) {
-  LgfGrid gr;
-  gr.dmax = -1;
-  gr.nthr = 1;
-  gr.seg = 1;
-  for (int d = 0; d < 4; d++) {
-    gr.n[d] = ctx->gf_grid[d];
-    gr.bs[d] = ctx->L[d] / gr.n[d];
-    gr.nthr *= gr.n[d];
-    if (gr.n[d] > 1) gr.dmax = d;
-  }
-  long steps = 1;
-  for (int d = 0; d < 4; d++) {
-    if (d <= gr.dmax)
-      steps *= gr.bs[d];
-    else
-      gr.seg *= ctx->L[d];
-  }
+  long steps;
+  const LgfGrid gr = thread_grid(ctx, steps);
   const int N = ctx->N, SS = ctx->SS;
   const Geo geo = ctx->geo;
   cudaStream_t st = ctx->st;
   double2 *U = ctx->U, *Uf = ctx->Uf;
+  // reads across a twisted face: the step's start field after an on-the-fly
+  // sweep (the reference's copy sites before twist_boundary)
+  const double2 *Ut = ctx->snap_valid ? ctx->F : U, *Utf = ctx->snap_valid ? ctx->Ff : Uf;
   const bool low = use_low(ctx);
   ctx->lg_current = false;
   // The team form (a warp of three groups per reference thread) shortens
@@ -539,9 +600,11 @@ static int do_local_gf(nspt_ctx *ctx, double alpha) {
     const unsigned grid = (unsigned)((gr.nthr + team_warps - 1) / team_warps);
     for (long p = 0; p < steps; p++) {
       if (low)
-        k_local_gf_team<true><<<grid, 32 * team_warps, smem, st>>>(U, Uf, N, SS, geo, alpha, gr, p);
+        k_local_gf_team<true><<<grid, 32 * team_warps, smem, st>>>(U, Uf, Ut, Utf, N, SS, geo,
+                                                                    alpha, gr, p);
       else
-        k_local_gf_team<false><<<grid, 32 * team_warps, smem, st>>>(U, Uf, N, SS, geo, alpha, gr, p);
+        k_local_gf_team<false><<<grid, 32 * team_warps, smem, st>>>(U, Uf, Ut, Utf, N, SS, geo,
+                                                                     alpha, gr, p);
     }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
@@ -555,9 +618,9 @@ static int do_local_gf(nspt_ctx *ctx, double alpha) {
         ctx, low ? (const void *)k_local_gf<true> : (const void *)k_local_gf<false>, 4, gr.nthr,
         [&](unsigned g, dim3 b, size_t sm) {
           if (low)
-            k_local_gf<true><<<g, b, sm, st>>>(U, Uf, N, SS, geo, alpha, gr, p);
+            k_local_gf<true><<<g, b, sm, st>>>(U, Uf, Ut, Utf, N, SS, geo, alpha, gr, p);
           else
-            k_local_gf<false><<<g, b, sm, st>>>(U, Uf, N, SS, geo, alpha, gr, p);
+            k_local_gf<false><<<g, b, sm, st>>>(U, Uf, Ut, Utf, N, SS, geo, alpha, gr, p);
         },
         "local gauge fixing", 0, low);
     if (rc) return rc;
@@ -637,8 +700,11 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   if (N < 1 || N > NSPT_MAX_ORDER) return NSPT_ERR_ORDER;
   const unsigned actions = NSPT_ACTION_TLSYM | NSPT_ACTION_IWA | NSPT_ACTION_DBW2;
   const unsigned known = NSPT_TWIST_Y | NSPT_TWIST_Z | NSPT_TWIST_T | NSPT_ZEROMODE | NSPT_GF_FA |
-                         NSPT_GF_LOCAL | actions | NSPT_PRECISION_FF;
+                         NSPT_GF_LOCAL | actions | NSPT_PRECISION_FF | NSPT_UPDATE_ONTHEFLY;
   if (flags & ~known) return NSPT_ERR_ARG;
+  // the on-the-fly update is built for the FP64 Wilson sweep
+  if ((flags & NSPT_UPDATE_ONTHEFLY) && (flags & (NSPT_PRECISION_FF | actions)))
+    return NSPT_ERR_ARG;
   // float-float products are built into the Wilson sweep only
   if ((flags & NSPT_PRECISION_FF) && (flags & actions)) return NSPT_ERR_ARG;
   if (__builtin_popcount(flags & actions) > 1) return NSPT_ERR_ARG;
@@ -671,6 +737,7 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   ctx->sweep_warps = 0;
   ctx->shape_mo = 0;
   ctx->lg_current = false;
+  ctx->snap_valid = false;
   ctx->launch_gen = 0;
   ctx->loop_part = nullptr;
   ctx->loop_part_n = 0;
@@ -1078,8 +1145,15 @@ extern "C" int nspt_step(nspt_ctx *ctx, double dt, int nsteps, int gf_every) {
       if ((rc = do_fa(ctx, ctx->alpha))) return rc;
     if ((ctx->flags & NSPT_GF_LOCAL) && gf_every > 0 && ((ctx->counter % gf_every) == 0))
       if ((rc = do_local_gf(ctx, ctx->alpha))) return rc;
+    ctx->snap_valid = false;  // twist_boundary ends the step (nspt.cc:1025-1027)
   }
   return timed_end(ctx);
+}
+
+extern "C" int nspt_twist_boundary(nspt_ctx *ctx) {
+  if (!ctx) return NSPT_ERR_ARG;
+  ctx->snap_valid = false;
+  return NSPT_OK;
 }
 
 extern "C" double nspt_last_step_ms(const nspt_ctx *ctx) { return ctx ? ctx->last_ms : 0.0; }

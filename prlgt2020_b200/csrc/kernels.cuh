@@ -229,6 +229,10 @@ struct SweepArgs {
   int N, SS;
   int gpc;             // link groups per CTA of the sweep, dealt to its warps as evenly
                        // as possible (sweep_group)
+  // on-the-fly update: what a read across a twisted face sees, the field of
+  // the step's start (the reference's copy sites, refreshed by
+  // twist_boundary only); the Jacobi sweep reads U there too
+  const double2 *Ut, *Utf;
   Geo g;
 };
 
@@ -302,7 +306,7 @@ __device__ __forceinline__ void sweep_link(const Geo &g, long u, int &mu, int &s
 // U_mu(x) in slot Y, observables written: W1 = reH(W1) tau_g - stau eta,
 // F = exp(W1) U_mu(x), and the per-link log for the zero modes.  W is a
 // free slot.  Shared by the Wilson and the improved-action sweeps.
-template <int MOx = MO>
+template <int MOx = MO, bool RW = false>
 __device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, double2 *Y, double2 *W,
                                             long link, int mu, int site, const Nb &self,
                                             const Lane &L) {
@@ -340,7 +344,7 @@ __device__ __forceinline__ void update_link(const SweepArgs &a, double2 *T, doub
   // ---- F = exp(W1) * U  (nspt.cc:429): exp into Y (W holds the square of
   // W1), U_mu(x) restaged into W
   ser_exp<MOx>(T, W, Y, N, L);
-  stage(W, a.U, a.Uf, mu, self, a.g, N, L);
+  stage<RW>(W, a.U, a.Uf, mu, self, a.g, N, L);
   const bool zm = a.Lg != nullptr;
   double2 *Fc = a.F + (size_t)mu * plane_mu + site;
   product<MOx, false>(LeftS{Y}, make_double2(1.0, 0.0), W, W[0], N, L,
@@ -415,23 +419,73 @@ __device__ __noinline__ double2 slot_acc(double2 *Wacc, const double2 *T, const 
 constexpr int MO_LOW = 4;
 constexpr int SWEEP_THREADS_LOW = 192;
 
-template <bool MEASURE, bool FF = false, bool LOW = false>
-__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ? 2 : 1)
-    k_sweep(SweepArgs a) {
+// Thread grid of the reference's OpenMP build (choices.h:124-128): n[d]
+// threads along direction d (ntt, ntx, nty, ntz), blocks of bs[d] sites
+// (Quenched.cc:518-531).  Threads take a barrier after every iteration of
+// the deepest split direction dmax (nspt.cc:796-815); between two barriers a
+// thread walks a segment of seg sites.
+struct LgfGrid {
+  int n[4], bs[4];
+  int dmax;   // -1 when no direction is split
+  int nthr;
+  long seg;
+};
+
+// The sites one reference thread visits in one barrier step of
+// stochastic_gauge_fixing (nspt.cc:731-828): thread tid owns block b of the
+// grid; the barrier step fixes the offset rel inside the split directions;
+// the directions that are not split are walked whole, the last fastest.
+struct LgfWalk {
+  int b[4], rel[4];
+  __device__ __forceinline__ LgfWalk(const LgfGrid &gr, long tid, long step) {
+    b[0] = (int)(tid / ((long)gr.n[1] * gr.n[2] * gr.n[3]));
+    b[1] = (int)((tid / ((long)gr.n[2] * gr.n[3])) % gr.n[1]);
+    b[2] = (int)((tid / gr.n[3]) % gr.n[2]);
+    b[3] = (int)(tid % gr.n[3]);
+    for (int d = 0; d < 4; d++) rel[d] = 0;
+    long q = step;
+    for (int d = gr.dmax; d >= 0; d--) {
+      rel[d] = (int)(q % gr.bs[d]);
+      q /= gr.bs[d];
+    }
+  }
+  // coordinates of the r-th site of the walk
+  __device__ __forceinline__ void site(const LgfGrid &gr, const Geo &geo, long r, int *x) const {
+    long t = r;
+    for (int d = 3; d >= 0; d--) {
+      if (d <= gr.dmax) {
+        x[d] = gr.bs[d] * b[d] + rel[d];
+      } else {
+        x[d] = (int)(t % geo.L[d]);
+        t /= geo.L[d];
+      }
+    }
+  }
+};
+
+// A neighbour link of the sweep into a slot.  OTF (on-the-fly update, the
+// field changing inside the kernel): coherent loads, and a read across a
+// twisted face from the step's start field.
+template <bool OTF>
+__device__ __forceinline__ void sweep_stage(double2 *slot, const SweepArgs &a, int mu, Nb n,
+                                            int N, const Lane &L, bool dag = false) {
+  if constexpr (OTF) {
+    const bool cross = ((n.fwd | n.bwd) & a.g.twist) != 0;
+    stage<true>(slot, cross ? a.Ut : a.U, cross ? a.Utf : a.Uf, mu, n, a.g, N, L, dag);
+  } else {
+    stage(slot, a.U, a.Uf, mu, n, a.g, N, L, dag);
+  }
+}
+
+// The update of link (mu, site) by one group: staples, force, observables,
+// noise, exp, the new link into a.F (a.U itself on the fly) and its log.
+template <bool MEASURE, bool FF, bool LOW, bool OTF>
+__device__ __forceinline__ void sweep_one(const SweepArgs &a, const Lane &L, double2 *T,
+                                          double2 *Y, double2 *W, int mu, int site) {
   constexpr int MOK = LOW ? MO_LOW : MO;
   const int ffe = FF ? *a.ff_scale : 0;
-  extern __shared__ double2 sm[];
-  Lane L;
-  int gi;
-  if (!sweep_group(L, gi, a.gpc)) return;
-  const int N = a.N, SS = a.SS, c = L.c;
+  const int N = a.N, c = L.c;
   const size_t V = (size_t)a.g.V;
-  double2 *T = sm + (size_t)gi * (SWEEP_SLOTS * SS), *Y = T + SS;
-  double2 *W = Y + SS;
-  const long unit = (long)blockIdx.x * a.gpc + gi;
-  if (unit >= 4L * a.g.V) return;  // groups are independent: a group past the end has no work
-  int mu, site;
-  sweep_link(a.g, unit, mu, site);
   const long link = (long)mu * a.g.V + site;
   int x[4];
   coords(a.g, site, x);
@@ -484,25 +538,25 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ?
     {
       const Nb m = neighbour(a.g, x, mu, 1);
       const Nb b = neighbour(a.g, x, nu, 1);
-      stage(T, a.U, a.Uf, nu, m, a.g, N, L);
-      stage(Y, a.U, a.Uf, mu, b, a.g, N, L, true);
+      sweep_stage<OTF>(T, a, nu, m, N, L);
+      sweep_stage<OTF>(Y, a, mu, b, N, L, true);
       mul(T, Y);
-      stage(Y, a.U, a.Uf, nu, self, a.g, N, L, true);
+      sweep_stage<OTF>(Y, a, nu, self, N, L, true);
       acc(T, Y);
     }
     {
       const Nb d = neighbour(a.g, x, nu, -1);
       const Nb dm = neighbour(a.g, x, nu, -1, mu, 1);
-      stage(T, a.U, a.Uf, nu, dm, a.g, N, L, true);
-      stage(Y, a.U, a.Uf, mu, d, a.g, N, L, true);
+      sweep_stage<OTF>(T, a, nu, dm, N, L, true);
+      sweep_stage<OTF>(Y, a, mu, d, N, L, true);
       mul(T, Y);
-      stage(Y, a.U, a.Uf, nu, d, a.g, N, L);
+      sweep_stage<OTF>(Y, a, nu, d, N, L);
       acc(T, Y);
     }
   }
   if (L.j == 0) W[0] = wflag;
   // ---- P = U_mu(x) * staples (nspt.cc:392) into T; U_mu(x) in Y
-  stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
+  sweep_stage<OTF>(Y, a, mu, self, N, L);
   const double2 pflag = flag_mul(Y[0], wflag);
   cprod<FF, MOK, false>(LeftS{Y}, Y[0], W, wflag, N, L, ffe,
                      [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
@@ -535,7 +589,65 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ?
   }
   if constexpr (MEASURE) return;
   __syncwarp(L.mask);
-  update_link<MOK>(a, T, Y, W, link, mu, site, self, L);
+  update_link<MOK, OTF>(a, T, Y, W, link, mu, site, self, L);
+}
+
+template <bool MEASURE, bool FF = false, bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ? 2 : 1)
+    k_sweep(SweepArgs a) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int gi;
+  if (!sweep_group(L, gi, a.gpc)) return;
+  const int SS = a.SS;
+  double2 *T = sm + (size_t)gi * (SWEEP_SLOTS * SS), *Y = T + SS;
+  double2 *W = Y + SS;
+  const long unit = (long)blockIdx.x * a.gpc + gi;
+  if (unit >= 4L * a.g.V) return;  // groups are independent: a group past the end has no work
+  int mu, site;
+  sweep_link(a.g, unit, mu, site);
+  sweep_one<MEASURE, FF, LOW, false>(a, L, T, Y, W, mu, site);
+}
+
+// One on-the-fly link update, out of line: the walk's state stays outside
+// the update's registers.
+template <bool LOW>
+__device__ __noinline__ void sweep_one_otf(const SweepArgs &a, const Lane &L, double2 *T,
+                                           double2 *Y, double2 *W, int mu, int site) {
+  sweep_one<false, false, LOW, true>(a, L, T, Y, W, mu, site);
+}
+
+// gauge_wilson with UPDATE_ONTHEFLY, the reference's default (choices.h:61,
+// nspt.cc:355-460): one barrier step of its OpenMP thread grid.  One group
+// per reference thread walks that thread's sites (LgfWalk) and updates
+// their links in place, mu = 0..3, each seeing the links updated before it;
+// the threads of one barrier step touch disjoint links.  Reads across a
+// twisted face come from a.Ut (the step's start field).
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ? 2 : 1)
+    k_sweep_otf(SweepArgs a, LgfGrid gr, long step) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int gi;
+  if (!sweep_group(L, gi, a.gpc)) return;
+  const int SS = a.SS;
+  double2 *T = sm + (size_t)gi * (SWEEP_SLOTS * SS), *Y = T + SS;
+  double2 *W = Y + SS;
+  const long tid = (long)blockIdx.x * a.gpc + gi;
+  if (tid >= gr.nthr) return;
+  const LgfWalk walk(gr, tid, step);
+#pragma unroll 1
+  for (long r = 0; r < gr.seg; r++) {
+    int x[4];
+    walk.site(gr, a.g, r, x);
+    const int site = x[0] * a.g.s0 + x[1] * a.g.s1 + x[2] * a.g.s2 + x[3];
+#pragma unroll 1
+    for (int mu = 0; mu < 4; mu++) {
+      sweep_one_otf<LOW>(a, L, T, Y, W, mu, site);
+      // the next link's stagings read what this one wrote
+      __syncwarp(L.mask);
+    }
+  }
 }
 
 // ---------------- improved gauge actions ----------------
@@ -931,50 +1043,6 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
 
 // ---------------- local stochastic gauge fixing ----------------
 
-// Thread grid of the reference's OpenMP build (choices.h:124-128): n[d]
-// threads along direction d (ntt, ntx, nty, ntz), blocks of bs[d] sites
-// (Quenched.cc:518-531).  Threads take a barrier after every iteration of
-// the deepest split direction dmax (nspt.cc:796-815); between two barriers a
-// thread walks a segment of seg sites.
-struct LgfGrid {
-  int n[4], bs[4];
-  int dmax;   // -1 when no direction is split
-  int nthr;
-  long seg;
-};
-
-// The sites one reference thread visits in one barrier step of
-// stochastic_gauge_fixing (nspt.cc:731-828): thread tid owns block b of the
-// grid; the barrier step fixes the offset rel inside the split directions;
-// the directions that are not split are walked whole, the last fastest.
-struct LgfWalk {
-  int b[4], rel[4];
-  __device__ __forceinline__ LgfWalk(const LgfGrid &gr, long tid, long step) {
-    b[0] = (int)(tid / ((long)gr.n[1] * gr.n[2] * gr.n[3]));
-    b[1] = (int)((tid / ((long)gr.n[2] * gr.n[3])) % gr.n[1]);
-    b[2] = (int)((tid / gr.n[3]) % gr.n[2]);
-    b[3] = (int)(tid % gr.n[3]);
-    for (int d = 0; d < 4; d++) rel[d] = 0;
-    long q = step;
-    for (int d = gr.dmax; d >= 0; d--) {
-      rel[d] = (int)(q % gr.bs[d]);
-      q /= gr.bs[d];
-    }
-  }
-  // coordinates of the r-th site of the walk
-  __device__ __forceinline__ void site(const LgfGrid &gr, const Geo &geo, long r, int *x) const {
-    long t = r;
-    for (int d = 3; d >= 0; d--) {
-      if (d <= gr.dmax) {
-        x[d] = gr.bs[d] * b[d] + rel[d];
-      } else {
-        x[d] = (int)(t % geo.L[d]);
-        t /= geo.L[d];
-      }
-    }
-  }
-};
-
 // A <- A - A^dag, then Trless (W -= dag(W); W.Trless(), nspt.cc:679-682,
 // QCDpt.cc:124-136 and 185-194): flag 0.  Lanes split the orders.
 __device__ __forceinline__ void ser_aherm_trless(double2 *P, int N, const Lane &L) {
@@ -1010,8 +1078,8 @@ __device__ __forceinline__ void ser_aherm_trless(double2 *P, int N, const Lane &
 // face, nspt.cc:690-719).  Four slots per group.
 template <bool LOW = false>
 __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
-    k_local_gf(double2 *U, double2 *Uf, int N, int SS, Geo geo, double alpha, LgfGrid gr,
-               long step) {
+    k_local_gf(double2 *U, double2 *Uf, const double2 *Ut, const double2 *Utf, int N, int SS,
+               Geo geo, double alpha, LgfGrid gr, long step) {
   extern __shared__ double2 sm[];
   Lane L;
   int g;
@@ -1034,7 +1102,9 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
     // W = sum_mu U_mu(x) - U_mu(x-mu)  (nspt.cc:672-675)
     for (int mu = 0; mu < 4; mu++) {
       stage<true>(Y2, U, Uf, mu, self, geo, N, L);
-      stage<true>(E1, U, Uf, mu, neighbour(geo, x, mu, -1), geo, N, L);
+      const Nb bn = neighbour(geo, x, mu, -1);
+      const bool cross = (bn.bwd & geo.twist) != 0;
+      stage<true>(E1, cross ? Ut : U, cross ? Utf : Uf, mu, bn, geo, N, L);
       for (int e = L.j; e < 1 + 9 * N; e += GROUP)
         A[e] = cadd(mu == 0 ? cz() : A[e], csub(Y2[e], E1[e]));
       __syncwarp(L.mask);
@@ -1137,8 +1207,8 @@ constexpr int LGF_TEAM_SLOTS = 15;
 
 template <bool LOW = false>
 __global__ void __launch_bounds__(64, LOW ? 5 : 4)
-    k_local_gf_team(double2 *U, double2 *Uf, int N, int SS, Geo geo, double alpha, LgfGrid gr,
-                    long step) {
+    k_local_gf_team(double2 *U, double2 *Uf, const double2 *Ut, const double2 *Utf, int N,
+                    int SS, Geo geo, double alpha, LgfGrid gr, long step) {
   constexpr int MOK = LOW ? MO_LOW : MO;
   constexpr int TEAM = LPW * GROUP;
   extern __shared__ double2 sm[];
@@ -1165,8 +1235,13 @@ __global__ void __launch_bounds__(64, LOW ? 5 : 4)
     const int self = x[0] * geo.s0 + x[1] * geo.s1 + x[2] * geo.s2 + x[3];
     for (int t = g; t < 8; t += LPW) {
       const int mu = t & 3;
-      stage_issue(S + (size_t)t * SS, U, Uf, mu, t < 4 ? self : neighbour(geo, x, mu, -1).site,
-                  V, N, L);
+      const Nb bn = neighbour(geo, x, mu, -1);
+      stage_issue(S + (size_t)t * SS, U, Uf, mu, t < 4 ? self : bn.site, V, N, L);
+      // a back link read across a twisted face, as the step's start field
+      // holds it (the same as U except after an on-the-fly sweep); the
+      // scratch slots are free until the link products
+      if (t >= 4 && Ut != U && (bn.bwd & geo.twist))
+        stage_issue(E2 + (size_t)mu * SS, Ut, Utf, mu, bn.site, V, N, L);
     }
     cp_commit();
     cp_wait0();
@@ -1177,8 +1252,9 @@ __global__ void __launch_bounds__(64, LOW ? 5 : 4)
 #pragma unroll
       for (int mu = 0; mu < 4; mu++) {
         const double2 *f = S + (size_t)mu * SS + 1 + 9 * (k - 1);
-        const double2 *bk = S + (size_t)(4 + mu) * SS + 1 + 9 * (k - 1);
         const unsigned tb = neighbour(geo, x, mu, -1).bwd & geo.twist;
+        const double2 *bk = (tb && Ut != U ? E2 + (size_t)mu * SS : S + (size_t)(4 + mu) * SS) +
+                            1 + 9 * (k - 1);
         double2 bv[9];
         if (tb) {
           double2 m[9];

@@ -27,7 +27,9 @@
 // REMOVE_GLUON_ZEROMOM), -A tlsym|iwa|dbw2 an improved gauge action
 // (GAUGE_ACTION; file names and the plaquette file's extra two columns of
 // rectangle traces follow Quenched.cc:327-348 and nspt.cc:586-597), -P
-// device Philox noise instead of the reference's rand55 stream.  The update is the Jacobi one (UPDATE_ONTHEFLY off).
+// device Philox noise instead of the reference's rand55 stream, -O the
+// reference's default on-the-fly update (UPDATE_ONTHEFLY: links updated in
+// place in the thread grid's order); without -O the Jacobi update.
 // With periodic boundaries the Wilson loops of ComputeLoops (__MANY_LOOP__,
 // the reference's periodic default) go to <plaq_out>_nxm_SU3_wil_..._o<N>.txt
 // after every BEAT steps and at the end (nspt.cc:1283-1306); with -W also
@@ -57,7 +59,7 @@ struct Params {
   long seed = 0;
   std::string plaqn, confn, damon = "damocle.dag";
   unsigned twist = 0;
-  bool fa = false, philox = false, wl2x2 = false;
+  bool fa = false, philox = false, wl2x2 = false, otf = false;
   int zm = -1;  // -1: as the boundary conditions imply
   int grid[4] = {0, 0, 0, 0};
   unsigned action = 0;  // NSPT_ACTION_* or 0 (Wilson)
@@ -130,6 +132,7 @@ void usage() {
          "-Z 0|1\t\tzero-mode subtraction off/on\n"
          "-A action\timproved gauge action: tlsym, iwa or dbw2\n"
          "-P\t\tdevice Philox noise instead of the reference's generator\n"
+         "-O\t\ton-the-fly update (UPDATE_ONTHEFLY) in the thread grid's order\n"
          "-W\t\t2x2 Wilson loops file (WL2x2, periodic boundaries)\n\n");
 }
 
@@ -210,7 +213,7 @@ int main(int argc, char **argv) {
     }
   if (!read_cfg(p)) return 1;
   int opt;
-  while ((opt = getopt(argc, argv, "l:s:b:d:r:g:a:t:p:c:n:hT:FG:Z:PA:W")) != -1) {
+  while ((opt = getopt(argc, argv, "l:s:b:d:r:g:a:t:p:c:n:hT:FG:Z:PA:WO")) != -1) {
     switch (opt) {
       case 'l': p.L[0] = p.L[1] = p.L[2] = p.L[3] = atoi(optarg); break;
       case 's': p.sweep = atoi(optarg); break;
@@ -244,6 +247,7 @@ int main(int argc, char **argv) {
       case 'Z': p.zm = atoi(optarg); break;
       case 'P': p.philox = true; break;
       case 'W': p.wl2x2 = true; break;
+      case 'O': p.otf = true; break;
       case 'A':
         if (!strcmp(optarg, "tlsym")) p.action = NSPT_ACTION_TLSYM;
         else if (!strcmp(optarg, "iwa")) p.action = NSPT_ACTION_IWA;
@@ -271,7 +275,7 @@ int main(int argc, char **argv) {
   const bool periodic = p.twist == 0;
   const bool zm = p.zm < 0 ? periodic : p.zm != 0;
   unsigned flags = p.twist | (zm ? NSPT_ZEROMODE : 0u) | (p.fa ? NSPT_GF_FA : NSPT_GF_LOCAL) |
-                   p.action;
+                   p.action | (p.otf ? NSPT_UPDATE_ONTHEFLY : 0u);
 
   // file names (Quenched.cc:376-407)
   const char *type = p.action == NSPT_ACTION_TLSYM  ? "SU3_tls"
@@ -307,7 +311,8 @@ int main(int argc, char **argv) {
     fprintf(stderr, "nspt_quenched: cannot open the output files\n");
     return 1;
   }
-  fprintf(logf, "Gauge group\t\tSU3\n\tgauge field update not \"on the fly\"\n");
+  fprintf(logf, "Gauge group\t\tSU3\n\tgauge field update %s\"on the fly\"\n",
+          p.otf ? "" : "not ");
   fprintf(logf, "Gauge field boundary conditions\t\t%s\n", periodic ? "PERIODIC" : "TWISTED");
   fprintf(logf,
           "Taglia\t\t%d %d %d %d\nSweep\t\t%d\nBeat\t\t%d\nTau_g\t\t%g\nAlpha\t\t%g\n"
@@ -399,6 +404,7 @@ int main(int argc, char **argv) {
       else
         rc = nspt_local_gauge_fixing(ctx, p.alpha);
       if (rc) return fail(ctx, rc, "gauge fixing");
+      if ((rc = nspt_twist_boundary(ctx))) return fail(ctx, rc, "twist_boundary");
       done++;
     }
     fflush(plaqf);
