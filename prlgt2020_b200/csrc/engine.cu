@@ -290,13 +290,27 @@ static int launch_sweep_otf(nspt_ctx *ctx, const SweepArgs &a0) {
   a.gpc = k.warps * LPW;
   const size_t smem = (size_t)a.gpc * group_bytes(ctx, SWEEP_SLOTS, 0);
   const unsigned grid = (unsigned)((gr.nthr + a.gpc - 1) / a.gpc);
-  const void *fn = low ? (const void *)k_sweep_otf<true> : (const void *)k_sweep_otf<false>;
-  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  for (long p = 0; p < steps; p++) {
-    if (low)
-      k_sweep_otf<true><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p);
-    else
-      k_sweep_otf<false><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p);
+  if (gr.seg == 1) {
+    // one site per thread and barrier step: a launch per (step, mu), the
+    // link update inline without a loop around it
+    const void *fn = low ? (const void *)k_sweep_otf1<true> : (const void *)k_sweep_otf1<false>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    for (long p = 0; p < steps; p++)
+      for (int mu = 0; mu < 4; mu++) {
+        if (low)
+          k_sweep_otf1<true><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, mu);
+        else
+          k_sweep_otf1<false><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, mu);
+      }
+  } else {
+    const void *fn = low ? (const void *)k_sweep_otf<true> : (const void *)k_sweep_otf<false>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    for (long p = 0; p < steps; p++) {
+      if (low)
+        k_sweep_otf<true><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p);
+      else
+        k_sweep_otf<false><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p);
+    }
   }
   CK(cudaGetLastError());
   return NSPT_OK;

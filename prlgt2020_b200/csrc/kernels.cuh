@@ -609,6 +609,29 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ?
   sweep_one<MEASURE, FF, LOW, false>(a, L, T, Y, W, mu, site);
 }
 
+// gauge_wilson on the fly, for a thread grid whose threads own one site per
+// barrier step (every direction up to the last split one is split: the
+// default grid of blocks of 2): link mu of each thread's site for barrier
+// step `step`, one launch per (step, mu) in that order, the update inline
+// as in k_sweep.
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ? 2 : 1)
+    k_sweep_otf1(SweepArgs a, LgfGrid gr, long step, int mu) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int gi;
+  if (!sweep_group(L, gi, a.gpc)) return;
+  const int SS = a.SS;
+  double2 *T = sm + (size_t)gi * (SWEEP_SLOTS * SS), *Y = T + SS;
+  double2 *W = Y + SS;
+  const long tid = (long)blockIdx.x * a.gpc + gi;
+  if (tid >= gr.nthr) return;
+  int x[4];
+  LgfWalk(gr, tid, step).site(gr, a.g, 0, x);
+  const int site = x[0] * a.g.s0 + x[1] * a.g.s1 + x[2] * a.g.s2 + x[3];
+  sweep_one<false, false, LOW, true>(a, L, T, Y, W, mu, site);
+}
+
 // One on-the-fly link update, out of line: the walk's state stays outside
 // the update's registers.
 template <bool LOW>
