@@ -50,6 +50,11 @@ CASES = [
     # the 16^4 x 20 workload's step: 20 orders, zero modes + FA every step
     dict(name="rand_pbc_zm_fa_n20", L=(4, 4, 4, 4), N=20, bc="pbc", gf="fa", steps=2,
          dt=0.01, alpha=0.05, seed=2020, start=20, zm=True),
+    # the reference's default on-the-fly update (UPDATE_ONTHEFLY), one thread
+    dict(name="rand_pbc_otf_localgf_n6", L=(4, 4, 4, 4), N=6, bc="pbc", gf="local", steps=3,
+         dt=0.01, alpha=-0.05, seed=61, start=16, zm=True, update="otf"),
+    dict(name="rand_tw_otf_localgf_n5", L=(4, 4, 4, 4), N=5, bc="tw", gf="local", steps=3,
+         dt=0.01, alpha=-0.05, seed=62, start=17, zm=False, update="otf"),
 ]
 C1 = {"wil": 0.0, "tlsym": -1.0 / 12.0, "iwa": -0.331, "dbw2": -1.4088}
 
@@ -58,7 +63,8 @@ LINK_SITES = 6  # sites of the final field kept in the fixture
 
 def make_case(c: dict) -> dict:
     action = c.get("action", "wil")
-    binary = O.build_reference(c["N"], c["bc"], c["gf"], (1, 1, 1), action)
+    binary = O.build_reference(c["N"], c["bc"], c["gf"], (1, 1, 1), action,
+                               c.get("update", "jacobi"))
     with tempfile.TemporaryDirectory() as d:
         start = "cold"
         twist_mask = 6 if c["bc"] == "tw" else 0
@@ -117,7 +123,8 @@ def main():
                             dt=c["dt"], alpha=c["alpha"], seed=c["seed"],
                             start=-1 if c["start"] is None else c["start"],
                             twisted=c["bc"] == "tw", fa=c["gf"] == "fa", zm=c["zm"],
-                            local_gf=c["gf"] == "local" and c["alpha"] != 0.0)
+                            local_gf=c["gf"] == "local" and c["alpha"] != 0.0,
+                            onthefly=c.get("update", "jacobi") == "otf")
         meta.append((c["name"], os.path.getsize(path)))
     for name, size in meta:
         print("%-28s %8d bytes" % (name, size))

@@ -96,6 +96,8 @@ def test_driver_replays_reference_fixture(driver, oracle_mod, tmp_path, path):
         args += ["-Z", "0"]
     if action != "wil":
         args += ["-A", action]
+    if "onthefly" in g and bool(g["onthefly"]):
+        args += ["-O"]
     r = subprocess.run(args, cwd=tmp_path, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     raw = np.loadtxt(tmp_path / ("plaq_" + name + ".txt"))

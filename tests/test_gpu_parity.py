@@ -220,11 +220,13 @@ def test_reference_golden_fixture(engine_mod, oracle_mod, path):
     o = oracle_mod.Oracle(L, N, twist_mask=6 if twist else 0)
     if int(g["start"]) >= 0:
         o.random_start(int(g["start"]), 0.5)
-    e = engine_mod.NsptEngine(L, N, twist=twist, zero_modes=zm, fa=fa, alpha=alpha, action=action)
+    otf = "onthefly" in g and bool(g["onthefly"])
+    e = engine_mod.NsptEngine(L, N, twist=twist, zero_modes=zm, fa=fa, alpha=alpha, action=action,
+                              update="onthefly" if otf else "jacobi")
     e.upload(o.links)
     ok, w = obs_close(e.plaquette_measure(), g["plaq0"], 1e-12)
     assert ok, ("start plaquette", w)
-    if local_gf:
+    if local_gf or otf:
         e.set_gf_grid((1, 1, 1, 1))  # the fixture's reference build runs one thread
     rng = oracle_mod.Rand55(int(g["seed"]))
     for s in range(int(g["steps"])):
@@ -243,6 +245,7 @@ def test_reference_golden_fixture(engine_mod, oracle_mod, path):
             e.FAstochastic_gauge_fixing(alpha)
         if local_gf:
             e.stochastic_gauge_fixing(alpha)
+        e.twist_boundary()
     rel = per_order_rel(e.download()[: g["links"].shape[0]], g["links"], N)
     bound = cold_bound(N, 1e-11) if (zm and int(g["start"]) < 0) else 1e-11
     assert np.all(rel <= bound), rel

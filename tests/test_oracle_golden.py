@@ -30,7 +30,8 @@ def replay(O, g):
         nz = rng.gauss(o.V * 32)
         if s == 0:
             noise0 = nz[:64].copy()
-        ob = o.sweep(float(g["dt"]), nz, zero_modes=bool(g["zm"]))
+        otf = "onthefly" in g and bool(g["onthefly"])
+        ob = o.sweep(float(g["dt"]), nz, zero_modes=bool(g["zm"]), onthefly=otf)
         if "c1" in g:
             ob.w2 = o.last_w2()
         obs.append(ob)
@@ -40,6 +41,7 @@ def replay(O, g):
             o.fa_gauge_fix(float(g["alpha"]))
         elif bool(g["local_gf"]):
             o.local_gauge_fix(float(g["alpha"]))
+        o.twist_boundary()
     return o, p0, noise0, obs
 
 
