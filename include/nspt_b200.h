@@ -112,16 +112,18 @@ int nspt_get_seed(nspt_ctx *ctx, uint64_t *seed, uint64_t *counter);
 
 /* NsptEvolve (nspt.cc:953-1039) with Beat = nsteps and dt = tau_g of
  * Quench.cfg (before the /(-2 NC) of Quenched.cc:584-589): per step a
- * Jacobi Langevin sweep, then the zero-mode subtraction and the gauge
- * fixing (NSPT_GF_FA or NSPT_GF_LOCAL, with the alpha given at creation)
- * selected at creation.  Twisted boundaries are applied on the fly
- * (no copy sites), so twist_boundary (nspt.cc:163-255) has no separate
- * call.  gf_every > 1 gauge-fixes only every gf_every-th step (0 = never). */
+ * Langevin sweep (Jacobi, or on the fly with NSPT_UPDATE_ONTHEFLY), then the
+ * zero-mode subtraction and the gauge fixing (NSPT_GF_FA or NSPT_GF_LOCAL,
+ * with the alpha given at creation) selected at creation, then
+ * twist_boundary.  Twisted boundaries are applied inside every neighbour
+ * read (no copy sites).  gf_every > 1 gauge-fixes only every gf_every-th
+ * step (0 = never). */
 int nspt_step(nspt_ctx *ctx, double dt, int nsteps, int gf_every);
 
 /* The three pieces of NsptEvolve, separately:
- * gauge_wilson (nspt.cc:258-600, Jacobi branch; also accumulates the zero
- * mode when the context has NSPT_ZEROMODE); zero_modes_subtraction
+ * gauge_wilson (nspt.cc:258-600, the Jacobi or the on-the-fly branch as
+ * selected at creation; also accumulates the zero mode when the context has
+ * NSPT_ZEROMODE); zero_modes_subtraction
  * (nspt.cc:605-654); FAstochastic_gauge_fixing (nspt.cc:866-948). */
 int nspt_gauge_wilson(nspt_ctx *ctx, double dt);
 int nspt_zero_modes_subtraction(nspt_ctx *ctx);
@@ -146,13 +148,15 @@ int nspt_twist_boundary(nspt_ctx *ctx);
 /* grid[d] threads along direction d; every L[d] % grid[d] == 0 and
  * L[d] / grid[d] >= 2 where grid[d] > 1, else NSPT_ERR_ARG. */
 int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]);
-/* Which kernel runs the local gauge fixing; both visit the sites in the
- * grid's order and give the same links.  NSPT_LGF_GROUP: one 9-lane link
- * group per reference thread.  NSPT_LGF_TEAM: a warp of three groups per
- * thread, the site's stagings and link products spread over them (shorter
- * per-site latency, for grids with few threads).  NSPT_LGF_AUTO (the
- * default): the team form when all the barrier step's teams fit on the GPU
- * at once.  Anything else: NSPT_ERR_ARG. */
+/* Which kernels run the work ordered by the thread grid -- the local gauge
+ * fixing and the on-the-fly sweep; both forms visit the sites in the grid's
+ * order and give the same links.  NSPT_LGF_GROUP: one 9-lane link group per
+ * reference thread.  NSPT_LGF_TEAM: a warp of three groups per thread (the
+ * gauge fixing's stagings and link products, or the sweep's three planes of
+ * staples, spread over them: shorter latency for grids with few threads;
+ * the on-the-fly team form needs one site per thread and barrier step).
+ * NSPT_LGF_AUTO (the default): the team form when all the barrier step's
+ * teams fit on the GPU at once.  Anything else: NSPT_ERR_ARG. */
 #define NSPT_LGF_AUTO 0
 #define NSPT_LGF_GROUP 1
 #define NSPT_LGF_TEAM 2

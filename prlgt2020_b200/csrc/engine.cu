@@ -290,7 +290,30 @@ static int launch_sweep_otf(nspt_ctx *ctx, const SweepArgs &a0) {
   a.gpc = k.warps * LPW;
   const size_t smem = (size_t)a.gpc * group_bytes(ctx, SWEEP_SLOTS, 0);
   const unsigned grid = (unsigned)((gr.nthr + a.gpc - 1) / a.gpc);
-  if (gr.seg == 1) {
+  // a warp of three groups per reference thread (the three planes' staples
+  // side by side) where every team of a barrier step fits on the GPU at once
+  const size_t team_bytes = (size_t)LPW * SWEEP_SLOTS * ctx->SS * sizeof(double2);
+  int team_warps = 4;
+  while (team_warps > 1 && (size_t)team_warps * team_bytes > ctx->smem_optin) team_warps /= 2;
+  bool team = gr.seg == 1 && team_bytes <= ctx->smem_optin && ctx->gf_form != NSPT_LGF_GROUP;
+  if (team && ctx->gf_form == NSPT_LGF_AUTO) {
+    const long per_sm = std::min<long>((long)((size_t)228 * 1024 / team_bytes), low ? 12 : 8);
+    team = gr.nthr <= per_sm * ctx->nsm;
+  }
+  if (team) {
+    const size_t tsmem = (size_t)team_warps * team_bytes;
+    const void *fn =
+        low ? (const void *)k_sweep_otf1_team<true> : (const void *)k_sweep_otf1_team<false>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsmem);
+    const unsigned tgrid = (unsigned)((gr.nthr + team_warps - 1) / team_warps);
+    for (long p = 0; p < steps; p++)
+      for (int mu = 0; mu < 4; mu++) {
+        if (low)
+          k_sweep_otf1_team<true><<<tgrid, 32 * team_warps, tsmem, ctx->st>>>(a, gr, p, mu);
+        else
+          k_sweep_otf1_team<false><<<tgrid, 32 * team_warps, tsmem, ctx->st>>>(a, gr, p, mu);
+      }
+  } else if (gr.seg == 1) {
     // one site per thread and barrier step: a launch per (step, mu), the
     // link update inline without a loop around it
     const void *fn = low ? (const void *)k_sweep_otf1<true> : (const void *)k_sweep_otf1<false>;

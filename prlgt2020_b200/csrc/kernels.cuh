@@ -477,6 +477,58 @@ __device__ __forceinline__ void sweep_stage(double2 *slot, const SweepArgs &a, i
   }
 }
 
+// The rest of a link update once the staple sum is in slot W (flag wflag):
+// P = U W into T with U in Y, the traces, then update_link.
+template <bool MEASURE, bool FF, bool LOW, bool OTF>
+__device__ __forceinline__ void sweep_tail(const SweepArgs &a, const Lane &L, double2 *T,
+                                           double2 *Y, double2 *W, int mu, int site,
+                                           double2 wflag) {
+  constexpr int MOK = LOW ? MO_LOW : MO;
+  const int ffe = FF ? *a.ff_scale : 0;
+  const int N = a.N, c = L.c;
+  const size_t V = (size_t)a.g.V;
+  const long link = (long)mu * a.g.V + site;
+  Nb self;
+  self.site = site;
+  self.fwd = self.bwd = 0;
+  if (L.j == 0) W[0] = wflag;
+  // ---- P = U_mu(x) * staples (nspt.cc:392) into T; U_mu(x) in Y
+  sweep_stage<OTF>(Y, a, mu, self, N, L);
+  const double2 pflag = flag_mul(Y[0], wflag);
+  cprod<FF, MOK, false>(LeftS{Y}, Y[0], W, wflag, N, L, ffe,
+                     [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
+  if (L.j == 0) T[0] = pflag;
+  __syncwarp(L.mask);
+  // ---- traces (ptSU3::Tr, QCDpt.cc:115-122), norm and Tr U_k (nspt.cc:393-402)
+  {
+    const size_t nl4 = 4 * V;
+    if (L.j == 0) a.obs_tr[link] = make_double2(3. * pflag.x, 3. * pflag.y);
+    for (int k = 1 + L.j; k <= N; k += GROUP) {
+      a.obs_tr[(size_t)k * nl4 + link] =
+          cadd(cadd(T[sidx(k, 0, 0)], T[sidx(k, 1, 1)]), T[sidx(k, 2, 2)]);
+      if constexpr (!MEASURE) {
+        double nrm = 0.0;
+#pragma unroll
+        for (int i = 0; i < 3; i++) {
+          double d = 0.0;
+#pragma unroll
+          for (int l = 0; l < 3; l++) {
+            const double2 u = Y[sidx(k, i, l)];
+            d += u.x * u.x + u.y * u.y;
+          }
+          nrm += d;
+        }
+        a.obs_norm[(size_t)(k - 1) * nl4 + link] = nrm;
+        a.obs_tru[(size_t)(k - 1) * nl4 + link] =
+            cadd(cadd(Y[sidx(k, 0, 0)], Y[sidx(k, 1, 1)]), Y[sidx(k, 2, 2)]);
+      }
+    }
+  }
+  if constexpr (MEASURE) return;
+  __syncwarp(L.mask);
+  update_link<MOK, OTF>(a, T, Y, W, link, mu, site, self, L);
+}
+
 // The update of link (mu, site) by one group: staples, force, observables,
 // noise, exp, the new link into a.F (a.U itself on the fly) and its log.
 template <bool MEASURE, bool FF, bool LOW, bool OTF>
@@ -485,11 +537,8 @@ __device__ __forceinline__ void sweep_one(const SweepArgs &a, const Lane &L, dou
   constexpr int MOK = LOW ? MO_LOW : MO;
   const int ffe = FF ? *a.ff_scale : 0;
   const int N = a.N, c = L.c;
-  const size_t V = (size_t)a.g.V;
-  const long link = (long)mu * a.g.V + site;
   int x[4];
   coords(a.g, site, x);
-  const size_t plane_mu = (size_t)9 * N * V;
 
   double2 wflag = cz();
   bool first = true;
@@ -554,42 +603,7 @@ __device__ __forceinline__ void sweep_one(const SweepArgs &a, const Lane &L, dou
       acc(T, Y);
     }
   }
-  if (L.j == 0) W[0] = wflag;
-  // ---- P = U_mu(x) * staples (nspt.cc:392) into T; U_mu(x) in Y
-  sweep_stage<OTF>(Y, a, mu, self, N, L);
-  const double2 pflag = flag_mul(Y[0], wflag);
-  cprod<FF, MOK, false>(LeftS{Y}, Y[0], W, wflag, N, L, ffe,
-                     [&](int k, int r, double2 v) { T[sidx(k, r, c)] = v; });
-  if (L.j == 0) T[0] = pflag;
-  __syncwarp(L.mask);
-  // ---- traces (ptSU3::Tr, QCDpt.cc:115-122), norm and Tr U_k (nspt.cc:393-402)
-  {
-    const size_t nl4 = 4 * V;
-    if (L.j == 0) a.obs_tr[link] = make_double2(3. * pflag.x, 3. * pflag.y);
-    for (int k = 1 + L.j; k <= N; k += GROUP) {
-      a.obs_tr[(size_t)k * nl4 + link] =
-          cadd(cadd(T[sidx(k, 0, 0)], T[sidx(k, 1, 1)]), T[sidx(k, 2, 2)]);
-      if constexpr (!MEASURE) {
-        double nrm = 0.0;
-#pragma unroll
-        for (int i = 0; i < 3; i++) {
-          double d = 0.0;
-#pragma unroll
-          for (int l = 0; l < 3; l++) {
-            const double2 u = Y[sidx(k, i, l)];
-            d += u.x * u.x + u.y * u.y;
-          }
-          nrm += d;
-        }
-        a.obs_norm[(size_t)(k - 1) * nl4 + link] = nrm;
-        a.obs_tru[(size_t)(k - 1) * nl4 + link] =
-            cadd(cadd(Y[sidx(k, 0, 0)], Y[sidx(k, 1, 1)]), Y[sidx(k, 2, 2)]);
-      }
-    }
-  }
-  if constexpr (MEASURE) return;
-  __syncwarp(L.mask);
-  update_link<MOK, OTF>(a, T, Y, W, link, mu, site, self, L);
+  sweep_tail<MEASURE, FF, LOW, OTF>(a, L, T, Y, W, mu, site, wflag);
 }
 
 template <bool MEASURE, bool FF = false, bool LOW = false>
@@ -630,6 +644,62 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ?
   LgfWalk(gr, tid, step).site(gr, a.g, 0, x);
   const int site = x[0] * a.g.s0 + x[1] * a.g.s1 + x[2] * a.g.s2 + x[3];
   sweep_one<false, false, LOW, true>(a, L, T, Y, W, mu, site);
+}
+
+// k_sweep_otf1 with a warp of three groups per reference thread, for barrier
+// steps with too few threads to fill the GPU (the 12^4 lattice's 6^4
+// threads): group g forms the upper and lower staples of the g-th plane
+// (nu != mu, ascending) into its own sum, the team adds the three plane sums
+// in plane order, as the reference's W1 += staple(nu) (nspt.cc:381-388),
+// and group 0 finishes the link.  Three slots per group.
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : SWEEP_THREADS, LOW ? 2 : 1)
+    k_sweep_otf1_team(SweepArgs a, LgfGrid gr, long step, int mu) {
+  constexpr int MOK = LOW ? MO_LOW : MO;
+  constexpr int TEAM = LPW * GROUP;
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long tid = (long)blockIdx.x * nw + warp;
+  if (tid >= gr.nthr) return;
+  const int SS = a.SS, N = a.N;
+  const unsigned tmask = (1u << TEAM) - 1u;
+  double2 *base = sm + (size_t)warp * (LPW * SWEEP_SLOTS) * SS;
+  double2 *T = base + (size_t)g * SWEEP_SLOTS * SS, *Y = T + SS, *W = Y + SS;
+  int x[4];
+  LgfWalk(gr, tid, step).site(gr, a.g, 0, x);
+  const int site = x[0] * a.g.s0 + x[1] * a.g.s1 + x[2] * a.g.s2 + x[3];
+  const int nu = g + (g >= mu ? 1 : 0);  // the g-th direction other than mu
+  Nb self;
+  self.site = site;
+  self.fwd = self.bwd = 0;
+  double2 wflag;
+  {  // upper U_nu(x+mu) U_mu(x+nu)^dag U_nu(x)^dag
+    const Nb m = neighbour(a.g, x, mu, 1);
+    const Nb b = neighbour(a.g, x, nu, 1);
+    sweep_stage<true>(T, a, nu, m, N, L);
+    sweep_stage<true>(Y, a, mu, b, N, L, true);
+    slot_mul<MOK>(T, Y, N, L);
+    sweep_stage<true>(Y, a, nu, self, N, L, true);
+    wflag = slot_acc<MOK>(W, T, Y, true, N, L);
+  }
+  {  // lower U_nu(x+mu-nu)^dag U_mu(x-nu)^dag U_nu(x-nu)
+    const Nb d = neighbour(a.g, x, nu, -1);
+    const Nb dm = neighbour(a.g, x, nu, -1, mu, 1);
+    sweep_stage<true>(T, a, nu, dm, N, L, true);
+    sweep_stage<true>(Y, a, mu, d, N, L, true);
+    slot_mul<MOK>(T, Y, N, L);
+    sweep_stage<true>(Y, a, nu, d, N, L);
+    wflag = cadd(wflag, slot_acc<MOK>(W, T, Y, false, N, L));
+  }
+  if (L.j == 0) W[0] = wflag;
+  __syncwarp(tmask);
+  double2 *W0 = base + 2 * SS, *W1 = W0 + SWEEP_SLOTS * SS, *W2 = W1 + SWEEP_SLOTS * SS;
+  for (int e = g * GROUP + L.j; e < 1 + 9 * N; e += TEAM) W0[e] = cadd(cadd(W0[e], W1[e]), W2[e]);
+  __syncwarp(tmask);
+  if (g == 0) sweep_tail<false, false, LOW, true>(a, L, T, Y, W, mu, site, W[0]);
 }
 
 // One on-the-fly link update, out of line: the walk's state stays outside

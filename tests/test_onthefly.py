@@ -47,10 +47,14 @@ def check_obs(eo, oo, tol):
     ((4, 4, 2, 4), 16, "", (1, 2, 1, 2)),
 ], ids=["sequential_n4", "grid2222_n8", "grid3212_6x_n6", "twisted_yz_sequential",
         "twisted_yzt_grid1221", "twisted_yz_n24_grid2222", "grid1212_n16"])
-def test_onthefly_sweep_matches_oracle(engine_mod, oracle_mod, L, N, twist, grid):
-    """gauge_wilson on the fly, one sweep, then twist_boundary."""
+@pytest.mark.parametrize("form", ["group", "team"])
+def test_onthefly_sweep_matches_oracle(engine_mod, oracle_mod, L, N, twist, grid, form):
+    """gauge_wilson on the fly, one sweep, then twist_boundary, by one
+    group per reference thread or by a warp of three (one plane's staples
+    each; grids with one site per thread and barrier step)."""
     P, O = engine_mod, oracle_mod
     e, o = pair(P, O, L, N, twist=twist, start=500 + N, grid=grid)
+    e.set_local_gf_form(form)
     rng = O.Rand55(7)
     for _ in range(2):
         nz = rng.gauss(o.V * 32)
