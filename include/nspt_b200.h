@@ -71,7 +71,7 @@ extern "C" {
  * start, as the reference's copy sites do until twist_boundary
  * (nspt_twist_boundary; nspt_step calls it at the end of every step).
  * Without the flag: the Jacobi update (F = exp(W1) U, then U = F).
- * Wilson action, FP64; not with FA gauge fixing on twisted boundaries. */
+ * FP64 only (not with NSPT_PRECISION_FF). */
 #define NSPT_UPDATE_ONTHEFLY (1u << 11)
 
 typedef struct nspt_ctx nspt_ctx;
@@ -146,7 +146,9 @@ int nspt_local_gauge_fixing(nspt_ctx *ctx, double alpha);
  * start field until this call.  A no-op otherwise. */
 int nspt_twist_boundary(nspt_ctx *ctx);
 /* grid[d] threads along direction d; every L[d] % grid[d] == 0 and
- * L[d] / grid[d] >= 2 where grid[d] > 1, else NSPT_ERR_ARG. */
+ * L[d] / grid[d] >= 2 where grid[d] > 1 (>= 3 for an improved action with
+ * NSPT_UPDATE_ONTHEFLY, whose rectangles reach two sites), else
+ * NSPT_ERR_ARG. */
 int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]);
 /* Which kernels run the work ordered by the thread grid -- the local gauge
  * fixing and the on-the-fly sweep; both forms visit the sites in the grid's

@@ -339,6 +339,33 @@ static int launch_sweep_otf(nspt_ctx *ctx, const SweepArgs &a0) {
   return NSPT_OK;
 }
 
+// The improved-action sweep on the fly (periodic boundaries only): one
+// launch per barrier step, or per (barrier step, mu) where every thread owns
+// one site per barrier step.
+static int launch_sweep_imp_otf(nspt_ctx *ctx, const SweepArgs &a) {
+  long steps;
+  const LgfGrid gr = thread_grid(ctx, steps);
+  const bool low = use_low(ctx);
+  const int max_warps = low ? SWEEP_THREADS_LOW / 32 : 8;
+  const KernelShape k = choose_shape(ctx, IMP_SLOTS, gr.nthr, 0, max_warps, low ? 2 : 1);
+  const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, IMP_SLOTS, 0);
+  const long per_cta = (long)k.warps * LPW;
+  const unsigned grid = (unsigned)((gr.nthr + per_cta - 1) / per_cta);
+  const void *fn = low ? (const void *)k_sweep_imp_otf<true> : (const void *)k_sweep_imp_otf<false>;
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int nmu = gr.seg == 1 ? 4 : 1;
+  for (long p = 0; p < steps; p++)
+    for (int q = 0; q < nmu; q++) {
+      const int lo = nmu == 4 ? q : 0, hi = nmu == 4 ? q + 1 : 4;
+      if (low)
+        k_sweep_imp_otf<true><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, lo, hi);
+      else
+        k_sweep_imp_otf<false><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, lo, hi);
+    }
+  CK(cudaGetLastError());
+  return NSPT_OK;
+}
+
 static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   SweepArgs a;
   a.U = ctx->U;
@@ -395,9 +422,10 @@ static int do_sweep(nspt_ctx *ctx, double dt, bool use_noise) {
   }
   const bool timed = ctx->kcount < nspt_ctx::KEV;
   if (timed) CK(cudaEventRecord(ctx->kev[2 * ctx->kcount], ctx->st));
-  int rc = otf                 ? launch_sweep_otf(ctx, a)
-           : ctx->c1 != 0.0    ? launch_sweep_imp(ctx, a)
-                               : launch_sweep(ctx, a, false);
+  int rc = otf && ctx->c1 != 0.0 ? launch_sweep_imp_otf(ctx, a)
+           : otf                 ? launch_sweep_otf(ctx, a)
+           : ctx->c1 != 0.0      ? launch_sweep_imp(ctx, a)
+                                 : launch_sweep(ctx, a, false);
   if (rc) return rc;
   if (timed) {
     CK(cudaEventRecord(ctx->kev[2 * ctx->kcount + 1], ctx->st));
@@ -665,12 +693,21 @@ static int do_local_gf(nspt_ctx *ctx, double alpha) {
   return NSPT_OK;
 }
 
-static bool grid_ok(const int L[4], const int grid[4]) {
+// minb: the smallest block along a split direction.  The reference needs 2
+// (threads of one barrier step then share no link); an on-the-fly sweep of
+// an improved action needs 3, because its rectangles reach two sites: with
+// blocks of 2 the reference's own threaded run races and differs from run
+// to run.
+static bool grid_ok(const int L[4], const int grid[4], int minb = 2) {
   for (int d = 0; d < 4; d++) {
     if (grid[d] < 1 || L[d] % grid[d]) return false;
-    if (grid[d] > 1 && L[d] / grid[d] < 2) return false;
+    if (grid[d] > 1 && L[d] / grid[d] < minb) return false;
   }
   return true;
+}
+
+static int grid_min_block(const nspt_ctx *ctx) {
+  return (ctx->flags & NSPT_UPDATE_ONTHEFLY) && ctx->c1 != 0.0 ? 3 : 2;
 }
 
 // ---------------- context ----------------
@@ -739,9 +776,8 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
   const unsigned known = NSPT_TWIST_Y | NSPT_TWIST_Z | NSPT_TWIST_T | NSPT_ZEROMODE | NSPT_GF_FA |
                          NSPT_GF_LOCAL | actions | NSPT_PRECISION_FF | NSPT_UPDATE_ONTHEFLY;
   if (flags & ~known) return NSPT_ERR_ARG;
-  // the on-the-fly update is built for the FP64 Wilson sweep
-  if ((flags & NSPT_UPDATE_ONTHEFLY) && (flags & (NSPT_PRECISION_FF | actions)))
-    return NSPT_ERR_ARG;
+  // the on-the-fly update is built for the FP64 sweeps
+  if ((flags & NSPT_UPDATE_ONTHEFLY) && (flags & NSPT_PRECISION_FF)) return NSPT_ERR_ARG;
   // float-float products are built into the Wilson sweep only
   if ((flags & NSPT_PRECISION_FF) && (flags & actions)) return NSPT_ERR_ARG;
   if (__builtin_popcount(flags & actions) > 1) return NSPT_ERR_ARG;
@@ -789,8 +825,18 @@ extern "C" int nspt_create(const int L[4], int N, unsigned flags, double alpha, 
           : (flags & NSPT_ACTION_IWA)   ? -0.331
           : (flags & NSPT_ACTION_DBW2)  ? -1.4088
                                         : 0.0;
-  // finest thread grid the reference accepts: blocks of 2 sites where L is even
-  for (int d = 0; d < 4; d++) ctx->gf_grid[d] = (L[d] % 2 == 0) ? L[d] / 2 : 1;
+  // the finest thread grid the reference accepts: blocks of 2 sites where L
+  // is even, one thread along odd extents (for an improved action on the
+  // fly: blocks of the smallest size >= 3 dividing L)
+  for (int d = 0; d < 4; d++) {
+    if (grid_min_block(ctx) == 2) {
+      ctx->gf_grid[d] = (L[d] % 2 == 0) ? L[d] / 2 : 1;
+    } else {
+      int b = 3;
+      while (L[d] % b) b++;
+      ctx->gf_grid[d] = L[d] / b;
+    }
+  }
   ctx->gf_form = NSPT_LGF_AUTO;
   ctx->obs_tr = ctx->obs_tru = ctx->red2 = nullptr;
   ctx->obs_norm = ctx->red1 = ctx->noise = nullptr;
@@ -1153,7 +1199,7 @@ extern "C" int nspt_local_gauge_fixing(nspt_ctx *ctx, double alpha) {
 }
 
 extern "C" int nspt_set_gf_grid(nspt_ctx *ctx, const int grid[4]) {
-  if (!ctx || !grid || !grid_ok(ctx->L, grid)) return NSPT_ERR_ARG;
+  if (!ctx || !grid || !grid_ok(ctx->L, grid, grid_min_block(ctx))) return NSPT_ERR_ARG;
   for (int d = 0; d < 4; d++) ctx->gf_grid[d] = grid[d];
   ctx->launch_gen++;
   return NSPT_OK;

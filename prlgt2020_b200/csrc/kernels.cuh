@@ -763,47 +763,39 @@ struct ImpLink {
   bool dag;
 };
 
+template <bool RW = false>
 __device__ __forceinline__ void imp_stage(const SweepArgs &a, double2 *slot, const ImpLink &l,
                                           const Lane &L) {
   Nb n;
   n.site = l.site;
   n.fwd = n.bwd = 0;
-  stage(slot, a.U, a.Uf, l.d, n, a.g, a.N, L, l.dag);
+  stage<RW>(slot, a.U, a.Uf, l.d, n, a.g, a.N, L, l.dag);
 }
 
 // Wacc (+)= l[0] l[1] ... l[n-1]; returns the flag of the chain
-template <int NL, int MOx = MO>
+template <int NL, int MOx = MO, bool RW = false>
 __device__ __forceinline__ double2 imp_chain(const SweepArgs &a, double2 *T, double2 *Y,
                                              double2 *Wacc, const ImpLink (&l)[NL], bool first,
                                              const Lane &L) {
-  imp_stage(a, T, l[0], L);
+  imp_stage<RW>(a, T, l[0], L);
 #pragma unroll
   for (int m = 1; m < NL - 1; m++) {
-    imp_stage(a, Y, l[m], L);
+    imp_stage<RW>(a, Y, l[m], L);
     slot_mul<MOx>(T, Y, a.N, L);
   }
-  imp_stage(a, Y, l[NL - 1], L);
+  imp_stage<RW>(a, Y, l[NL - 1], L);
   return slot_acc<MOx>(Wacc, T, Y, first, a.N, L);
 }
 
-template <bool LOW = false>
-__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
-    k_sweep_imp(SweepArgs a) {
+// The improved-action update of link (mu, site) by one group (slots T, Y,
+// W, W2); OTF: in place (a.F = a.U), coherent loads.
+template <bool LOW, bool OTF>
+__device__ __forceinline__ void imp_one(const SweepArgs &a, const Lane &L, double2 *T,
+                                        double2 *Y, double2 *W, double2 *W2, int mu, int site) {
   constexpr int MOK = LOW ? MO_LOW : MO;
-  extern __shared__ double2 sm[];
-  Lane L;
-  int g;
-  if (!make_lane(L, g)) return;
-  const int warp = threadIdx.x >> 5;
-  const int N = a.N, SS = a.SS;
+  const int N = a.N;
   const size_t V = (size_t)a.g.V;
-  double2 *T = sm + (size_t)(warp * LPW + g) * (IMP_SLOTS * SS), *Y = T + SS;
-  double2 *W = Y + SS, *W2 = W + SS;
-  bool valid;
-  const long link = group_unit(g, 4L * a.g.V, valid);
-  if (!valid) return;
-  const int mu = (int)(link / a.g.V);
-  const int site = (int)(link - (long)mu * a.g.V);
+  const long link = (long)mu * a.g.V + site;
   int x[4];
   coords(a.g, site, x);
 
@@ -829,7 +821,7 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
     if (nu == mu) continue;
     const int m = mu, n = nu;
     auto st = [&](double2 *slot, int d, int st_site, bool dag) {
-      imp_stage(a, slot, ImpLink{d, st_site, dag}, L);
+      imp_stage<OTF>(a, slot, ImpLink{d, st_site, dag}, L);
     };
     // ---- Wilson staples (QCDenvNODEpt_test.h:554-557) and the two
     // rectangles that begin with a Wilson staple's first two links, which
@@ -873,20 +865,20 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
       // U_nu(a) U_nu(b) dag(U_nu(x) U_nu(c) U_mu(d)),  a=x+mu b=x+mu+nu c=x+nu d=x+2nu
       const ImpLink r1[5] = {{n, at(1, 0), false}, {n, at(1, 1), false}, {m, at(0, 2), true},
                              {n, at(0, 1), true}, {n, site, true}};
-      acc2(imp_chain<5, MOK>(a, T, Y, W2, r1, first2, L));
+      acc2(imp_chain<5, MOK, OTF>(a, T, Y, W2, r1, first2, L));
       // U_mu(a) U_nu(e) dag(U_nu(x) U_mu(c) U_mu(b)),  e=x+2mu
       const ImpLink r2[5] = {{m, at(1, 0), false}, {n, at(2, 0), false}, {m, at(1, 1), true},
                              {m, at(0, 1), true}, {n, site, true}};
-      acc2(imp_chain<5, MOK>(a, T, Y, W2, r2, first2, L));
+      acc2(imp_chain<5, MOK, OTF>(a, T, Y, W2, r2, first2, L));
       // dag(U_mu(d) U_nu(e) U_nu(b)) U_nu(d) U_nu(c),
       // b=x+mu-nu c=x-nu d=x-2nu e=x+mu-2nu
       const ImpLink r4[5] = {{n, at(1, -1), true}, {n, at(1, -2), true}, {m, at(0, -2), true},
                              {n, at(0, -2), false}, {n, at(0, -1), false}};
-      acc2(imp_chain<5, MOK>(a, T, Y, W2, r4, first2, L));
+      acc2(imp_chain<5, MOK, OTF>(a, T, Y, W2, r4, first2, L));
       // U_mu(a) dag(U_mu(c) U_mu(b) U_nu(f)) U_nu(c),  f=x+2mu-nu
       const ImpLink r5[5] = {{m, at(1, 0), false}, {n, at(2, -1), true}, {m, at(1, -1), true},
                              {m, at(0, -1), true}, {n, at(0, -1), false}};
-      acc2(imp_chain<5, MOK>(a, T, Y, W2, r5, first2, L));
+      acc2(imp_chain<5, MOK, OTF>(a, T, Y, W2, r5, first2, L));
     }
   }
   if (L.j == 0) {
@@ -899,7 +891,7 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
   Nb self;
   self.site = site;
   self.fwd = self.bwd = 0;
-  stage(Y, a.U, a.Uf, mu, self, a.g, N, L);
+  stage<OTF>(Y, a.U, a.Uf, mu, self, a.g, N, L);
   const double2 pflag = flag_mul(Y[0], wflag), p2flag = flag_mul(Y[0], w2flag);
   slot_mul_to<MOK>(T, Y, W, N, L);
   slot_mul_to<MOK>(W2, Y, W2, N, L);
@@ -940,7 +932,57 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
   for (int e = L.j; e < 1 + 9 * N; e += GROUP)
     T[e] = cadd(cscale(T[e], a.c0), cscale(W2[e], a.c1));
   __syncwarp(L.mask);
-  update_link<MOK>(a, T, Y, W, link, mu, site, self, L);
+  update_link<MOK, OTF>(a, T, Y, W, link, mu, site, self, L);
+}
+
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
+    k_sweep_imp(SweepArgs a) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5;
+  const int SS = a.SS;
+  double2 *T = sm + (size_t)(warp * LPW + g) * (IMP_SLOTS * SS), *Y = T + SS;
+  double2 *W = Y + SS, *W2 = W + SS;
+  bool valid;
+  const long link = group_unit(g, 4L * a.g.V, valid);
+  if (!valid) return;
+  const int mu = (int)(link / a.g.V);
+  const int site = (int)(link - (long)mu * a.g.V);
+  imp_one<LOW, false>(a, L, T, Y, W, W2, mu, site);
+}
+
+// The improved-action sweep on the fly (periodic boundaries): as
+// k_sweep_otf, one group per reference thread walking its sites for one
+// barrier step, links mu_lo..mu_hi-1 of each site in place (a launch per
+// (step, mu) where each thread owns one site per barrier step).
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
+    k_sweep_imp_otf(SweepArgs a, LgfGrid gr, long step, int mu_lo, int mu_hi) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long tid = ((long)blockIdx.x * nw + warp) * LPW + g;
+  if (tid >= gr.nthr) return;
+  const int SS = a.SS;
+  double2 *T = sm + (size_t)(warp * LPW + g) * (IMP_SLOTS * SS), *Y = T + SS;
+  double2 *W = Y + SS, *W2 = W + SS;
+  const LgfWalk walk(gr, tid, step);
+#pragma unroll 1
+  for (long r = 0; r < gr.seg; r++) {
+    int x[4];
+    walk.site(gr, a.g, r, x);
+    const int site = x[0] * a.g.s0 + x[1] * a.g.s1 + x[2] * a.g.s2 + x[3];
+#pragma unroll 1
+    for (int mu = mu_lo; mu < mu_hi; mu++) {
+      imp_one<LOW, true>(a, L, T, Y, W, W2, mu, site);
+      __syncwarp(L.mask);
+    }
+  }
 }
 
 // Advance a device step counter by one (a kernel, so that it replays

@@ -139,6 +139,46 @@ def test_onthefly_with_fa_gauge_fixing(engine_mod, oracle_mod):
 
 def test_onthefly_rejects_what_is_not_built(engine_mod):
     P = engine_mod
-    for kw in (dict(precision="ff"), dict(action="tlsym")):
-        with pytest.raises(Exception):
-            P.NsptEngine((4, 4, 4, 4), 4, update="onthefly", **kw)
+    with pytest.raises(Exception):
+        P.NsptEngine((4, 4, 4, 4), 4, update="onthefly", precision="ff")
+
+
+@pytest.mark.parametrize("action,c1,L,grid", [
+    ("tlsym", -1.0 / 12.0, (6, 6, 6, 4), (2, 2, 2, 1)),
+    ("dbw2", -1.4088, (4, 4, 4, 4), (1, 1, 1, 1)),
+    ("iwa", -0.331, (4, 6, 6, 4), (1, 2, 2, 1)),
+], ids=["tlsym_blocks3", "dbw2_sequential", "iwa_blocks3"])
+def test_onthefly_improved_action(engine_mod, oracle_mod, action, c1, L, grid):
+    """The improved-action sweep on the fly (periodic): plaquette and
+    rectangle traces and the links against the oracle, on grids whose
+    blocks are at least 3 sites (the rectangles reach two)."""
+    P, O = engine_mod, oracle_mod
+    N = 5
+    o = O.Oracle(L, N)
+    o.random_start(41, 0.5)
+    o.set_action(c1)
+    e = P.NsptEngine(L, N, action=action, update="onthefly")
+    e.set_gf_grid(grid)
+    e.upload(o.links)
+    rng = O.Rand55(13)
+    for _ in range(2):
+        nz = rng.gauss(o.V * 32)
+        e.set_noise(nz)
+        eo = e.gauge_wilson(0.01)
+        oo = o.sweep(0.01, nz, onthefly=True, grid=grid)
+        check_obs(eo, oo, 1e-11)
+        ok, w = obs_close(e.rect_observables(), o.last_w2(), 1e-11)
+        assert ok, ("w2", w)
+    assert per_order_rel(e.download(), o.links, N).max() <= 1e-12
+
+
+def test_onthefly_improved_action_needs_blocks_of_three(engine_mod):
+    """Blocks of 2 would let a thread's rectangles read links another thread
+    of the same barrier step updates (the reference's threaded run then
+    races): rejected, and the default grid uses blocks of 3 or more."""
+    P = engine_mod
+    e = P.NsptEngine((4, 4, 4, 4), 3, action="tlsym", update="onthefly")
+    with pytest.raises(Exception):
+        e.set_gf_grid((2, 2, 2, 2))
+    e.set_gf_grid((1, 1, 1, 1))
+    P.NsptEngine((4, 4, 4, 4), 3, action="tlsym").set_gf_grid((2, 2, 2, 2))

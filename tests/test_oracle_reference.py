@@ -198,3 +198,35 @@ def test_oracle_onthefly_matches_reference(oracle_mod, case):
         o.local_gauge_fix(alpha, grid=g)
         o.twist_boundary()
     assert per_order_rel(o.links, r["links"], N).max() <= 1e-12
+
+
+@pytest.mark.parametrize("L,grid", [((4, 4, 4, 4), (1, 1, 1)), ((4, 6, 6, 6), (2, 2, 2))],
+                         ids=["sequential", "grid222_blocks3"])
+def test_oracle_onthefly_improved_action_matches_reference(oracle_mod, L, grid):
+    """The reference's on-the-fly build with the tree-level Symanzik action
+    (GAUGE_ACTION TLSYM, choices.h:110; staple2x1 QCDenvNODEpt_test.h:
+    579-611): plaquette and rectangle traces per step and the final links.
+    The rectangles reach two sites, so threads of one barrier step only stay
+    apart with blocks of 3 or more: with blocks of 2 the reference's own
+    threaded run differs from run to run, and there is nothing to pin."""
+    O = oracle_mod
+    N, steps, dt, c1 = 4, 2, 0.01, -1.0 / 12.0
+    b = O.ref_binary(N, "pbc", "local", grid, "tlsym", "otf")
+    if not os.path.exists(b):
+        if not os.path.exists(os.path.join(O.reference_dir(), "nspt.cc")):
+            pytest.skip("reference sources not available")
+        b = O.build_reference(N, "pbc", "local", grid, "tlsym", "otf")
+    o = O.Oracle(L, N)
+    o.random_start(29, 0.5)
+    o.set_action(c1)
+    with tempfile.TemporaryDirectory() as d:
+        O.write_config(os.path.join(d, "s.dat"), o.links, o.plaquette())
+        r = O.run_reference(b, L, steps, dt, 0.0, 47, d, start=os.path.join(d, "s.dat"))
+    g = (1,) + tuple(grid)
+    for s in range(steps):
+        ob = o.sweep(dt, r["noise"][s], zero_modes=True, onthefly=True, grid=g)
+        assert obs_close(ob.plaq, r["plaq"][s], 1e-12)[0]
+        assert obs_close(o.last_w2()[:N], r["w2"][s][:N], 1e-12)[0]
+        o.zero_modes()
+        o.local_gauge_fix(0.0, grid=g)
+    assert per_order_rel(o.links, r["links"], N).max() <= 1e-12
