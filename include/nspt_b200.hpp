@@ -61,7 +61,8 @@ struct act_params_t {
 };
 
 /* choices.h switches as run-time flags (NSPT_TWIST_*, NSPT_ZEROMODE,
- * NSPT_GF_FA, NSPT_GF_LOCAL, NSPT_ACTION_*, NSPT_PRECISION_FF) */
+ * NSPT_GF_FA, NSPT_GF_LOCAL, NSPT_ACTION_*, NSPT_PRECISION_FF,
+ * NSPT_UPDATE_ONTHEFLY) */
 using choices = unsigned;
 
 /* QCDenvNODEpt_test.h:331-338: the gauge field, here on the device */
@@ -145,8 +146,9 @@ inline int FAstochastic_gauge_fixing(ptGluon_fld &U) {
 inline int NsptEvolve(ptGluon_fld &U, int beat = 1, int gf_every = 1) {
   return nspt_step(U.ctx(), U.params().tau_g, beat, gf_every);
 }
-/* twists are applied on the fly inside the sweep: no copy sites to refresh */
-inline int twist_boundary(ptGluon_fld &) { return NSPT_OK; }
+/* twists are applied inside every neighbour read; this ends the stale
+ * twisted reads an on-the-fly gauge_wilson leaves (the copy sites) */
+inline int twist_boundary(ptGluon_fld &U) { return nspt_twist_boundary(U.ctx()); }
 inline int plaquette_measure(ptGluon_fld &U, Cplx *w) {
   return nspt_plaquette_measure(U.ctx(), &w[0].re);
 }
