@@ -286,8 +286,20 @@ static int launch_sweep_otf(nspt_ctx *ctx, const SweepArgs &a0) {
   const bool low = use_low(ctx);
   const int max_warps = (low ? SWEEP_THREADS_LOW : SWEEP_THREADS) / 32;
   const KernelShape k = choose_shape(ctx, SWEEP_SLOTS, gr.nthr, 0, max_warps, low ? 2 : 1);
+  int warps = k.warps;
   SweepArgs a = a0;
   a.gpc = k.warps * LPW;
+  if (!low && k.warps < max_warps) {
+    // as the Jacobi sweep: as many groups as shared memory holds, dealt over
+    // all max_warps warps (sweep_group), where that keeps >= 2.5 per warp
+    const long fit = std::min<long>((long)(ctx->smem_optin / group_bytes(ctx, SWEEP_SLOTS, 0)),
+                                    (long)max_warps * LPW);
+    const long want = (gr.nthr + 2L * ctx->nsm - 1) / (2L * ctx->nsm);
+    if (fit > a.gpc && want >= fit && 2 * fit >= 5L * max_warps) {
+      a.gpc = (int)fit;
+      warps = max_warps;
+    }
+  }
   const size_t smem = (size_t)a.gpc * group_bytes(ctx, SWEEP_SLOTS, 0);
   const unsigned grid = (unsigned)((gr.nthr + a.gpc - 1) / a.gpc);
   // a warp of three groups per reference thread (the three planes' staples
@@ -321,18 +333,18 @@ static int launch_sweep_otf(nspt_ctx *ctx, const SweepArgs &a0) {
     for (long p = 0; p < steps; p++)
       for (int mu = 0; mu < 4; mu++) {
         if (low)
-          k_sweep_otf1<true><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, mu);
+          k_sweep_otf1<true><<<grid, 32 * warps, smem, ctx->st>>>(a, gr, p, mu);
         else
-          k_sweep_otf1<false><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, mu);
+          k_sweep_otf1<false><<<grid, 32 * warps, smem, ctx->st>>>(a, gr, p, mu);
       }
   } else {
     const void *fn = low ? (const void *)k_sweep_otf<true> : (const void *)k_sweep_otf<false>;
     cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     for (long p = 0; p < steps; p++) {
       if (low)
-        k_sweep_otf<true><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p);
+        k_sweep_otf<true><<<grid, 32 * warps, smem, ctx->st>>>(a, gr, p);
       else
-        k_sweep_otf<false><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p);
+        k_sweep_otf<false><<<grid, 32 * warps, smem, ctx->st>>>(a, gr, p);
     }
   }
   CK(cudaGetLastError());
