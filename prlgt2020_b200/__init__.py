@@ -383,7 +383,8 @@ class NsptBatch:
     step dt[r] and noise seed seeds[r]; all share N, the flags and alpha."""
 
     def __init__(self, L, N: int, dt, seeds, zero_modes: bool = False, fa: bool = False,
-                 local_gf: bool = False, alpha: float = 0.0, twist: str = ""):
+                 local_gf: bool = False, alpha: float = 0.0, twist: str = "",
+                 update: str = "jacobi"):
         lib = load_library()
         L = [tuple(int(x) for x in l) for l in L]
         n = len(L)
@@ -394,6 +395,7 @@ class NsptBatch:
             flags |= {"y": NSPT_TWIST_Y, "z": NSPT_TWIST_Z, "t": NSPT_TWIST_T}[d]
         flags |= (NSPT_ZEROMODE if zero_modes else 0) | (NSPT_GF_FA if fa else 0)
         flags |= NSPT_GF_LOCAL if local_gf else 0
+        flags |= {"jacobi": 0, "onthefly": _lib.NSPT_UPDATE_ONTHEFLY}[update]
         self.N, self.n = int(N), n
         Ls = (ctypes.c_int * (4 * n))(*[x for l in L for x in l])
         dts = (ctypes.c_double * n)(*[float(x) for x in dt])

@@ -3,8 +3,9 @@ for the statistical comparison of the plaquette series (test_statistics.py).
 
 The reference's default program (Quenched.cc with choices.h as shipped:
 periodic boundaries, zero-mode subtraction, local stochastic gauge fixing,
-the on-the-fly update and its rand55 noise) and its Jacobi build (the parity
-build, UPDATE_ONTHEFLY off) each run R independent replicas from a cold
+the on-the-fly update and its rand55 noise), its Jacobi build (the parity
+build, UPDATE_ONTHEFLY off) and its on-the-fly build with OpenMP thread grid
+(2,2,2) each run R independent replicas from a cold
 start: THERM steps, then MEAS steps whose plaquette coefficients
 (nspt.cc:570-597) are averaged per replica.  Only the per-replica averages
 are stored, so the fixture is small.
@@ -42,9 +43,14 @@ def main():
     cfg = CFG
     seeds = [cfg["seed0"] + 17 * r for r in range(cfg["reps"])]
     res = {}
-    for upd in ("otf", "jacobi"):
-        b = O.build_reference(cfg["N"], "pbc", "local", (1, 1, 1), "wil", upd)
-        with ThreadPoolExecutor(max_workers=os.cpu_count()) as ex:
+    # the default on-the-fly build (one thread), the Jacobi build, and the
+    # on-the-fly build with OpenMP thread grid (2,2,2): blocks of 2 sites
+    for upd, grid in (("otf", (1, 1, 1)), ("jacobi", (1, 1, 1)), ("otf_grid222", (2, 2, 2))):
+        b = O.build_reference(cfg["N"], "pbc", "local", grid, "wil", upd.split("_")[0])
+        # a threaded build runs its replicas one at a time: its OpenMP
+        # barriers crawl when the cores are oversubscribed
+        workers = os.cpu_count() if grid == (1, 1, 1) else 1
+        with ThreadPoolExecutor(max_workers=workers) as ex:
             means = list(ex.map(lambda s: replica_means(b, s, cfg), seeds))
         res[upd] = np.array(means)
         m = res[upd].mean(axis=0)[:, 0]
@@ -53,7 +59,8 @@ def main():
     np.savez_compressed(os.path.join(OUT, "ref_longrun_pbc_n6.npz"),
                         L=np.array(cfg["L"]), N=cfg["N"], dt=cfg["dt"], alpha=cfg["alpha"],
                         therm=cfg["therm"], meas=cfg["meas"], seeds=np.array(seeds),
-                        means_otf=res["otf"], means_jacobi=res["jacobi"])
+                        means_otf=res["otf"], means_jacobi=res["jacobi"],
+                        means_otf_grid222=res["otf_grid222"])
 
 
 if __name__ == "__main__":

@@ -14,6 +14,8 @@ the same Langevin equation with other O(dt) corrections: the reference's
 two builds, run on the same seeds, differ by 0.0034 in the order-2
 coefficient at dt = 0.01 (-2.0041 vs -2.0006, errors 0.0013).  That
 measured difference enters the on-the-fly comparison as a systematic error.
+The engine's own on-the-fly update is compared, with no systematic, with
+the reference's on-the-fly build of the same OpenMP thread grid.
 """
 import os
 
@@ -60,3 +62,32 @@ def test_plaquette_series_agree_with_the_reference_long_runs(engine_mod):
         # order 0 is the exact flag 1; order 1 vanishes identically
         assert np.all(z[2:] <= Z_MAX), (build, m, mr, s, sr, z)
         assert abs(m[0] - 1.0) < 1e-12
+
+
+def test_onthefly_plaquette_series_agree_with_the_reference_long_runs(engine_mod):
+    """The engine's on-the-fly update against the reference's on-the-fly
+    build with the same OpenMP thread grid (1,2,2,2), so that both run the
+    same algorithm with different noise: no systematic error enters.  The
+    16 replicas run as one batch (one CUDA graph per step)."""
+    P = engine_mod
+    g = np.load(FIXTURE)
+    if "means_otf_grid222" not in g:
+        pytest.skip("fixture without the threaded on-the-fly runs")
+    L = tuple(int(x) for x in g["L"])
+    N, dt, alpha = int(g["N"]), float(g["dt"]), float(g["alpha"])
+    therm, meas, reps = int(g["therm"]), int(g["meas"]), len(g["seeds"])
+    b = P.NsptBatch([L] * reps, N, [dt] * reps, [515151 + 7919 * r for r in range(reps)],
+                    zero_modes=True, local_gf=True, alpha=alpha, update="onthefly")
+    for e in b.replicas:
+        e.set_gf_grid((1, 2, 2, 2))
+    b.step(therm, 1)
+    acc = np.zeros((reps, N + 1, 2))
+    for _ in range(meas):
+        b.step(1, 1)
+        acc += b.plaquettes()
+    b.close()
+    m, s = mean_err(acc / meas)
+    mr, sr = mean_err(g["means_otf_grid222"])
+    z = np.abs(m - mr) / np.sqrt(s ** 2 + sr ** 2 + 1e-300)
+    assert np.all(z[2:] <= Z_MAX), (m, mr, s, sr, z)
+    assert abs(m[0] - 1.0) < 1e-12
