@@ -147,7 +147,8 @@ def test_onthefly_rejects_what_is_not_built(engine_mod):
     ("tlsym", -1.0 / 12.0, (6, 6, 6, 4), (2, 2, 2, 1)),
     ("dbw2", -1.4088, (4, 4, 4, 4), (1, 1, 1, 1)),
     ("iwa", -0.331, (4, 6, 6, 4), (1, 2, 2, 1)),
-], ids=["tlsym_blocks3", "dbw2_sequential", "iwa_blocks3"])
+    ("tlsym", -1.0 / 12.0, (6, 6, 6, 6), (2, 2, 2, 2)),
+], ids=["tlsym_blocks3", "dbw2_sequential", "iwa_blocks3", "tlsym_one_site_per_thread"])
 def test_onthefly_improved_action(engine_mod, oracle_mod, action, c1, L, grid):
     """The improved-action sweep on the fly (periodic): plaquette and
     rectangle traces and the links against the oracle, on grids whose
