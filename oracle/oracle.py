@@ -103,6 +103,43 @@ class Rand55:
             self._h = None
 
 
+class ThreadNoise:
+    """The noise of the reference's OpenMP build with thread grid
+    grid = (ntt, ntx, nty, ntz): thread tid draws from its own MyRand,
+    seeded with seeds[tid], the 8 Gaussians of every link of its block
+    (blocks as Quenched.cc:518-531), sites in the block's lexicographic order
+    and mu inner (nspt.cc:355-440).  gauss_links() gives one step's V*4*8
+    draws by link (site lexicographic, mu inner)."""
+
+    def __init__(self, L, grid, seeds):
+        self.L = tuple(int(x) for x in L)
+        self.grid = tuple(int(x) for x in grid)
+        nthr = int(np.prod(self.grid))
+        if len(seeds) < nthr:
+            raise ValueError("one seed per thread")
+        self.rngs = [Rand55(int(seeds[t])) for t in range(nthr)]
+        bs = [l // n for l, n in zip(self.L, self.grid)]
+        s3, s2, s1 = self.L[3], self.L[2] * self.L[3], self.L[1] * self.L[2] * self.L[3]
+        self.blocks = []
+        for tid in range(nthr):
+            b = (tid // (self.grid[1] * self.grid[2] * self.grid[3]),
+                 (tid // (self.grid[2] * self.grid[3])) % self.grid[1],
+                 (tid // self.grid[3]) % self.grid[2], tid % self.grid[3])
+            sites = [(x0 * s1 + x1 * s2 + x2 * s3 + x3)
+                     for x0 in range(b[0] * bs[0], (b[0] + 1) * bs[0])
+                     for x1 in range(b[1] * bs[1], (b[1] + 1) * bs[1])
+                     for x2 in range(b[2] * bs[2], (b[2] + 1) * bs[2])
+                     for x3 in range(b[3] * bs[3], (b[3] + 1) * bs[3])]
+            self.blocks.append(np.array(sites, dtype=np.int64))
+        self.V = s1 * self.L[0]
+
+    def gauss_links(self) -> np.ndarray:
+        out = np.empty((self.V, 32))
+        for rng, sites in zip(self.rngs, self.blocks):
+            out[sites] = rng.gauss(sites.size * 32).reshape(-1, 32)
+        return out.reshape(-1)
+
+
 @dataclass
 class SweepObs:
     plaq: np.ndarray  # (N+1, 2)

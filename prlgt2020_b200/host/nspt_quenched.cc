@@ -29,7 +29,11 @@
 // rectangle traces follow Quenched.cc:327-348 and nspt.cc:586-597), -P
 // device Philox noise instead of the reference's rand55 stream, -O the
 // reference's default on-the-fly update (UPDATE_ONTHEFLY: links updated in
-// place in the thread grid's order); without -O the Jacobi update.
+// place in the thread grid's order); without -O the Jacobi update.  -M
+// draws the noise as an OpenMP build of the reference does: one rand55
+// stream per thread of the -G grid, seeded from the `seed` lines of
+// Quench.cfg (one per thread) or by -r through srand/rand; a hot start
+// reseeds them, as the reference keeps no noise state.
 // With periodic boundaries the Wilson loops of ComputeLoops (__MANY_LOOP__,
 // the reference's periodic default) go to <plaq_out>_nxm_SU3_wil_..._o<N>.txt
 // after every BEAT steps and at the end (nspt.cc:1283-1306); with -W also
@@ -60,6 +64,9 @@ struct Params {
   std::string plaqn, confn, damon = "damocle.dag";
   unsigned twist = 0;
   bool fa = false, philox = false, wl2x2 = false, otf = false;
+  bool thread_noise = false;  // -M: one rand55 stream per thread of the -G grid
+  std::vector<long> seeds;    // every `seed` line of Quench.cfg (one per thread)
+  bool seed_given = false;    // -r
   int zm = -1;  // -1: as the boundary conditions imply
   int grid[4] = {0, 0, 0, 0};
   unsigned action = 0;  // NSPT_ACTION_* or 0 (Wilson)
@@ -108,6 +115,13 @@ bool read_cfg(Params &p) {
   if (ok && (ok = get_word(fp, "last_conf", s, sizeof(s)))) p.confn = s;
   ok = ok && get_int(fp, "PTORD", &p.N);
   if (ok && (ok = get_word(fp, "seed", s, sizeof(s)))) p.seed = atol(s);
+  if (ok) {
+    // the reference reads one `seed` line per OpenMP thread (Quenched.cc:171-174)
+    p.seeds.push_back(p.seed);
+    char w[128], v[128];
+    while (fscanf(fp, "%127s %127s", w, v) == 2 && strcmp(w, "seed") == 0)
+      p.seeds.push_back(atol(v));
+  }
   fclose(fp);
   if (!ok) fprintf(stderr, "Errore: Quench.cfg non valido.\n");
   return ok;
@@ -133,6 +147,7 @@ void usage() {
          "-A action\timproved gauge action: tlsym, iwa or dbw2\n"
          "-P\t\tdevice Philox noise instead of the reference's generator\n"
          "-O\t\ton-the-fly update (UPDATE_ONTHEFLY) in the thread grid's order\n"
+         "-M\t\tone noise stream per thread of the -G grid (an OpenMP build)\n"
          "-W\t\t2x2 Wilson loops file (WL2x2, periodic boundaries)\n\n");
 }
 
@@ -213,12 +228,15 @@ int main(int argc, char **argv) {
     }
   if (!read_cfg(p)) return 1;
   int opt;
-  while ((opt = getopt(argc, argv, "l:s:b:d:r:g:a:t:p:c:n:hT:FG:Z:PA:WO")) != -1) {
+  while ((opt = getopt(argc, argv, "l:s:b:d:r:g:a:t:p:c:n:hT:FG:Z:PA:WOM")) != -1) {
     switch (opt) {
       case 'l': p.L[0] = p.L[1] = p.L[2] = p.L[3] = atoi(optarg); break;
       case 's': p.sweep = atoi(optarg); break;
       case 'b': p.beat = atoi(optarg); break;
-      case 'r': p.seed = atol(optarg); break;
+      case 'r':
+        p.seed = atol(optarg);
+        p.seed_given = true;
+        break;
       case 'n': p.N = atoi(optarg); break;
       case 'g': p.tau_g = atof(optarg); break;
       case 'a': p.alpha = -atof(optarg); break;
@@ -248,6 +266,7 @@ int main(int argc, char **argv) {
       case 'P': p.philox = true; break;
       case 'W': p.wl2x2 = true; break;
       case 'O': p.otf = true; break;
+      case 'M': p.thread_noise = true; break;
       case 'A':
         if (!strcmp(optarg, "tlsym")) p.action = NSPT_ACTION_TLSYM;
         else if (!strcmp(optarg, "iwa")) p.action = NSPT_ACTION_IWA;
@@ -368,6 +387,46 @@ int main(int argc, char **argv) {
     return fail(ctx, rc, "noise state");
   std::vector<double> eta;
   if (!p.philox) eta.resize((size_t)p.L[0] * p.L[1] * p.L[2] * p.L[3] * 32);
+  // -M: the noise of an OpenMP build.  Thread tid draws from its own rand55
+  // seeded with the tid-th `seed` line (Quenched.cc:171-174, 296-299), or
+  // with rand() after srand(-r) (Quenched.cc:199-205); it draws the 8
+  // Gaussians of every link of its block (Quenched.cc:518-531), sites in the
+  // block's lexicographic order and mu inner (nspt.cc:355-440).
+  std::vector<Rand55> trng;
+  std::vector<std::vector<long>> tsites;
+  if (p.thread_noise && !p.philox) {
+    if (!p.grid[0]) {
+      fprintf(stderr, "nspt_quenched: -M needs the build's thread grid (-G)\n");
+      return 1;
+    }
+    const int nthr = p.grid[0] * p.grid[1] * p.grid[2] * p.grid[3];
+    std::vector<long> sd(nthr);
+    if (p.seed_given) {
+      srand((unsigned)p.seed);
+      for (int t = 0; t < nthr; t++) sd[t] = rand();
+    } else {
+      if ((int)p.seeds.size() < nthr) {
+        fprintf(stderr, "Error reading input file at seed\n");
+        return 1;
+      }
+      for (int t = 0; t < nthr; t++) sd[t] = p.seeds[t];
+    }
+    int bs[4];
+    for (int d = 0; d < 4; d++) bs[d] = p.L[d] / p.grid[d];
+    for (int t = 0; t < nthr; t++) {
+      trng.emplace_back(sd[t]);
+      const int b[4] = {t / (p.grid[1] * p.grid[2] * p.grid[3]),
+                        (t / (p.grid[2] * p.grid[3])) % p.grid[1], (t / p.grid[3]) % p.grid[2],
+                        t % p.grid[3]};
+      std::vector<long> st;
+      for (int x0 = b[0] * bs[0]; x0 < (b[0] + 1) * bs[0]; x0++)
+        for (int x1 = b[1] * bs[1]; x1 < (b[1] + 1) * bs[1]; x1++)
+          for (int x2 = b[2] * bs[2]; x2 < (b[2] + 1) * bs[2]; x2++)
+            for (int x3 = b[3] * bs[3]; x3 < (b[3] + 1) * bs[3]; x3++)
+              st.push_back(((long)(x0 * p.L[1] + x1) * p.L[2] + x2) * p.L[3] + x3);
+      tsites.push_back(st);
+    }
+  }
   stamp(logf, "Inizio run");
 
   int t1 = 0, done = 0, config_counter = 0;
@@ -375,7 +434,12 @@ int main(int argc, char **argv) {
     t1 += p.beat;
     for (int t2 = 0; t2 < p.beat; t2++) {  // NsptEvolve (nspt.cc:963-1036)
       if (!p.philox) {
-        rng.fill(eta.data(), (long)eta.size());
+        if (trng.empty()) {
+          rng.fill(eta.data(), (long)eta.size());
+        } else {
+          for (size_t t = 0; t < trng.size(); t++)
+            for (long site : tsites[t]) trng[t].fill(eta.data() + site * 32, 32);
+        }
         if ((rc = nspt_set_noise(ctx, eta.data()))) return fail(ctx, rc, "noise");
       }
       if ((rc = nspt_gauge_wilson(ctx, p.tau_g))) return fail(ctx, rc, "gauge_wilson");

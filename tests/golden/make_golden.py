@@ -55,6 +55,10 @@ CASES = [
          dt=0.01, alpha=-0.05, seed=61, start=16, zm=True, update="otf"),
     dict(name="rand_tw_otf_localgf_n5", L=(4, 4, 4, 4), N=5, bc="tw", gf="local", steps=3,
          dt=0.01, alpha=-0.05, seed=62, start=17, zm=False, update="otf"),
+    # ... and its OpenMP build with thread grid (2,2,2): thread tid draws from
+    # its own MyRand, seeded seed + tid by the harness
+    dict(name="rand_pbc_otf_grid222_n4", L=(4, 4, 4, 4), N=4, bc="pbc", gf="local", steps=3,
+         dt=0.01, alpha=-0.05, seed=63, start=18, zm=True, update="otf", grid=(2, 2, 2)),
 ]
 C1 = {"wil": 0.0, "tlsym": -1.0 / 12.0, "iwa": -0.331, "dbw2": -1.4088}
 
@@ -63,7 +67,7 @@ LINK_SITES = 6  # sites of the final field kept in the fixture
 
 def make_case(c: dict) -> dict:
     action = c.get("action", "wil")
-    binary = O.build_reference(c["N"], c["bc"], c["gf"], (1, 1, 1), action,
+    binary = O.build_reference(c["N"], c["bc"], c["gf"], c.get("grid", (1, 1, 1)), action,
                                c.get("update", "jacobi"))
     with tempfile.TemporaryDirectory() as d:
         start = "cold"
@@ -124,7 +128,8 @@ def main():
                             start=-1 if c["start"] is None else c["start"],
                             twisted=c["bc"] == "tw", fa=c["gf"] == "fa", zm=c["zm"],
                             local_gf=c["gf"] == "local" and c["alpha"] != 0.0,
-                            onthefly=c.get("update", "jacobi") == "otf")
+                            onthefly=c.get("update", "jacobi") == "otf",
+                            grid=np.array((1,) + tuple(c.get("grid", (1, 1, 1)))))
         meta.append((c["name"], os.path.getsize(path)))
     for name, size in meta:
         print("%-28s %8d bytes" % (name, size))

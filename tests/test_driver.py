@@ -32,12 +32,17 @@ def driver():
     return path
 
 
-def write_cfg(d, L, sweep, beat, tau_g, alpha, init, N, seed, plaq="plaq", conf="conf"):
+def write_cfg(d, L, sweep, beat, tau_g, alpha, init, N, seed, plaq="plaq", conf="conf",
+              nthr=1):
+    """Quench.cfg; an OpenMP build reads one seed line per thread
+    (Quenched.cc:171-174): seed, seed + 1, ... as the harness seeds them."""
     with open(os.path.join(d, "Quench.cfg"), "w") as f:
         f.write("taglia %d %d %d %d\n" % tuple(L))
         f.write("SWEEP %d\nBEAT %d\ntau_g %r\nalpha %r\ninit_status %d\n" % (sweep, beat, tau_g, alpha,
                                                                              init))
-        f.write("plaq_out %s\nlast_conf %s\nPTORD %d\nseed %d\n" % (plaq, conf, N, seed))
+        f.write("plaq_out %s\nlast_conf %s\nPTORD %d\n" % (plaq, conf, N))
+        for t in range(nthr):
+            f.write("seed %d\n" % (seed + t))
 
 
 def write_damocle(d, tau_g, alpha, sweep=0, beat=1, save=0, kill=0):
@@ -79,13 +84,17 @@ def test_driver_replays_reference_fixture(driver, oracle_mod, tmp_path, path):
     action = {-1.0 / 12.0: "tlsym", -0.331: "iwa", -1.4088: "dbw2"}.get(
         float(g["c1"]) if "c1" in g else 0.0, "wil")
     name = stem(L, alpha, dt, N).replace("SU3_wil", "SU3_" + action[:3])
-    write_cfg(tmp_path, L, steps, steps, dt, alpha, 1 if start >= 0 else 0, N, seed)
+    grid = tuple(int(x) for x in g["grid"]) if "grid" in g else (1, 1, 1, 1)
+    nthr = int(np.prod(grid))
+    write_cfg(tmp_path, L, steps, steps, dt, alpha, 1 if start >= 0 else 0, N, seed, nthr=nthr)
     write_damocle(tmp_path, dt, alpha)
     if start >= 0:
         o = O.Oracle(L, N, twist_mask=6 if twisted else 0)
         o.random_start(start, 0.5)
         O.write_config(str(tmp_path / ("conf" + name)), o.links, o.plaquette())
-    args = [driver, "-G", "1,1,1,1"]  # the fixtures' reference builds run one thread
+    args = [driver, "-G", ",".join(str(x) for x in grid)]  # the fixture build's thread grid
+    if nthr > 1:
+        args += ["-M"]  # one noise stream per thread
     if twisted:
         args += ["-T", "yz"]
     else:

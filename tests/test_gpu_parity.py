@@ -226,11 +226,18 @@ def test_reference_golden_fixture(engine_mod, oracle_mod, path):
     e.upload(o.links)
     ok, w = obs_close(e.plaquette_measure(), g["plaq0"], 1e-12)
     assert ok, ("start plaquette", w)
+    grid = tuple(int(x) for x in g["grid"]) if "grid" in g else (1, 1, 1, 1)
+    nthr = int(np.prod(grid))
     if local_gf or otf:
-        e.set_gf_grid((1, 1, 1, 1))  # the fixture's reference build runs one thread
-    rng = oracle_mod.Rand55(int(g["seed"]))
+        e.set_gf_grid(grid)  # the fixture's reference build's OpenMP thread grid
+    if nthr > 1:  # one MyRand per thread, seeded seed + tid
+        tn = oracle_mod.ThreadNoise(L, grid, [int(g["seed"]) + t for t in range(nthr)])
+        draw = tn.gauss_links
+    else:
+        rng = oracle_mod.Rand55(int(g["seed"]))
+        draw = lambda: rng.gauss(o.V * 32)  # noqa: E731
     for s in range(int(g["steps"])):
-        nz = rng.gauss(o.V * 32)
+        nz = draw()
         e.set_noise(nz)
         ob = e.gauge_wilson(float(g["dt"]))
         for name, a, b in (("plaq", ob.plaq, g["plaq"][s]), ("norm", ob.norm, g["norm"][s])):

@@ -23,15 +23,22 @@ def replay(O, g):
     if "c1" in g:
         o.set_action(float(g["c1"]))
     p0 = o.plaquette()
-    rng = O.Rand55(int(g["seed"]))
+    grid = tuple(int(x) for x in g["grid"]) if "grid" in g else (1, 1, 1, 1)
+    nthr = int(np.prod(grid))
+    if nthr > 1:  # an OpenMP build: one MyRand per thread, seeded seed + tid
+        tn = O.ThreadNoise(L, grid, [int(g["seed"]) + t for t in range(nthr)])
+        draw = tn.gauss_links
+    else:
+        rng = O.Rand55(int(g["seed"]))
+        draw = lambda: rng.gauss(o.V * 32)  # noqa: E731
     obs = []
     noise0 = None
     for s in range(int(g["steps"])):
-        nz = rng.gauss(o.V * 32)
+        nz = draw()
         if s == 0:
             noise0 = nz[:64].copy()
         otf = "onthefly" in g and bool(g["onthefly"])
-        ob = o.sweep(float(g["dt"]), nz, zero_modes=bool(g["zm"]), onthefly=otf)
+        ob = o.sweep(float(g["dt"]), nz, zero_modes=bool(g["zm"]), onthefly=otf, grid=grid)
         if "c1" in g:
             ob.w2 = o.last_w2()
         obs.append(ob)
@@ -40,7 +47,7 @@ def replay(O, g):
         if bool(g["fa"]):
             o.fa_gauge_fix(float(g["alpha"]))
         elif bool(g["local_gf"]):
-            o.local_gauge_fix(float(g["alpha"]))
+            o.local_gauge_fix(float(g["alpha"]), grid=grid)
         o.twist_boundary()
     return o, p0, noise0, obs
 
