@@ -363,17 +363,28 @@ static int launch_sweep_imp_otf(nspt_ctx *ctx, const SweepArgs &a) {
   const size_t smem = (size_t)k.warps * LPW * group_bytes(ctx, IMP_SLOTS, 0);
   const long per_cta = (long)k.warps * LPW;
   const unsigned grid = (unsigned)((gr.nthr + per_cta - 1) / per_cta);
-  const void *fn = low ? (const void *)k_sweep_imp_otf<true> : (const void *)k_sweep_imp_otf<false>;
-  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int nmu = gr.seg == 1 ? 4 : 1;
-  for (long p = 0; p < steps; p++)
-    for (int q = 0; q < nmu; q++) {
-      const int lo = nmu == 4 ? q : 0, hi = nmu == 4 ? q + 1 : 4;
+  if (gr.seg == 1) {
+    const void *fn =
+        low ? (const void *)k_sweep_imp_otf1<true> : (const void *)k_sweep_imp_otf1<false>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    for (long p = 0; p < steps; p++)
+      for (int mu = 0; mu < 4; mu++) {
+        if (low)
+          k_sweep_imp_otf1<true><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, mu);
+        else
+          k_sweep_imp_otf1<false><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, mu);
+      }
+  } else {
+    const void *fn =
+        low ? (const void *)k_sweep_imp_otf<true> : (const void *)k_sweep_imp_otf<false>;
+    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    for (long p = 0; p < steps; p++) {
       if (low)
-        k_sweep_imp_otf<true><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, lo, hi);
+        k_sweep_imp_otf<true><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, 0, 4);
       else
-        k_sweep_imp_otf<false><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, lo, hi);
+        k_sweep_imp_otf<false><<<grid, 32 * k.warps, smem, ctx->st>>>(a, gr, p, 0, 4);
     }
+  }
   CK(cudaGetLastError());
   return NSPT_OK;
 }

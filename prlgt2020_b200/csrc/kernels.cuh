@@ -954,6 +954,28 @@ __global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
   imp_one<LOW, false>(a, L, T, Y, W, W2, mu, site);
 }
 
+// The improved-action sweep on the fly where each reference thread owns one
+// site per barrier step: link mu of that site, one launch per (step, mu),
+// the update inline without a walk around it.
+template <bool LOW = false>
+__global__ void __launch_bounds__(LOW ? SWEEP_THREADS_LOW : 256, LOW ? 2 : 1)
+    k_sweep_imp_otf1(SweepArgs a, LgfGrid gr, long step, int mu) {
+  extern __shared__ double2 sm[];
+  Lane L;
+  int g;
+  if (!make_lane(L, g)) return;
+  const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const long tid = ((long)blockIdx.x * nw + warp) * LPW + g;
+  if (tid >= gr.nthr) return;
+  const int SS = a.SS;
+  double2 *T = sm + (size_t)(warp * LPW + g) * (IMP_SLOTS * SS), *Y = T + SS;
+  double2 *W = Y + SS, *W2 = W + SS;
+  int x[4];
+  LgfWalk(gr, tid, step).site(gr, a.g, 0, x);
+  const int site = x[0] * a.g.s0 + x[1] * a.g.s1 + x[2] * a.g.s2 + x[3];
+  imp_one<LOW, true>(a, L, T, Y, W, W2, mu, site);
+}
+
 // The improved-action sweep on the fly (periodic boundaries): as
 // k_sweep_otf, one group per reference thread walking its sites for one
 // barrier step, links mu_lo..mu_hi-1 of each site in place (a launch per
