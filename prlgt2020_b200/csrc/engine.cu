@@ -965,6 +965,7 @@ extern "C" size_t nspt_device_bytes(const nspt_ctx *ctx) { return ctx ? ctx->byt
 extern "C" int nspt_cold_start(nspt_ctx *ctx) {
   if (!ctx) return NSPT_ERR_ARG;
   ctx->lg_current = false;
+  ctx->snap_valid = false;  // a new field: no stale twisted reads
   const size_t nU = (size_t)4 * 9 * ctx->N * ctx->V, nF = (size_t)4 * ctx->V;
   k_cold<<<ctx->nsm * 8, 256, 0, ctx->st>>>(ctx->U, ctx->Uf, nU, nF);
   CK(cudaGetLastError());
@@ -977,6 +978,7 @@ static const size_t kChunkBytes = 64u << 20;
 extern "C" int nspt_upload_links(nspt_ctx *ctx, const void *aos, int A) {
   if (!ctx || !aos || A < ctx->N) return NSPT_ERR_ARG;
   ctx->lg_current = false;
+  ctx->snap_valid = false;  // a new field: no stale twisted reads
   const size_t per_site = (size_t)4 * (1 + 9 * A) * sizeof(double2);
   const int cs = (int)std::max<size_t>(1, std::min<size_t>(kChunkBytes / per_site, ctx->V));
   double2 *buf = nullptr;

@@ -183,3 +183,25 @@ def test_onthefly_improved_action_needs_blocks_of_three(engine_mod):
         e.set_gf_grid((2, 2, 2, 2))
     e.set_gf_grid((1, 1, 1, 1))
     P.NsptEngine((4, 4, 4, 4), 3, action="tlsym").set_gf_grid((2, 2, 2, 2))
+
+
+def test_onthefly_new_field_ends_stale_twisted_reads(engine_mod, oracle_mod):
+    """Uploading a field replaces the step's start field as well: a sweep
+    right after it, with no twist_boundary between, reads the new field
+    across the twisted faces."""
+    P, O = engine_mod, oracle_mod
+    L, N, grid = (4, 4, 4, 4), 5, (2, 2, 2, 2)
+    e, o = pair(P, O, L, N, twist="yz", start=301, grid=grid)
+    rng = O.Rand55(5)
+    nz = rng.gauss(o.V * 32)
+    e.set_noise(nz)
+    e.gauge_wilson(0.01)  # leaves the start field for twisted reads
+    o2 = O.Oracle(L, N, twist_mask=6)
+    o2.random_start(302, 0.5)
+    e.upload(o2.links)
+    nz = rng.gauss(o.V * 32)
+    e.set_noise(nz)
+    eo = e.gauge_wilson(0.01)
+    oo = o2.sweep(0.01, nz, onthefly=True, grid=grid)
+    check_obs(eo, oo, 1e-11)
+    assert per_order_rel(e.download(), o2.links, N).max() <= 1e-12
